@@ -1,0 +1,345 @@
+#!/usr/bin/env python3
+"""Benchmark: imputed genotypes/s of the imputation step on the batched
+dense-cohort workload (4,432 x 50,000 panel, 10,000 targets typed at 3,000
+evenly spaced markers, L=8, Ne=20,000), one JSON line on rank 0.
+
+A step = one pass of the hot path over the whole batch: per-marker L-state
+selection from the resident PBWT index, then the fused FP32 forward-backward
+with posterior dosage and argmax haplotypes, for all 10,000 chains. The PBWT
+index is built once per panel before timing (reported as pbwt_build_ms).
+
+  value  device-resident inputs/outputs, CUDA events on the launch stream,
+         max over ranks; inputs (500 MB) exceed L2 so no flush is needed.
+  e2e    the public C ABI call si_impute with pinned host buffers: H2D of the
+         genotype codes and D2H of dosage + haplotypes inside the timed region.
+
+--impl reference times the reference's path on the host cores instead: the
+reference has no CPU forward-backward, so its recurrences are run through the
+FP64 C port (oracle/), threaded over samples, on a bounded sample per step.
+
+Multi-GPU (torchrun): every rank imputes its own copy of the per-GPU batch
+(independent chains, no data-path collective): weak scaling.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import time
+from pathlib import Path
+
+import numpy as np
+
+ROOT = Path(__file__).resolve().parent
+sys.path.insert(0, str(ROOT))
+
+CONFIGS = {
+    "dense-cohort": dict(M=50_000, N=4432, B=10_000, n_typed=3000, founders=100, L=8, ne=20000, seed=1),
+    "plain-small": dict(M=1644, N=4432, B=444, every=5, founders=40, L=8, ne=10000, seed=0),
+}
+ALGO_BYTES_PER_CELL = 7  # 1 B genotype code in, 4 B dosage + 2 B haplotype alleles out
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--config", choices=sorted(CONFIGS), default="dense-cohort")
+    ap.add_argument("--samples", type=int, default=0, help="override the batch size B")
+    ap.add_argument("--markers", type=int, default=0, help="override the marker count M")
+    ap.add_argument("--e2e-steps", type=int, default=3)
+    ap.add_argument("--cpu-seconds", type=float, default=12.0)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def make_workload(cfg):
+    from swiftimpute_b200 import synth
+    M, N, B = cfg["M"], cfg["N"], cfg["B"]
+    panel, pos, _ = synth.make_panel(M, N, cfg["founders"], (0.5, 0.5), 0.01, 0.005, seed=cfg["seed"])
+    typed = synth.typed_evenly(M, cfg["n_typed"]) if "n_typed" in cfg else synth.typed_every(M, cfg["every"])
+    codes, truth, _ = synth.make_targets(panel, B, typed, seed=cfg["seed"] + 1000)
+    return panel, pos, typed, codes, truth
+
+
+def clock_sampler_start(device: int):
+    import tempfile
+    try:
+        f = tempfile.NamedTemporaryFile("w", suffix=".clocks.csv", delete=False)
+        p = subprocess.Popen(
+            ["nvidia-smi", f"--id={device}",
+             "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
+             "--format=csv,noheader,nounits", "-lms", "100"], stdout=f, stderr=subprocess.DEVNULL)
+        return p, f
+    except Exception:
+        return None, None
+
+
+def clock_sampler_stop(handle):
+    p, f = handle
+    if p is None:
+        return None
+    p.terminate()
+    try:
+        p.wait(timeout=5)
+    except Exception:
+        p.kill()
+    f.close()
+    rows = []
+    for line in Path(f.name).read_text().splitlines():
+        parts = [x.strip() for x in line.split(",")]
+        if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
+            rows.append(parts)
+    if not rows:
+        return None
+    sm = [float(r[1]) for r in rows]
+    reasons = set()
+    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+    for r in rows:
+        for name, v in zip(names, r[5:9]):
+            if v.lower() in ("active", "1"):
+                reasons.add(name)
+    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
+            "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+
+
+def peaks():
+    try:
+        d = json.loads((ROOT / "MEASURED_PEAKS.json").read_text())
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def profile_traffic(kernel: str, config: str):
+    """Per-launch DRAM bytes from the committed ncu summary of this kernel and workload, if any."""
+    f = ROOT / "profiles" / f"{kernel}.{config}.md"
+    if not f.exists():
+        return None
+    for line in f.read_text().splitlines():
+        if line.startswith("traffic_bytes_per_launch:"):
+            return float(line.split(":", 1)[1].strip())
+    return None
+
+
+def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds):
+    """The FP64 port of the reference recurrences on all host threads, on the
+    first S samples of the workload (S sized to ~`seconds` of CPU work)."""
+    import oracle
+    threads = os.cpu_count() or 1
+    M = codes.shape[1]
+    s = max(1, threads)
+    t0 = time.perf_counter()
+    oracle.fb_batch(codes[:s], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
+    dt = time.perf_counter() - t0
+    S = int(min(codes.shape[0], max(s, round(s * seconds / max(dt, 1e-3)))))
+    t0 = time.perf_counter()
+    oracle.fb_batch(codes[:S], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
+    dt = time.perf_counter() - t0
+    imputed = S * (M - len(typed))
+    return {"value": imputed / dt, "unit": "imputed genotypes/s", "cores": threads, "kind": "port",
+            "sample": f"first {S} of {codes.shape[0]} targets x {M} markers, FP64 log-space restatement of the "
+                      f"reference recurrences, {dt:.1f} s"}
+
+
+def run_reference(args, cfg):
+    """Reference arm: the reference's recurrences on the host cores (rank 0)."""
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return
+    import oracle
+    from swiftimpute_b200 import synth
+    cfg = dict(cfg)
+    panel, pos, typed, codes, truth = make_workload(cfg)
+    pairs = oracle.select_pairs(oracle.pbwt_build_packed(synth.pack_panel(panel), cfg["N"])[0], cfg["L"])
+    threads = os.cpu_count() or 1
+    M = codes.shape[1]
+    # each step: a bounded sample of the batch (~4 s of CPU work)
+    t0 = time.perf_counter()
+    oracle.fb_batch(codes[:threads], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
+    per = (time.perf_counter() - t0) / threads
+    S = int(max(threads, min(codes.shape[0], threads * round(4.0 / max(per * threads, 1e-3)))))
+    for w in range(args.warmup):
+        oracle.fb_batch(codes[:threads], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
+    times = []
+    for k in range(args.steps):
+        rows = codes[(k * S) % max(1, codes.shape[0] - S):][:S]
+        t0 = time.perf_counter()
+        oracle.fb_batch(rows, pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
+        times.append(time.perf_counter() - t0)
+    ms = 1e3 * sum(times) / len(times)
+    value = S * (M - len(typed)) / (ms / 1e3)
+    unit = "imputed genotypes/s"
+    line = {
+        "impl": "reference", "metric": "imputed genotypes/s", "value": value, "unit": unit, "n_gpus": args.gpus,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, config shape)",
+        "config": {"workload": args.config, "markers": M, "haplotypes": cfg["N"], "targets_per_step": S,
+                   "typed_markers": int(len(typed)), "L": cfg["L"], "ne": cfg["ne"]},
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+                         "sample": f"{S} targets x {M} markers per step; the reference has no CPU forward-backward, "
+                                   "so its recurrences run through the FP64 C port"},
+        "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, cfg):
+    import torch
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200.engine import Engine
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dist = None
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300), device_id=torch.device("cuda", local))
+
+    panel, pos, typed, codes, truth = make_workload(cfg)
+    B, M = codes.shape
+    eng = Engine(local)
+    eng.upload_panel(panel)
+    eng.set_map(pos)
+    pbwt_ms = eng.pbwt_build()
+    params = N.default_params(num_states=cfg["L"], ne=cfg["ne"], flags=N.IMPUTE_RESELECT)
+
+    dev = torch.device("cuda", local)
+    d_geno = torch.from_numpy(codes).to(dev)
+    d_dos = torch.empty((B, M), dtype=torch.float32, device=dev)
+    d_haps = torch.empty((B, 2, M), dtype=torch.uint8, device=dev)
+    stream = torch.cuda.Stream(dev)  # a real (non-legacy) stream: the events below bracket our kernels
+    torch.cuda.synchronize(dev)
+
+    def step():
+        eng.impute_device(d_geno.data_ptr(), B, params, d_dos.data_ptr(), None, d_haps.data_ptr(), stream.cuda_stream)
+
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize(dev)
+    # correctness spot-check of the device path against the host-buffer path is in tests; here only timing
+    clocks = clock_sampler_start(local)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize(dev)
+    evs = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    t_start = torch.cuda.Event(enable_timing=True)
+    t_end = torch.cuda.Event(enable_timing=True)
+    t_start.record(stream)
+    for k in range(args.steps):
+        evs[k][0].record(stream)
+        step()
+        evs[k][1].record(stream)
+    t_end.record(stream)
+    torch.cuda.synchronize(dev)
+    if dist:
+        dist.barrier()
+    clock_info = clock_sampler_stop(clocks)
+    total_ms = t_start.elapsed_time(t_end)
+    kern_ms = [a.elapsed_time(b) for a, b in evs]
+    if dist:
+        t = torch.tensor([total_ms], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    imputed_per_gpu = B * (M - len(typed))
+    value = world * imputed_per_gpu / (ms_per_step / 1e3)
+
+    # end to end through the public C ABI with pinned host buffers
+    h_geno = torch.from_numpy(codes).pin_memory()
+    h_dos = torch.empty((B, M), dtype=torch.float32).pin_memory()
+    h_haps = torch.empty((B, 2, M), dtype=torch.uint8).pin_memory()
+    from ctypes import byref, c_void_p
+    p_e2e = N.default_params(num_states=cfg["L"], ne=cfg["ne"], flags=N.IMPUTE_RESELECT)
+
+    def e2e_step():
+        eng._check(eng.lib.si_impute(eng.h, byref(p_e2e), c_void_p(h_geno.data_ptr()), B,
+                                     c_void_p(h_dos.data_ptr()), None, c_void_p(h_haps.data_ptr())))
+    e2e_step()
+    if dist:
+        dist.barrier()
+    t0 = time.perf_counter()
+    for _ in range(args.e2e_steps):
+        e2e_step()
+    e2e_s = (time.perf_counter() - t0) / args.e2e_steps
+    if dist:
+        t = torch.tensor([e2e_s], device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        e2e_s = float(t.item())
+    e2e_value = world * imputed_per_gpu / e2e_s
+    # quality vs truth on the device outputs (masked markers)
+    dos = d_dos.cpu().numpy()
+    masked = np.setdiff1d(np.arange(M), typed)
+    sub = slice(0, min(B, 500))
+    r2 = float(np.corrcoef(dos[sub][:, masked].ravel(), truth[sub][:, masked].ravel())[0, 1] ** 2)
+
+    if rank != 0:
+        eng.close()
+        if dist:
+            dist.destroy_process_group()
+        return
+
+    peak, peak_kind = peaks()
+    avg_kern = sum(kern_ms) / len(kern_ms)
+    algo = ALGO_BYTES_PER_CELL * B * M
+    achieved = algo / (avg_kern / 1e3) / 1e9
+    traffic = profile_traffic("fb_chain_kernel", args.config)
+    line = {
+        "metric": "imputed genotypes/s", "value": value, "unit": "imputed genotypes/s", "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32",
+        "data": "synthetic (seeded generator with the config's shape; the reference's dataset is unavailable)",
+        "config": {"workload": f"{args.config}: {cfg['N']} haplotypes x {M} markers, {B} targets typed at "
+                               f"{len(typed)} markers, L={cfg['L']}, Ne={cfg['ne']}",
+                   "markers": M, "haplotypes": cfg["N"], "targets": B, "typed_markers": int(len(typed)),
+                   "L": cfg["L"], "ne": cfg["ne"], "l2": "inputs (B*M bytes) larger than L2, no flush",
+                   "parallelism": f"replicas x{world} (independent chains)"},
+        "roofline": {"bound": "hbm", "kernel": "fb_chain_kernel", "achieved": achieved, "peak": peak,
+                     "unit": "GB/s", "frac": achieved / peak, "peak_kind": peak_kind,
+                     "traffic": traffic, "algorithmic_bytes_per_launch": algo,
+                     "avg_launch_ms": avg_kern},
+        "e2e": {"value": e2e_value, "unit": "imputed genotypes/s", "h2d_bytes_per_step": int(B * M),
+                "d2h_bytes_per_step": int(B * M * 4 + B * 2 * M), "ms_per_step": e2e_s * 1e3},
+        "gpu_launches": 2 * args.steps,
+        "pbwt_build_ms": pbwt_ms,
+        "dosage_r2_vs_truth": r2,
+    }
+    if clock_info:
+        line["clocks"] = clock_info
+    if not args.no_cpu_baseline and world == 1:
+        import oracle
+        pairs = eng.select_states(cfg["L"])
+        line["cpu_baseline"] = cpu_baseline(panel, pos, codes, pairs, typed, cfg, args.cpu_seconds)
+    eng.close()
+    print(json.dumps(line), flush=True)
+    if dist:
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse()
+    cfg = dict(CONFIGS[args.config])
+    if args.samples:
+        cfg["B"] = args.samples
+    if args.markers:
+        cfg["M"] = args.markers
+        if "n_typed" in cfg:
+            cfg["n_typed"] = max(1, round(cfg["n_typed"] * args.markers / CONFIGS[args.config]["M"]))
+    if args.impl == "reference":
+        run_reference(args, cfg)
+    else:
+        run_ours(args, cfg)
+
+
+if __name__ == "__main__":
+    main()

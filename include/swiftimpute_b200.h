@@ -1,0 +1,180 @@
+/*
+ * swiftimpute_b200.h — C ABI of the B200 Li–Stephens imputation engine.
+ *
+ * Plain pointers and sizes only; every call returns an si_status and never
+ * throws. Host pointers are read/written before the call returns unless a
+ * function says otherwise. One si_ctx per device; a ctx is not thread-safe
+ * except for the si_serve_* functions.
+ *
+ * Each entry point names the reference (tcBio/SwiftImpute) interface it
+ * replaces, as path:line in the reference source tree.
+ */
+#ifndef SWIFTIMPUTE_B200_H
+#define SWIFTIMPUTE_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define SI_ABI_VERSION 1
+
+typedef enum {
+    SI_OK = 0,
+    SI_ERR_INVALID_ARG = 1,   /* bad pointer, size or enum */
+    SI_ERR_CUDA = 2,          /* a CUDA runtime call failed; see si_last_error */
+    SI_ERR_OUT_OF_MEMORY = 3, /* cudaMalloc failed */
+    SI_ERR_UNSUPPORTED = 4,   /* shape or parameter outside what the kernels handle */
+    SI_ERR_STATE = 5,         /* call order (e.g. impute before panel upload) */
+    SI_ERR_TIMEOUT = 6,       /* a bounded device or host wait gave up */
+    SI_ERR_BUDGET = 7,        /* request exceeds the context's HBM budget */
+    SI_ERR_CANCELLED = 8      /* serving request cancelled */
+} si_status;
+
+typedef struct si_ctx si_ctx;
+
+/* Selection kinds: which reference kernel's pattern to reproduce. AUTO picks
+ * as launch_select_states does (pbwt_selector.cu:413-456). */
+enum { SI_SEL_AUTO = 0, SI_SEL_WARP = 1, SI_SEL_INSERTION = 2 };
+
+/* Transition modes. MATRIX0 reproduces the reference, whose forward-backward
+ * reads the first gap's matrix for every gap (forward_backward.cu:108,201,234,269).
+ * PER_GAP uses each gap's own matrix. */
+enum { SI_TRANS_MATRIX0 = 0, SI_TRANS_PER_GAP = 1 };
+
+/* Haplotype output: argmax slot (sampling.cu:138-182 with a tie tolerance) or
+ * a draw from the posterior with a counter-based Philox4x32-10 stream keyed by
+ * (seed, sample id, marker), so a sample's draw never depends on its batch. */
+enum { SI_SAMPLE_ARGMAX = 0, SI_SAMPLE_PHILOX = 1 };
+
+/* si_pbwt_build flags */
+enum {
+    SI_PBWT_STORE_INDEX = 1u,  /* keep the full prefix array [M][N] u32 on the device */
+    SI_PBWT_ROW_HASHES = 2u    /* keep a 64-bit hash of every prefix row */
+};
+
+/* si_impute_params.flags */
+enum {
+    SI_IMPUTE_RESELECT = 1u  /* recompute the per-marker selection tables in this call (else cached per L) */
+};
+
+/* Genotype codes for si_impute: 0, 1, 2 = ALT allele count of a hard call,
+ * 3 = missing (the reference's GL triple {0,0,0}, imputer.cpp:253-267). */
+enum { SI_GENO_MISSING = 3 };
+
+typedef struct {
+    uint32_t num_states;          /* L, 1..32 (HMMParameters::num_states, core/types.hpp:81) */
+    uint32_t ne;                  /* effective population size (HMMParameters::ne) */
+    double rho_rate;              /* HMMParameters::rho_rate (default 4.0) */
+    double theta;                 /* HMMParameters::theta (unused by the reference kernels) */
+    int32_t transition_mode;      /* SI_TRANS_* */
+    int32_t selection_kind;       /* SI_SEL_* */
+    int32_t sampling;             /* SI_SAMPLE_* */
+    uint32_t flags;               /* SI_IMPUTE_* */
+    double tie_eps;               /* argmax picks the first slot with p >= (1 - tie_eps) * max p */
+    uint64_t seed;                /* Philox key */
+    uint64_t sample_id_base;      /* Philox counter: sample id of row 0 */
+    uint32_t checkpoint_interval; /* markers per forward checkpoint; 0 = autotuned */
+    uint32_t block_threads;       /* chains per CTA; 0 = autotuned */
+    uint64_t reserved[4];
+} si_impute_params;
+
+/* Library / context ------------------------------------------------------ */
+
+int si_abi_version(void);
+const char* si_status_string(si_status s);
+
+/* Replaces Imputer::initialize_gpu (imputer.cpp:555-567). hbm_budget_bytes = 0
+ * means "all free memory". */
+si_status si_ctx_create(int device, uint64_t hbm_budget_bytes, si_ctx** out);
+si_status si_ctx_destroy(si_ctx* ctx);
+/* Message of the last failed call on this ctx (never NULL). */
+const char* si_last_error(const si_ctx* ctx);
+/* Replaces Imputer::device_memory_usage (imputer.cpp:1176-1212). */
+si_status si_ctx_memory(const si_ctx* ctx, uint64_t* used_bytes, uint64_t* budget_bytes);
+
+/* Panel ------------------------------------------------------------------ */
+
+/* Upload a u8 panel [M][N] (ReferencePanel::haplotypes(), imputer.hpp:86).
+ * Alleles must be 0 or 1; it is stored bit-packed on the device. Replaces the
+ * panel copies of EmissionComputer::set_reference_panel (emission.cu:189) and
+ * HaplotypeSampler::set_reference_panel (sampling.cu:219). */
+si_status si_panel_upload_u8(si_ctx* ctx, const uint8_t* alleles, uint32_t M, uint32_t N);
+
+/* Upload an already bit-packed panel [M][words_per_row] u32: bit i of word w
+ * is haplotype 32 w + i. words_per_row >= ceil(N / 32). */
+si_status si_panel_upload_packed(si_ctx* ctx, const uint32_t* words, uint32_t M, uint32_t N,
+                                 uint32_t words_per_row);
+
+/* Marker positions for the genetic map: Morgans = cM / 100 where cM > 0, else
+ * pos / 1e8, as Imputer::initialize_gpu_kernels (imputer.cpp:596-604).
+ * cM may be NULL. Replaces TransitionComputer::set_genetic_map (transition.cu:218). */
+si_status si_panel_set_map(si_ctx* ctx, const uint64_t* pos, const double* cM);
+
+/* PBWT ------------------------------------------------------------------- */
+
+/* Run the PBWT prefix sweep on the device. Replaces Imputer::build_index
+ * (imputer.cpp:706-728) -> PBWTIndex::build (pbwt_index.cpp:12) and
+ * GPUStateSelector::transfer_index_to_device (pbwt_index.cpp:355). The
+ * divergence array of the reference is m in every entry of row m
+ * (pbwt_index.cpp:173-191), so it is implicit. */
+si_status si_pbwt_build(si_ctx* ctx, uint32_t flags);
+
+/* Copy prefix rows [m0, m0 + count) to host out [count][N]. Needs
+ * SI_PBWT_STORE_INDEX. Replaces PBWTIndex::prefix() (pbwt_index.hpp:61). */
+si_status si_pbwt_get_prefix_rows(si_ctx* ctx, uint32_t m0, uint32_t count, uint32_t* out);
+
+/* Copy the per-row hashes [M] (needs SI_PBWT_ROW_HASHES). */
+si_status si_pbwt_row_hashes(si_ctx* ctx, uint64_t* out);
+
+/* Milliseconds of the last si_pbwt_build sweep (CUDA events). */
+si_status si_pbwt_last_ms(const si_ctx* ctx, float* ms);
+
+/* Selection -------------------------------------------------------------- */
+
+/* Slots of markers [m0, m1) as haplotype pairs out [m1-m0][L][2], the result
+ * of launch_select_states (pbwt_selector.cu:400) followed by the host pair
+ * expansion (h, (h + 1) % N) (imputer.cpp:863-874). The selection does not
+ * depend on the target sample, so it is computed once per marker. */
+si_status si_select_states(si_ctx* ctx, uint32_t L, int32_t kind, uint32_t m0, uint32_t m1,
+                           uint32_t* out_pairs);
+
+/* Imputation ------------------------------------------------------------- */
+
+si_status si_impute_params_default(si_impute_params* p);
+
+/* Impute B samples over all M markers from HOST buffers (copies inside).
+ * geno [B][M] genotype codes. Outputs (each may be NULL):
+ *   dosage   [B][M]     posterior ALT dosage
+ *   hap_prob [B][M][2]  P(hap0 = 1), P(hap1 = 1) (ImputationResult::posteriors_, imputer.hpp:192)
+ *   haps     [B][2][M]  phased alleles (ImputationResult::haplotypes_, imputer.hpp:191)
+ * Replaces Imputer::impute_batch (imputer.cpp:787-1042): selection, emission
+ * (emission.cu:208), forward/backward (forward_backward.cu:321,356) and
+ * HaplotypeSampler::sample (sampling.cu:269) run as one fused device pass. */
+si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno, uint32_t B,
+                    float* dosage, float* hap_prob, uint8_t* haps);
+
+/* Same, from reference-layout genotype likelihoods gl [B][M][3] (log10,
+ * TargetData::genotype_likelihoods(), imputer.hpp:125). Cells whose three
+ * values are equal are missing; cells with one 0 and two -999 are hard calls;
+ * any other triple is SI_ERR_UNSUPPORTED. */
+si_status si_impute_gl(si_ctx* ctx, const si_impute_params* p, const float* gl, uint32_t B,
+                       float* dosage, float* hap_prob, uint8_t* haps);
+
+/* Device-pointer variant: all buffers are device memory owned by the caller,
+ * work is queued on `stream` (a cudaStream_t, may be NULL) and the call
+ * returns without synchronising. Scratch memory comes from the ctx. */
+si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
+                           float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
+
+/* Milliseconds of the last si_impute* device work (CUDA events): [0] selection,
+ * [1] forward-backward kernel, [2] whole call including copies (host-buffer
+ * calls only). For si_impute_device this waits for the call's kernels. */
+si_status si_last_timings(si_ctx* ctx, float* ms3);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

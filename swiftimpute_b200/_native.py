@@ -1,0 +1,114 @@
+"""ctypes binding of the C ABI declared in ``include/swiftimpute_b200.h``.
+
+The library is the in-tree ``swiftimpute_b200/lib/libswiftimpute_b200.so``.
+There is no fallback: if the library is missing or fails to load, every entry
+point raises :class:`NativeLibraryError`.
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import POINTER, c_char_p, c_double, c_float, c_int, c_int32, c_uint32, c_uint64, c_void_p
+from pathlib import Path
+
+LIB_PATH = Path(__file__).resolve().parent / "lib" / "libswiftimpute_b200.so"
+
+SI_OK = 0
+STATUS_NAMES = {
+    0: "SI_OK", 1: "SI_ERR_INVALID_ARG", 2: "SI_ERR_CUDA", 3: "SI_ERR_OUT_OF_MEMORY",
+    4: "SI_ERR_UNSUPPORTED", 5: "SI_ERR_STATE", 6: "SI_ERR_TIMEOUT", 7: "SI_ERR_BUDGET",
+    8: "SI_ERR_CANCELLED",
+}
+SEL_AUTO, SEL_WARP, SEL_INSERTION = 0, 1, 2
+TRANS_MATRIX0, TRANS_PER_GAP = 0, 1
+SAMPLE_ARGMAX, SAMPLE_PHILOX = 0, 1
+PBWT_STORE_INDEX, PBWT_ROW_HASHES = 1, 2
+GENO_MISSING = 3
+IMPUTE_RESELECT = 1
+
+
+class NativeLibraryError(RuntimeError):
+    """The CUDA library could not be loaded; there is no CPU fallback."""
+
+
+class SIError(RuntimeError):
+    def __init__(self, status: int, message: str):
+        self.status = status
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {message}")
+
+
+class ImputeParams(ctypes.Structure):
+    """Mirror of ``si_impute_params``."""
+    _fields_ = [
+        ("num_states", c_uint32),
+        ("ne", c_uint32),
+        ("rho_rate", c_double),
+        ("theta", c_double),
+        ("transition_mode", c_int32),
+        ("selection_kind", c_int32),
+        ("sampling", c_int32),
+        ("flags", c_uint32),
+        ("tie_eps", c_double),
+        ("seed", c_uint64),
+        ("sample_id_base", c_uint64),
+        ("checkpoint_interval", c_uint32),
+        ("block_threads", c_uint32),
+        ("reserved", c_uint64 * 4),
+    ]
+
+
+# (name, restype, argtypes) for every symbol the header declares.
+SIGNATURES = [
+    ("si_abi_version", c_int, []),
+    ("si_status_string", c_char_p, [c_int]),
+    ("si_ctx_create", c_int, [c_int, c_uint64, POINTER(c_void_p)]),
+    ("si_ctx_destroy", c_int, [c_void_p]),
+    ("si_last_error", c_char_p, [c_void_p]),
+    ("si_ctx_memory", c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
+    ("si_panel_upload_u8", c_int, [c_void_p, c_void_p, c_uint32, c_uint32]),
+    ("si_panel_upload_packed", c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32]),
+    ("si_panel_set_map", c_int, [c_void_p, c_void_p, c_void_p]),
+    ("si_pbwt_build", c_int, [c_void_p, c_uint32]),
+    ("si_pbwt_get_prefix_rows", c_int, [c_void_p, c_uint32, c_uint32, c_void_p]),
+    ("si_pbwt_row_hashes", c_int, [c_void_p, c_void_p]),
+    ("si_pbwt_last_ms", c_int, [c_void_p, POINTER(c_float)]),
+    ("si_select_states", c_int, [c_void_p, c_uint32, c_int32, c_uint32, c_uint32, c_void_p]),
+    ("si_impute_params_default", c_int, [POINTER(ImputeParams)]),
+    ("si_impute", c_int, [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p]),
+    ("si_impute_gl", c_int, [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p]),
+    ("si_impute_device", c_int,
+     [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("si_last_timings", c_int, [c_void_p, POINTER(c_float)]),
+]
+
+_lib = None
+
+
+def load() -> ctypes.CDLL:
+    """Load the library once; raise NativeLibraryError if it is absent."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not LIB_PATH.exists():
+        raise NativeLibraryError(
+            f"{LIB_PATH} not found: build it with `python -m swiftimpute_b200.build` "
+            "(there is no CPU fallback)")
+    try:
+        lib = ctypes.CDLL(str(LIB_PATH))
+    except OSError as e:  # pragma: no cover - depends on the host
+        raise NativeLibraryError(f"cannot load {LIB_PATH}: {e}") from e
+    for name, res, args in SIGNATURES:
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def default_params(**overrides) -> ImputeParams:
+    p = ImputeParams()
+    load().si_impute_params_default(ctypes.byref(p))
+    for k, v in overrides.items():
+        if not hasattr(p, k):
+            raise AttributeError(k)
+        setattr(p, k, v)
+    return p

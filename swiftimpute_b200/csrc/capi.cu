@@ -1,0 +1,539 @@
+// capi.cu — the C ABI (include/swiftimpute_b200.h) over the device kernels.
+#include "si_internal.hpp"
+
+#include <algorithm>
+#include <cmath>
+#include <cstring>
+#include <new>
+
+namespace si {
+
+si_status fail(si_ctx* ctx, si_status s, const std::string& msg) {
+    if (ctx) ctx->err = msg;
+    return s;
+}
+
+si_status cuda_fail(si_ctx* ctx, cudaError_t e, const char* what) {
+    std::string m = std::string(what) + ": " + cudaGetErrorName(e) + " (" + cudaGetErrorString(e) + ")";
+    return fail(ctx, e == cudaErrorMemoryAllocation ? SI_ERR_OUT_OF_MEMORY : SI_ERR_CUDA, m);
+}
+
+si_status dev_alloc(si_ctx* ctx, DeviceBuffer& buf, size_t bytes) {
+    dev_free(ctx, buf);
+    if (bytes == 0) bytes = 16;
+    bytes = (bytes + 255) & ~size_t(255);
+    if (ctx->used + bytes > ctx->budget)
+        return fail(ctx, SI_ERR_BUDGET, "HBM budget exceeded: need " + std::to_string(bytes) + " more bytes, " +
+                                            std::to_string(ctx->budget - ctx->used) + " left");
+    void* p = nullptr;
+    cudaError_t e = cudaMalloc(&p, bytes);
+    if (e != cudaSuccess) { cudaGetLastError(); return cuda_fail(ctx, e, "cudaMalloc"); }
+    buf.ptr = p;
+    buf.bytes = bytes;
+    ctx->used += bytes;
+    return SI_OK;
+}
+
+void dev_free(si_ctx* ctx, DeviceBuffer& buf) {
+    if (buf.ptr) {
+        cudaFree(buf.ptr);
+        ctx->used -= buf.bytes;
+    }
+    buf.ptr = nullptr;
+    buf.bytes = 0;
+}
+
+si_status dev_reserve(si_ctx* ctx, DeviceBuffer& buf, size_t bytes) {
+    if (buf.ptr && buf.bytes >= bytes) return SI_OK;
+    return dev_alloc(ctx, buf, bytes);
+}
+
+}  // namespace si
+
+using namespace si;
+
+#define SI_CUDA(ctx, call, what)                           \
+    do {                                                   \
+        cudaError_t e_ = (call);                           \
+        if (e_ != cudaSuccess) return cuda_fail(ctx, e_, what); \
+    } while (0)
+#define SI_TRY(x)                      \
+    do {                               \
+        si_status st_ = (x);           \
+        if (st_ != SI_OK) return st_;  \
+    } while (0)
+
+namespace {
+
+si_status set_device(si_ctx* ctx) {
+    SI_CUDA(ctx, cudaSetDevice(ctx->device), "cudaSetDevice");
+    return SI_OK;
+}
+
+void reset_index(si_ctx* ctx) {
+    dev_free(ctx, ctx->head);
+    dev_free(ctx, ctx->prefix);
+    dev_free(ctx, ctx->row_hash);
+    for (auto& kv : ctx->sel) {
+        dev_free(ctx, kv.second.pairs);
+        dev_free(ctx, kv.second.masks);
+    }
+    ctx->sel.clear();
+    ctx->has_index = false;
+    ctx->pbwt_flags = 0;
+}
+
+// Li–Stephens transition between genetic positions (Morgans), as
+// compute_transition_probs_kernel (transition.cu:83-115): FP64 maths, log10
+// values rounded to float, then read by natural-log recursions, so the linear
+// weights are exp(log10 value).
+LinTrans lin_trans(double gd0, double gd1, double ne, double rho_rate) {
+    double dist = gd1 - gd0;
+    if (dist < 0.0) dist = 0.0;
+    const double exponent = -4.0 * ne * dist * rho_rate;
+    double rho = 1.0 - std::exp(exponent);
+    if (rho < 0.0) rho = 0.0;
+    if (rho > 1.0) rho = 1.0;
+    const double stay = (1.0 - rho) + rho / (2.0 * ne);
+    const double sw = rho / (2.0 * ne);
+    const float t_diag = (float)std::log10(stay);
+    const float t_off = (sw < 1e-300) ? -999.0f : (float)std::log10(sw);
+    const double c = std::exp((double)t_off), d = std::exp((double)t_diag);
+    return LinTrans{(float)c, (float)(d - c)};
+}
+
+si_status ensure_trans(si_ctx* ctx, const si_impute_params* p) {
+    if (!ctx->has_map) return fail(ctx, SI_ERR_STATE, "marker positions not set (si_panel_set_map)");
+    uint64_t key = (uint64_t)p->transition_mode * 0x9E3779B97F4A7C15ull;
+    double pr[2] = {(double)p->ne, p->rho_rate};
+    uint64_t bits[2];
+    std::memcpy(bits, pr, sizeof bits);
+    key ^= bits[0] * 0xBF58476D1CE4E5B9ull ^ bits[1] * 0x94D049BB133111EBull;
+    if (ctx->trans.ptr && ctx->trans_key == key) return SI_OK;
+    const uint32_t M = ctx->M;
+    std::vector<LinTrans> t(M);
+    const double ne = (double)p->ne;
+    LinTrans t0 = M >= 2 ? lin_trans(ctx->morgans[0], ctx->morgans[1], ne, p->rho_rate) : LinTrans{1.f, 0.f};
+    for (uint32_t m = 0; m < M; ++m) {
+        if (p->transition_mode == SI_TRANS_PER_GAP && m >= 1)
+            t[m] = lin_trans(ctx->morgans[m - 1], ctx->morgans[m], ne, p->rho_rate);
+        else
+            t[m] = t0;
+        if (m >= 1 && !(t[m].c >= 1e-30f))
+            return fail(ctx, SI_ERR_UNSUPPORTED,
+                        "switch weight exp(log10 switch) = " + std::to_string(t[m].c) + " at marker " +
+                            std::to_string(m) +
+                            " is below 1e-30 (zero genetic distance); the FP32 linear-space kernel needs a "
+                            "representable switch weight");
+    }
+    SI_TRY(dev_reserve(ctx, ctx->trans, sizeof(LinTrans) * M));
+    SI_CUDA(ctx, cudaMemcpy(ctx->trans.ptr, t.data(), sizeof(LinTrans) * M, cudaMemcpyHostToDevice), "copy trans");
+    ctx->trans_key = key;
+    return SI_OK;
+}
+
+si_status ensure_selection(si_ctx* ctx, uint32_t L, int kind, SelectionCache** out, bool force = false,
+                           cudaStream_t s = nullptr) {
+    if (!ctx->has_index) return fail(ctx, SI_ERR_STATE, "PBWT index not built (si_pbwt_build)");
+    if (L == 0 || L > kHead) return fail(ctx, SI_ERR_INVALID_ARG, "L must be in 1..128");
+    if (kind == SI_SEL_AUTO) kind = (L <= 32 && ctx->N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+    if (kind != SI_SEL_WARP && kind != SI_SEL_INSERTION) return fail(ctx, SI_ERR_INVALID_ARG, "bad selection kind");
+    auto& c = ctx->sel[{L, kind}];
+    if (!c.pairs.ptr || force) {
+        c.L = L;
+        c.kind = kind;
+        if (!c.pairs.ptr) {
+            SI_TRY(dev_alloc(ctx, c.pairs, (size_t)ctx->M * L * 2 * sizeof(uint32_t)));
+            SI_TRY(dev_alloc(ctx, c.masks, (size_t)ctx->M * sizeof(SlotMasks)));
+        }
+        SI_CUDA(ctx,
+                launch_select((const uint32_t*)ctx->head.ptr, (const uint32_t*)ctx->panel.ptr, ctx->M, ctx->N, ctx->W,
+                              L, kind, (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, s ? s : ctx->stream),
+                "select kernel");
+    }
+    *out = &c;
+    return SI_OK;
+}
+
+si_status check_params(si_ctx* ctx, const si_impute_params* p) {
+    if (!p) return fail(ctx, SI_ERR_INVALID_ARG, "params is NULL");
+    if (p->num_states == 0 || p->num_states > 32)
+        return fail(ctx, SI_ERR_UNSUPPORTED, "num_states must be 1..32 (the reference sampler holds 32 slots)");
+    if (p->ne == 0) return fail(ctx, SI_ERR_INVALID_ARG, "ne must be positive");
+    if (p->transition_mode != SI_TRANS_MATRIX0 && p->transition_mode != SI_TRANS_PER_GAP)
+        return fail(ctx, SI_ERR_INVALID_ARG, "bad transition_mode");
+    if (p->sampling != SI_SAMPLE_ARGMAX && p->sampling != SI_SAMPLE_PHILOX)
+        return fail(ctx, SI_ERR_INVALID_ARG, "bad sampling mode");
+    if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
+    if (p->checkpoint_interval > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "checkpoint_interval must be <= 32");
+    if (p->block_threads && (p->block_threads % 32 || p->block_threads > 128))
+        return fail(ctx, SI_ERR_UNSUPPORTED, "block_threads must be a multiple of 32, <= 128");
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    return SI_OK;
+}
+
+// Tile choice per slot count: chains per CTA and markers per segment. The
+// alpha tile of a segment (C * Lmax * T floats) sits in shared memory.
+void default_tiles(uint32_t L, uint32_t* T, uint32_t* C) {
+    const uint32_t lm = fb_lmax(L);
+    *C = lm >= 32 ? 16 : 32;
+    *T = lm <= 8 ? 64 : 32;
+}
+
+// Device part of an imputation over B chains whose inputs/outputs are device
+// pointers; queued on stream s.
+si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B, float* d_dosage,
+                     float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
+    SelectionCache* sel = nullptr;
+    SI_TRY(ensure_selection(ctx, p->num_states, p->selection_kind, &sel, (p->flags & SI_IMPUTE_RESELECT) != 0, s));
+    if (s != ctx->stream && !(p->flags & SI_IMPUTE_RESELECT)) {
+        // a cached table may have been built on the ctx stream: order it before s
+        SI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream), "event");
+        SI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->ev[3], 0), "stream wait");
+    }
+    SI_TRY(ensure_trans(ctx, p));
+    uint32_t T, C;
+    default_tiles(p->num_states, &T, &C);
+    if (p->checkpoint_interval) C = p->checkpoint_interval;
+    if (p->block_threads) T = p->block_threads;
+    if (fb_smem_bytes(p->num_states, T, C) > 227u * 1024u)
+        return fail(ctx, SI_ERR_UNSUPPORTED,
+                    "tile (" + std::to_string(T) + " chains x " + std::to_string(C) + " markers) needs " +
+                        std::to_string(fb_smem_bytes(p->num_states, T, C)) + " bytes of shared memory (max 227 KB)");
+    SI_TRY(dev_reserve(ctx, ctx->ckpt, fb_ckpt_bytes(B, ctx->M, p->num_states, C)));
+    FbLaunch l;
+    l.geno = d_geno; l.masks = (const SlotMasks*)sel->masks.ptr; l.trans = (const LinTrans*)ctx->trans.ptr;
+    l.B = B; l.M = ctx->M; l.L = p->num_states; l.C = C; l.threads = T;
+    l.sampling = p->sampling; l.tie_eps = (float)p->tie_eps; l.seed = p->seed; l.sample_id_base = p->sample_id_base;
+    l.ckpt = (float*)ctx->ckpt.ptr; l.dosage = d_dosage; l.hprob = d_hprob; l.haps = d_haps;
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[1], s), "event");
+    SI_CUDA(ctx, launch_fb(l, s), "forward-backward kernel");
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[2], s), "event");
+    ctx->timings_pending = true;
+    return SI_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+int si_abi_version(void) { return SI_ABI_VERSION; }
+
+const char* si_status_string(si_status s) {
+    switch (s) {
+        case SI_OK: return "ok";
+        case SI_ERR_INVALID_ARG: return "invalid argument";
+        case SI_ERR_CUDA: return "CUDA error";
+        case SI_ERR_OUT_OF_MEMORY: return "out of device memory";
+        case SI_ERR_UNSUPPORTED: return "unsupported";
+        case SI_ERR_STATE: return "bad call order";
+        case SI_ERR_TIMEOUT: return "timeout";
+        case SI_ERR_BUDGET: return "HBM budget exceeded";
+        case SI_ERR_CANCELLED: return "cancelled";
+    }
+    return "unknown status";
+}
+
+si_status si_ctx_create(int device, uint64_t hbm_budget_bytes, si_ctx** out) {
+    if (!out) return SI_ERR_INVALID_ARG;
+    *out = nullptr;
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) { cudaGetLastError(); return SI_ERR_CUDA; }
+    if (device < 0 || device >= n) return SI_ERR_INVALID_ARG;
+    si_ctx* ctx = new (std::nothrow) si_ctx();
+    if (!ctx) return SI_ERR_OUT_OF_MEMORY;
+    ctx->device = device;
+    if (cudaSetDevice(device) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
+    ctx->budget = hbm_budget_bytes ? hbm_budget_bytes : (uint64_t)free_b;
+    if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
+    for (auto& e : ctx->ev)
+        if (cudaEventCreate(&e) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
+    *out = ctx;
+    return SI_OK;
+}
+
+si_status si_ctx_destroy(si_ctx* ctx) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    cudaSetDevice(ctx->device);
+    if (ctx->stream) cudaStreamSynchronize(ctx->stream);
+    reset_index(ctx);
+    dev_free(ctx, ctx->panel);
+    dev_free(ctx, ctx->trans);
+    dev_free(ctx, ctx->ckpt);
+    dev_free(ctx, ctx->io_geno);
+    dev_free(ctx, ctx->io_dosage);
+    dev_free(ctx, ctx->io_hprob);
+    dev_free(ctx, ctx->io_haps);
+    for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    delete ctx;
+    return SI_OK;
+}
+
+const char* si_last_error(const si_ctx* ctx) { return ctx ? ctx->err.c_str() : "no context"; }
+
+si_status si_ctx_memory(const si_ctx* ctx, uint64_t* used_bytes, uint64_t* budget_bytes) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (used_bytes) *used_bytes = ctx->used;
+    if (budget_bytes) *budget_bytes = ctx->budget;
+    return SI_OK;
+}
+
+si_status si_panel_upload_packed(si_ctx* ctx, const uint32_t* words, uint32_t M, uint32_t N,
+                                 uint32_t words_per_row) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!words || M == 0 || N < 2 || words_per_row < (N + 31) / 32)
+        return fail(ctx, SI_ERR_INVALID_ARG, "bad packed panel arguments (need M >= 1, N >= 2)");
+    SI_TRY(set_device(ctx));
+    reset_index(ctx);
+    const uint32_t W = words_per_row_pad(N);
+    SI_TRY(dev_alloc(ctx, ctx->panel, (size_t)M * W * 4));
+    SI_CUDA(ctx,
+            cudaMemcpy2D(ctx->panel.ptr, (size_t)W * 4, words, (size_t)words_per_row * 4, (size_t)((N + 31) / 32) * 4,
+                         M, cudaMemcpyHostToDevice),
+            "copy packed panel");
+    if (W > (N + 31) / 32)
+        SI_CUDA(ctx,
+                cudaMemset2D((char*)ctx->panel.ptr + (size_t)((N + 31) / 32) * 4, (size_t)W * 4, 0,
+                             (size_t)(W - (N + 31) / 32) * 4, M),
+                "pad panel");
+    // clear bits past N in the last word of every row
+    if (N % 32) {
+        std::vector<uint32_t> last(M);
+        SI_CUDA(ctx,
+                cudaMemcpy2D(last.data(), 4, (char*)ctx->panel.ptr + (size_t)(N / 32) * 4, (size_t)W * 4, 4, M,
+                             cudaMemcpyDeviceToHost),
+                "read last words");
+        const uint32_t keep = (1u << (N % 32)) - 1u;
+        for (auto& v : last) v &= keep;
+        SI_CUDA(ctx,
+                cudaMemcpy2D((char*)ctx->panel.ptr + (size_t)(N / 32) * 4, (size_t)W * 4, last.data(), 4, 4, M,
+                             cudaMemcpyHostToDevice),
+                "write last words");
+    }
+    ctx->M = M; ctx->N = N; ctx->W = W;
+    ctx->has_map = false;
+    ctx->trans_key = ~0ull;
+    return SI_OK;
+}
+
+si_status si_panel_upload_u8(si_ctx* ctx, const uint8_t* alleles, uint32_t M, uint32_t N) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!alleles || M == 0 || N < 2) return fail(ctx, SI_ERR_INVALID_ARG, "bad panel arguments (need M >= 1, N >= 2)");
+    SI_TRY(set_device(ctx));
+    reset_index(ctx);
+    const uint32_t W = words_per_row_pad(N);
+    SI_TRY(dev_alloc(ctx, ctx->panel, (size_t)M * W * 4));
+    SI_CUDA(ctx, cudaMemsetAsync(ctx->panel.ptr, 0, (size_t)M * W * 4, ctx->stream), "memset panel");
+    // stream the u8 panel through a bounded staging buffer
+    const size_t row_bytes = N;
+    const uint32_t rows_per_chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(M, (256u << 20) / row_bytes));
+    DeviceBuffer stage, bad;
+    SI_TRY(dev_alloc(ctx, stage, (size_t)rows_per_chunk * row_bytes));
+    si_status st = dev_alloc(ctx, bad, 4);
+    if (st != SI_OK) { dev_free(ctx, stage); return st; }
+    cudaError_t e = cudaMemsetAsync(bad.ptr, 0, 4, ctx->stream);
+    for (uint32_t m0 = 0; m0 < M && e == cudaSuccess; m0 += rows_per_chunk) {
+        const uint32_t rows = std::min(rows_per_chunk, M - m0);
+        e = cudaMemcpyAsync(stage.ptr, alleles + (size_t)m0 * N, (size_t)rows * N, cudaMemcpyHostToDevice, ctx->stream);
+        if (e == cudaSuccess)
+            e = launch_pack_panel((const uint8_t*)stage.ptr, rows, N, W, (uint32_t*)ctx->panel.ptr + (size_t)m0 * W,
+                                  (uint32_t*)bad.ptr, ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // staging buffer reuse
+    }
+    uint32_t h_bad = 0;
+    if (e == cudaSuccess) e = cudaMemcpy(&h_bad, bad.ptr, 4, cudaMemcpyDeviceToHost);
+    dev_free(ctx, stage);
+    dev_free(ctx, bad);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "panel upload");
+    if (h_bad) {
+        dev_free(ctx, ctx->panel);
+        return fail(ctx, SI_ERR_UNSUPPORTED,
+                    "panel alleles must be 0 or 1 (missing or multi-allelic panel entries are not supported)");
+    }
+    ctx->M = M; ctx->N = N; ctx->W = W;
+    ctx->has_map = false;
+    ctx->trans_key = ~0ull;
+    return SI_OK;
+}
+
+si_status si_panel_set_map(si_ctx* ctx, const uint64_t* pos, const double* cM) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    if (!pos) return fail(ctx, SI_ERR_INVALID_ARG, "pos is NULL");
+    ctx->morgans.resize(ctx->M);
+    for (uint32_t m = 0; m < ctx->M; ++m)
+        ctx->morgans[m] = (cM && cM[m] > 0.0) ? cM[m] / 100.0 : (double)pos[m] / 1e8;
+    ctx->has_map = true;
+    ctx->trans_key = ~0ull;
+    return SI_OK;
+}
+
+si_status si_pbwt_build(si_ctx* ctx, uint32_t flags) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    SI_TRY(set_device(ctx));
+    reset_index(ctx);
+    const uint32_t M = ctx->M, N = ctx->N;
+    SI_TRY(dev_alloc(ctx, ctx->head, (size_t)M * kHead * 4));
+    SI_CUDA(ctx, cudaMemsetAsync(ctx->head.ptr, 0, (size_t)M * kHead * 4, ctx->stream), "memset head");
+    if (flags & SI_PBWT_STORE_INDEX) SI_TRY(dev_alloc(ctx, ctx->prefix, (size_t)M * N * 4));
+    if (flags & SI_PBWT_ROW_HASHES) {
+        SI_TRY(dev_alloc(ctx, ctx->row_hash, (size_t)M * 8));
+        SI_CUDA(ctx, cudaMemsetAsync(ctx->row_hash.ptr, 0, (size_t)M * 8, ctx->stream), "memset hash");
+    }
+    DeviceBuffer perm;
+    SI_TRY(dev_alloc(ctx, perm, (size_t)2 * N * 4));
+    cudaError_t e = cudaEventRecord(ctx->ev[0], ctx->stream);
+    if (e == cudaSuccess)
+        e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, M, N, ctx->W, (uint32_t*)ctx->head.ptr,
+                              (uint32_t*)ctx->prefix.ptr, (unsigned long long*)ctx->row_hash.ptr, (uint32_t*)perm.ptr,
+                              ctx->stream);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ctx->pbwt_ms, ctx->ev[0], ctx->ev[1]);
+    dev_free(ctx, perm);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "PBWT sweep");
+    ctx->has_index = true;
+    ctx->pbwt_flags = flags;
+    return SI_OK;
+}
+
+si_status si_pbwt_get_prefix_rows(si_ctx* ctx, uint32_t m0, uint32_t count, uint32_t* out) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!ctx->has_index || !ctx->prefix.ptr)
+        return fail(ctx, SI_ERR_STATE, "full prefix index not stored (build with SI_PBWT_STORE_INDEX)");
+    if (!out || (uint64_t)m0 + count > ctx->M) return fail(ctx, SI_ERR_INVALID_ARG, "row range out of bounds");
+    SI_TRY(set_device(ctx));
+    SI_CUDA(ctx,
+            cudaMemcpy(out, (uint32_t*)ctx->prefix.ptr + (size_t)m0 * ctx->N, (size_t)count * ctx->N * 4,
+                       cudaMemcpyDeviceToHost),
+            "copy prefix rows");
+    return SI_OK;
+}
+
+si_status si_pbwt_row_hashes(si_ctx* ctx, uint64_t* out) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!ctx->has_index || !ctx->row_hash.ptr)
+        return fail(ctx, SI_ERR_STATE, "row hashes not stored (build with SI_PBWT_ROW_HASHES)");
+    if (!out) return fail(ctx, SI_ERR_INVALID_ARG, "out is NULL");
+    SI_TRY(set_device(ctx));
+    SI_CUDA(ctx, cudaMemcpy(out, ctx->row_hash.ptr, (size_t)ctx->M * 8, cudaMemcpyDeviceToHost), "copy hashes");
+    return SI_OK;
+}
+
+si_status si_pbwt_last_ms(const si_ctx* ctx, float* ms) {
+    if (!ctx || !ms) return SI_ERR_INVALID_ARG;
+    *ms = ctx->pbwt_ms;
+    return SI_OK;
+}
+
+si_status si_select_states(si_ctx* ctx, uint32_t L, int32_t kind, uint32_t m0, uint32_t m1, uint32_t* out_pairs) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!out_pairs || m0 > m1 || m1 > ctx->M) return fail(ctx, SI_ERR_INVALID_ARG, "bad marker range");
+    SI_TRY(set_device(ctx));
+    SelectionCache* c = nullptr;
+    SI_TRY(ensure_selection(ctx, L, kind, &c));
+    SI_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "selection");
+    SI_CUDA(ctx,
+            cudaMemcpy(out_pairs, (uint32_t*)c->pairs.ptr + (size_t)m0 * L * 2, (size_t)(m1 - m0) * L * 2 * 4,
+                       cudaMemcpyDeviceToHost),
+            "copy pairs");
+    return SI_OK;
+}
+
+si_status si_impute_params_default(si_impute_params* p) {
+    if (!p) return SI_ERR_INVALID_ARG;
+    std::memset(p, 0, sizeof *p);
+    p->num_states = 8;         // HMMParameters defaults, core/types.hpp:84-89
+    p->ne = 10000;
+    p->rho_rate = 4.0;
+    p->theta = 0.001;
+    p->transition_mode = SI_TRANS_MATRIX0;
+    p->selection_kind = SI_SEL_AUTO;
+    p->sampling = SI_SAMPLE_ARGMAX;
+    p->tie_eps = 1e-4;
+    p->seed = 12345;           // the reference's fixed cuRAND seed, sampling.cu:302
+    return SI_OK;
+}
+
+si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
+                           float* d_dosage, float* d_hprob, uint8_t* d_haps, void* stream) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    SI_TRY(check_params(ctx, p));
+    if (!d_geno || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "geno is NULL or B == 0");
+    SI_TRY(set_device(ctx));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[0], s), "event");
+    return run_device(ctx, p, d_geno, B, d_dosage, d_hprob, d_haps, s);
+}
+
+si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno, uint32_t B, float* dosage,
+                    float* hap_prob, uint8_t* haps) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    SI_TRY(check_params(ctx, p));
+    if (!geno || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "geno is NULL or B == 0");
+    SI_TRY(set_device(ctx));
+    const uint32_t M = ctx->M;
+    const size_t cells = (size_t)B * M;
+    cudaStream_t s = ctx->stream;
+    cudaEvent_t start;
+    SI_CUDA(ctx, cudaEventCreate(&start), "event");
+    SI_CUDA(ctx, cudaEventRecord(start, s), "event");
+    SI_TRY(dev_reserve(ctx, ctx->io_geno, cells));
+    if (dosage) SI_TRY(dev_reserve(ctx, ctx->io_dosage, cells * 4));
+    if (hap_prob) SI_TRY(dev_reserve(ctx, ctx->io_hprob, cells * 8));
+    if (haps) SI_TRY(dev_reserve(ctx, ctx->io_haps, cells * 2));
+    SI_CUDA(ctx, cudaMemcpyAsync(ctx->io_geno.ptr, geno, cells, cudaMemcpyHostToDevice, s), "copy geno");
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[0], s), "event");
+    SI_TRY(run_device(ctx, p, (const uint8_t*)ctx->io_geno.ptr, B, dosage ? (float*)ctx->io_dosage.ptr : nullptr,
+                      hap_prob ? (float*)ctx->io_hprob.ptr : nullptr, haps ? (uint8_t*)ctx->io_haps.ptr : nullptr, s));
+    if (dosage) SI_CUDA(ctx, cudaMemcpyAsync(dosage, ctx->io_dosage.ptr, cells * 4, cudaMemcpyDeviceToHost, s), "copy dosage");
+    if (hap_prob) SI_CUDA(ctx, cudaMemcpyAsync(hap_prob, ctx->io_hprob.ptr, cells * 8, cudaMemcpyDeviceToHost, s), "copy hprob");
+    if (haps) SI_CUDA(ctx, cudaMemcpyAsync(haps, ctx->io_haps.ptr, cells * 2, cudaMemcpyDeviceToHost, s), "copy haps");
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[3], s), "event");
+    SI_CUDA(ctx, cudaStreamSynchronize(s), "imputation");
+    cudaEventElapsedTime(&ctx->last_ms[0], ctx->ev[0], ctx->ev[1]);
+    cudaEventElapsedTime(&ctx->last_ms[1], ctx->ev[1], ctx->ev[2]);
+    cudaEventElapsedTime(&ctx->last_ms[2], start, ctx->ev[3]);
+    ctx->timings_pending = false;
+    cudaEventDestroy(start);
+    return SI_OK;
+}
+
+si_status si_impute_gl(si_ctx* ctx, const si_impute_params* p, const float* gl, uint32_t B, float* dosage,
+                       float* hap_prob, uint8_t* haps) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!gl || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "gl is NULL or B == 0");
+    const size_t cells = (size_t)B * ctx->M;
+    std::vector<uint8_t> codes(cells);
+    for (size_t i = 0; i < cells; ++i) {
+        const float a = gl[3 * i], b = gl[3 * i + 1], c = gl[3 * i + 2];
+        if (a == b && b == c) codes[i] = SI_GENO_MISSING;
+        else if (a == 0.f && b == -999.f && c == -999.f) codes[i] = 0;
+        else if (a == -999.f && b == 0.f && c == -999.f) codes[i] = 1;
+        else if (a == -999.f && b == -999.f && c == 0.f) codes[i] = 2;
+        else
+            return fail(ctx, SI_ERR_UNSUPPORTED,
+                        "genotype likelihood triple at cell " + std::to_string(i) +
+                            " is not a hard call {0,-999,-999} pattern or missing");
+    }
+    return si_impute(ctx, p, codes.data(), B, dosage, hap_prob, haps);
+}
+
+si_status si_last_timings(si_ctx* ctx, float* ms3) {
+    if (!ctx || !ms3) return SI_ERR_INVALID_ARG;
+    if (ctx->timings_pending) {
+        SI_CUDA(ctx, cudaEventSynchronize(ctx->ev[2]), "wait for kernels");
+        cudaEventElapsedTime(&ctx->last_ms[0], ctx->ev[0], ctx->ev[1]);
+        cudaEventElapsedTime(&ctx->last_ms[1], ctx->ev[1], ctx->ev[2]);
+        ctx->last_ms[2] = 0.f;
+        ctx->timings_pending = false;
+    }
+    for (int i = 0; i < 3; ++i) ms3[i] = ctx->last_ms[i];
+    return SI_OK;
+}
+
+}  // extern "C"

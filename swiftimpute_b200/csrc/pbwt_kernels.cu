@@ -1,0 +1,173 @@
+// pbwt_kernels.cu — panel bit-packing and the PBWT prefix sweep.
+//
+// The reference builds the index on the CPU, one std::vector partition per
+// marker (PBWTBuilder::build_marker, pbwt_index.cpp:153-208), and copies both
+// [M][N] u32 arrays to the device (pbwt_selector.cu:487-513). Here the sweep
+// runs on the device over the bit-packed panel: one CTA carries the whole
+// permutation in shared memory and performs the stable allele partition of
+// each marker as a block-wide exclusive scan of per-thread zero counts.
+#include "si_internal.hpp"
+
+namespace si {
+namespace {
+
+// u8 [M][N] -> bit-packed [M][W]. One warp builds one 32-haplotype word with
+// a ballot, so loads are coalesced bytes. Any value other than 0/1 raises
+// *bad (the bit-packed path stores one bit per allele).
+__global__ void pack_panel_kernel(const uint8_t* __restrict__ u8, uint32_t M, uint32_t N, uint32_t W,
+                                  uint32_t* __restrict__ words, uint32_t* __restrict__ bad) {
+    const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
+    const uint64_t word = gtid >> 5;
+    const uint32_t lane = threadIdx.x & 31;
+    if (word >= (uint64_t)M * W) return;  // whole warps exit together (blockDim multiple of 32)
+    const uint32_t m = (uint32_t)(word / W), w = (uint32_t)(word % W);
+    const uint32_t h = w * 32 + lane;
+    uint8_t v = 0;
+    if (h < N) v = u8[(uint64_t)m * N + h];
+    if (v > 1) atomicOr(bad, 1u);
+    const uint32_t bits = __ballot_sync(0xffffffffu, v != 0);
+    if (lane == 0) words[word] = bits;
+}
+
+__device__ __forceinline__ unsigned long long mix_entry(uint32_t value, uint32_t pos) {
+    unsigned long long x = (unsigned long long)value + (unsigned long long)pos * 0x9E3779B97F4A7C15ull;
+    x ^= x >> 30; x *= 0xBF58476D1CE4E5B9ull;
+    x ^= x >> 27; x *= 0x94D049BB133111EBull;
+    x ^= x >> 31;
+    return x;
+}
+
+constexpr int kSweepThreads = 1024;
+
+// Sequential sweep over all markers in one CTA. Thread t owns the contiguous
+// positions [t*E, t*E + E) of the current order. Per marker:
+//   1. count zeros among the owned haplotypes' bits of the marker row,
+//   2. block-exclusive scan of per-thread zero counts (warp shuffles, one
+//      barrier, every warp rescans the 32 warp totals itself),
+//   3. scatter into the next order: zeros keep their relative order at
+//      [zeros-before), ones at [Z + ones-before) — the stable partition of
+//      pbwt_index.cpp:176-207 — and emit the row's outputs.
+// Two barriers per marker. perm arrays live in shared memory when they fit,
+// otherwise in the global scratch (L2-resident at these sizes).
+template <bool kSmemPerm>
+__global__ void __launch_bounds__(kSweepThreads, 1)
+pbwt_sweep_kernel(const uint32_t* __restrict__ panel, uint32_t M, uint32_t N, uint32_t W, uint32_t E,
+                  uint32_t* __restrict__ head, uint32_t* __restrict__ prefix,
+                  unsigned long long* __restrict__ row_hash, uint32_t* __restrict__ gperm) {
+    extern __shared__ __align__(16) uint32_t smem[];
+    uint32_t* rows = smem;                       // [2][W]
+    uint32_t* wsum = rows + 2 * W;               // [2][32]
+    uint32_t* perm_base = kSmemPerm ? (wsum + 64) : gperm;
+    uint32_t* cur = perm_base;
+    uint32_t* nxt = perm_base + N;
+
+    const uint32_t t = threadIdx.x, lane = t & 31, warp = t >> 5;
+    const uint32_t nwarps = blockDim.x >> 5;
+    const uint32_t beg = t * E;
+
+    for (uint32_t i = t; i < N; i += blockDim.x) cur[i] = i;  // iota, pbwt_index.cpp:226
+    for (uint32_t i = t; i < W; i += blockDim.x) rows[i] = panel[i];
+    __syncthreads();
+
+    for (uint32_t m = 0; m < M; ++m) {
+        const uint32_t* row = rows + (m & 1) * W;
+        // prefetch the next marker's row into the other buffer
+        if (m + 1 < M)
+            for (uint32_t i = t; i < W; i += blockDim.x) rows[((m + 1) & 1) * W + i] = panel[(uint64_t)(m + 1) * W + i];
+
+        uint32_t n_own = 0;
+        if (beg < N) n_own = min(E, N - beg);
+        // pass 1: zero count of the owned entries
+        uint32_t z = 0;
+        for (uint32_t i = 0; i < n_own; ++i) {
+            const uint32_t v = cur[beg + i];
+            z += ((row[v >> 5] >> (v & 31)) & 1u) ^ 1u;
+        }
+
+        // warp inclusive scan of zero counts
+        uint32_t incl = z;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+            if (lane >= (uint32_t)o) incl += y;
+        }
+        uint32_t* ws = wsum + (m & 1) * 32;
+        if (lane == 31) ws[warp] = incl;
+        __syncthreads();
+        // every warp scans the warp totals itself (no second barrier)
+        uint32_t wt = (lane < nwarps) ? ws[lane] : 0u;
+        uint32_t wincl = wt;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, wincl, o);
+            if (lane >= (uint32_t)o) wincl += y;
+        }
+        const uint32_t total_zeros = __shfl_sync(0xffffffffu, wincl, 31);
+        const uint32_t warp_before = __shfl_sync(0xffffffffu, wincl - wt, warp);
+        uint32_t zb = warp_before + incl - z;  // zeros before my first entry
+        uint32_t ob = beg - zb;                // ones before my first entry
+
+        unsigned long long hacc = 0;
+        uint32_t* out_row = prefix ? prefix + (uint64_t)m * N : nullptr;
+        uint32_t* head_row = head + (uint64_t)m * kHead;
+        // pass 2: stable scatter
+        for (uint32_t i = 0; i < n_own; ++i) {
+            const uint32_t v = cur[beg + i];
+            const uint32_t pos = ((row[v >> 5] >> (v & 31)) & 1u) ? (total_zeros + ob++) : zb++;
+            nxt[pos] = v;
+            if (out_row) out_row[pos] = v;
+            if (pos < kHead) head_row[pos] = v;
+            if (row_hash) hacc += mix_entry(v, pos);
+        }
+        if (row_hash) {
+#pragma unroll
+            for (int o = 16; o > 0; o >>= 1) hacc += __shfl_xor_sync(0xffffffffu, hacc, o);
+            if (lane == 0) atomicAdd(row_hash + m, hacc);
+        }
+        __syncthreads();
+        uint32_t* tmp = cur; cur = nxt; nxt = tmp;
+    }
+}
+
+}  // namespace
+
+cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,
+                              uint32_t* d_bad, cudaStream_t s) {
+    const uint64_t threads = (uint64_t)M * W * 32;
+    const uint32_t bs = 256;
+    const uint64_t grid = (threads + bs - 1) / bs;
+    if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
+    pack_panel_kernel<<<(uint32_t)grid, bs, 0, s>>>(d_u8, M, N, W, d_words, d_bad);
+    return cudaGetLastError();
+}
+
+size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W) {
+    return (size_t)(2 * W + 64) * 4 + (size_t)2 * N * 4;
+}
+
+// Single-CTA sweep; head must be zero-filled for rows shorter than kHead.
+cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_head,
+                              uint32_t* d_prefix, unsigned long long* d_hash, uint32_t* d_perm_scratch,
+                              cudaStream_t s) {
+    const uint32_t T = kSweepThreads;
+    const uint32_t E = (N + T - 1) / T;
+    int dev = 0, max_optin = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
+    const size_t full = pbwt_sweep_smem_bytes(N, W);
+    if (full <= (size_t)max_optin) {
+        cudaError_t e = cudaFuncSetAttribute(pbwt_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)full);
+        if (e != cudaSuccess) return e;
+        pbwt_sweep_kernel<true><<<1, T, full, s>>>(d_panel, M, N, W, E, d_head, d_prefix, d_hash, nullptr);
+    } else {
+        const size_t small = (size_t)(2 * W + 64) * 4;
+        cudaError_t e = cudaFuncSetAttribute(pbwt_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                             (int)small);
+        if (e != cudaSuccess) return e;
+        pbwt_sweep_kernel<false><<<1, T, small, s>>>(d_panel, M, N, W, E, d_head, d_prefix, d_hash, d_perm_scratch);
+    }
+    return cudaGetLastError();
+}
+
+}  // namespace si

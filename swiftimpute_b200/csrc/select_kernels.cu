@@ -1,0 +1,56 @@
+// select_kernels.cu — per-marker L-state selection with fused pair expansion.
+//
+// Every divergence entry of the reference index at marker m equals m
+// (pbwt_index.cpp:173-191), so the reference selectors' top-L by divergence
+// reduces to fixed positions of the marker's prefix row, identical for every
+// target sample:
+//   warp kernel (pbwt_selector.cu:212-312, used for L <= 32 and N <= 10000):
+//     slot r = prefix[m][32 r] for r < min(4, ceil(N / 32)), else r % N;
+//   insertion kernels (pbwt_selector.cu:320-394 and, in its defined case,
+//     :47-204): slot r = prefix[m][r] for r < min(N, L), else r % N.
+// Each slot h becomes the pair (h, (h + 1) % N) (imputer.cpp:863-874). The
+// reference computes this per (sample, marker) by scanning whole N-long rows
+// (B * M * N * 8 bytes); here it is one thread per marker reading at most L
+// entries of the head rows the sweep kept.
+#include "si_internal.hpp"
+
+namespace si {
+namespace {
+
+__global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t* __restrict__ panel, uint32_t M,
+                              uint32_t N, uint32_t W, uint32_t L, int kind, uint32_t* __restrict__ pairs,
+                              SlotMasks* __restrict__ masks) {
+    const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
+    if (m >= M) return;
+    const uint32_t* hrow = head + (uint64_t)m * kHead;
+    const uint32_t* prow = panel + (uint64_t)m * W;
+    const uint32_t lane0 = min(4u, (N + 31) / 32);
+    const uint32_t top = min(N, L);
+    uint32_t a0 = 0, a1 = 0;
+    for (uint32_t k = 0; k < L; ++k) {
+        uint32_t h;
+        if (kind == SI_SEL_WARP) h = (k < lane0) ? hrow[32 * k] : (k % N);
+        else h = (k < top) ? hrow[k] : (k % N);
+        const uint32_t h1 = (h + 1) % N;
+        if (pairs) {
+            pairs[((uint64_t)m * L + k) * 2 + 0] = h;
+            pairs[((uint64_t)m * L + k) * 2 + 1] = h1;
+        }
+        if (k < 32) {
+            a0 |= ((prow[h >> 5] >> (h & 31)) & 1u) << k;
+            a1 |= ((prow[h1 >> 5] >> (h1 & 31)) & 1u) << k;
+        }
+    }
+    if (masks) masks[m] = SlotMasks{a0, a1};
+}
+
+}  // namespace
+
+cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
+                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, cudaStream_t s) {
+    const uint32_t bs = 128;
+    select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_pairs, d_masks);
+    return cudaGetLastError();
+}
+
+}  // namespace si

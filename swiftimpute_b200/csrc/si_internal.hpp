@@ -1,0 +1,127 @@
+// si_internal.hpp — device context shared by the C ABI translation units.
+#pragma once
+
+#include "../../include/swiftimpute_b200.h"
+
+#include <cuda_runtime.h>
+
+#include <cstdint>
+#include <map>
+#include <string>
+#include <utility>
+#include <vector>
+
+namespace si {
+
+// Bit-packed panel row: ceil(N / 32) words, padded to a multiple of 4 so every
+// row starts on a 16-byte boundary (128-bit loads, bulk copies).
+inline uint32_t words_per_row_pad(uint32_t N) { return ((N + 31) / 32 + 3) & ~3u; }
+
+// Number of prefix entries kept per marker for selection: the warp pattern
+// reads positions 0, 32, 64, 96 and the insertion pattern positions 0..L-1
+// (L <= 64), so the first 128 entries of each row cover every pattern.
+constexpr uint32_t kHead = 128;
+
+// Per-marker slot data consumed by the forward-backward kernels: for slot k,
+// bit k of a0 / a1 is the panel allele of the pair's first / second haplotype.
+struct SlotMasks {
+    uint32_t a0;
+    uint32_t a1;
+};
+
+// Linear-space transition into a marker: T[i][j] = c + delta * [i == j], with
+// c = exp(log10 switch) and c + delta = exp(log10 stay) as the reference's
+// log10 values are consumed by natural-log recursions.
+struct LinTrans {
+    float c;
+    float delta;
+};
+
+struct DeviceBuffer {
+    void* ptr = nullptr;
+    size_t bytes = 0;
+};
+
+struct SelectionCache {
+    uint32_t L = 0;
+    int kind = 0;
+    DeviceBuffer pairs;  // [M][L][2] u32
+    DeviceBuffer masks;  // [M] SlotMasks
+};
+
+}  // namespace si
+
+struct si_ctx {
+    int device = 0;
+    uint64_t budget = 0;
+    uint64_t used = 0;
+    std::string err;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+
+    // panel
+    uint32_t M = 0, N = 0, W = 0;
+    si::DeviceBuffer panel;          // [M][W] u32 bit-packed
+    std::vector<double> morgans;     // genetic position per marker
+    bool has_map = false;
+
+    // PBWT
+    bool has_index = false;
+    uint32_t pbwt_flags = 0;
+    si::DeviceBuffer head;           // [M][kHead] u32, first entries of each prefix row
+    si::DeviceBuffer prefix;         // [M][N] u32 (SI_PBWT_STORE_INDEX)
+    si::DeviceBuffer row_hash;       // [M] u64 (SI_PBWT_ROW_HASHES)
+    float pbwt_ms = 0.f;
+
+    // selection, keyed by (L, kind)
+    std::map<std::pair<uint32_t, int>, si::SelectionCache> sel;
+
+    // imputation scratch, grown on demand
+    si::DeviceBuffer trans;          // [M] LinTrans
+    uint64_t trans_key = ~0ull;
+    si::DeviceBuffer ckpt;           // forward checkpoints
+    si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
+    float last_ms[3] = {0.f, 0.f, 0.f};
+    bool timings_pending = false;
+};
+
+namespace si {
+
+// Allocation under the ctx's HBM budget.
+si_status dev_alloc(si_ctx* ctx, DeviceBuffer& buf, size_t bytes);
+void dev_free(si_ctx* ctx, DeviceBuffer& buf);
+// Grow-only scratch: keep the buffer if it is already large enough.
+si_status dev_reserve(si_ctx* ctx, DeviceBuffer& buf, size_t bytes);
+si_status fail(si_ctx* ctx, si_status s, const std::string& msg);
+si_status cuda_fail(si_ctx* ctx, cudaError_t e, const char* what);
+
+// Kernel launchers (pbwt_kernels.cu, select_kernels.cu, fb_kernels.cu).
+cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,
+                              uint32_t* d_bad, cudaStream_t s);
+cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_head,
+                              uint32_t* d_prefix, unsigned long long* d_hash, uint32_t* d_perm_scratch,
+                              cudaStream_t s);
+size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W);
+cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
+                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, cudaStream_t s);
+
+struct FbLaunch {
+    const uint8_t* geno;   // [B][M]
+    const SlotMasks* masks;
+    const LinTrans* trans;
+    uint32_t B, M, L, C;
+    uint32_t threads;
+    int sampling;
+    float tie_eps;
+    uint64_t seed, sample_id_base;
+    float* ckpt;           // [B][nseg][Lmax]
+    float* dosage;         // [B][M] or null
+    float* hprob;          // [B][M][2] or null
+    uint8_t* haps;         // [B][2][M] or null
+};
+cudaError_t launch_fb(const FbLaunch& a, cudaStream_t s);
+size_t fb_ckpt_bytes(uint32_t B, uint32_t M, uint32_t L, uint32_t C);
+uint32_t fb_lmax(uint32_t L);
+size_t fb_smem_bytes(uint32_t L, uint32_t T, uint32_t C);
+
+}  // namespace si

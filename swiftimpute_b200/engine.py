@@ -1,0 +1,139 @@
+"""Python handle on a device context (thin layer over the C ABI).
+
+``Engine`` owns one ``si_ctx``: the bit-packed panel, the PBWT index and the
+selection caches stay resident on the device between calls, as the reference
+``Imputer`` keeps its panel copies and index (src/api/imputer.hpp:235-259).
+"""
+from __future__ import annotations
+
+import ctypes
+from ctypes import byref, c_float, c_uint64, c_void_p
+
+import numpy as np
+
+from . import _native as N
+
+
+def _ptr(a: np.ndarray | None):
+    return None if a is None else a.ctypes.data_as(c_void_p)
+
+
+class Engine:
+    def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
+        self.lib = N.load()
+        h = c_void_p()
+        st = self.lib.si_ctx_create(device, hbm_budget_bytes, byref(h))
+        if st != N.SI_OK:
+            raise N.SIError(st, "si_ctx_create failed (is a CUDA device visible?)")
+        self.h = h
+        self.M = self.N = 0
+
+    # -- plumbing -------------------------------------------------------------
+    def _check(self, st: int) -> None:
+        if st != N.SI_OK:
+            raise N.SIError(st, self.lib.si_last_error(self.h).decode())
+
+    def close(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.si_ctx_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):  # pragma: no cover
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def memory(self) -> tuple[int, int]:
+        used, budget = c_uint64(), c_uint64()
+        self._check(self.lib.si_ctx_memory(self.h, byref(used), byref(budget)))
+        return used.value, budget.value
+
+    # -- panel ----------------------------------------------------------------
+    def upload_panel(self, panel: np.ndarray) -> None:
+        panel = np.ascontiguousarray(panel, dtype=np.uint8)
+        M, N_ = panel.shape
+        self._check(self.lib.si_panel_upload_u8(self.h, _ptr(panel), M, N_))
+        self.M, self.N = M, N_
+
+    def upload_packed(self, words: np.ndarray, n_haplotypes: int) -> None:
+        words = np.ascontiguousarray(words, dtype=np.uint32)
+        M, W = words.shape
+        self._check(self.lib.si_panel_upload_packed(self.h, _ptr(words), M, n_haplotypes, W))
+        self.M, self.N = M, n_haplotypes
+
+    def set_map(self, pos: np.ndarray, cM: np.ndarray | None = None) -> None:
+        pos = np.ascontiguousarray(pos, dtype=np.uint64)
+        cm = None if cM is None else np.ascontiguousarray(cM, dtype=np.float64)
+        self._check(self.lib.si_panel_set_map(self.h, _ptr(pos), _ptr(cm)))
+
+    # -- PBWT -------------------------------------------------------------------
+    def pbwt_build(self, store_index: bool = False, row_hashes: bool = False) -> float:
+        flags = (N.PBWT_STORE_INDEX if store_index else 0) | (N.PBWT_ROW_HASHES if row_hashes else 0)
+        self._check(self.lib.si_pbwt_build(self.h, flags))
+        ms = c_float()
+        self._check(self.lib.si_pbwt_last_ms(self.h, byref(ms)))
+        return ms.value
+
+    def prefix_rows(self, m0: int = 0, count: int | None = None) -> np.ndarray:
+        count = self.M - m0 if count is None else count
+        out = np.empty((count, self.N), dtype=np.uint32)
+        self._check(self.lib.si_pbwt_get_prefix_rows(self.h, m0, count, _ptr(out)))
+        return out
+
+    def row_hashes(self) -> np.ndarray:
+        out = np.empty(self.M, dtype=np.uint64)
+        self._check(self.lib.si_pbwt_row_hashes(self.h, _ptr(out)))
+        return out
+
+    # -- selection ----------------------------------------------------------------
+    def select_states(self, L: int, kind: int = N.SEL_AUTO, m0: int = 0, m1: int | None = None) -> np.ndarray:
+        m1 = self.M if m1 is None else m1
+        out = np.empty((m1 - m0, L, 2), dtype=np.uint32)
+        self._check(self.lib.si_select_states(self.h, L, kind, m0, m1, _ptr(out)))
+        return out
+
+    # -- imputation ---------------------------------------------------------------
+    def impute(self, geno: np.ndarray, params: N.ImputeParams | None = None, *, dosage: bool = True,
+               hap_prob: bool = False, haps: bool = True, gl: bool = False):
+        """Impute rows of ``geno`` ([B][M] codes, or [B][M][3] log10 GL when gl=True).
+
+        Returns a dict of numpy arrays: dosage [B][M], hap_prob [B][M][2],
+        haps [B][2][M] (only the requested ones).
+        """
+        params = params or N.default_params()
+        geno = np.ascontiguousarray(geno, dtype=np.float32 if gl else np.uint8)
+        B = geno.shape[0]
+        out = {}
+        d = np.empty((B, self.M), np.float32) if dosage else None
+        hp = np.empty((B, self.M, 2), np.float32) if hap_prob else None
+        hh = np.empty((B, 2, self.M), np.uint8) if haps else None
+        fn = self.lib.si_impute_gl if gl else self.lib.si_impute
+        self._check(fn(self.h, byref(params), _ptr(geno), B, _ptr(d), _ptr(hp), _ptr(hh)))
+        if dosage:
+            out["dosage"] = d
+        if hap_prob:
+            out["hap_prob"] = hp
+        if haps:
+            out["haps"] = hh
+        return out
+
+    def impute_device(self, d_geno: int, B: int, params: N.ImputeParams, d_dosage: int | None,
+                      d_hap_prob: int | None, d_haps: int | None, stream: int | None = None) -> None:
+        """Queue an imputation on device buffers (raw device addresses)."""
+        self._check(self.lib.si_impute_device(self.h, byref(params), c_void_p(d_geno), B,
+                                              c_void_p(d_dosage) if d_dosage else None,
+                                              c_void_p(d_hap_prob) if d_hap_prob else None,
+                                              c_void_p(d_haps) if d_haps else None,
+                                              c_void_p(stream) if stream else None))
+
+    def last_timings(self) -> tuple[float, float, float]:
+        ms = (c_float * 3)()
+        self._check(self.lib.si_last_timings(self.h, ms))
+        return tuple(ms)
