@@ -36,8 +36,11 @@ typedef enum {
 typedef struct si_ctx si_ctx;
 
 /* Selection kinds: which reference kernel's pattern to reproduce. AUTO picks
- * as launch_select_states does (pbwt_selector.cu:413-456). */
-enum { SI_SEL_AUTO = 0, SI_SEL_WARP = 1, SI_SEL_INSERTION = 2 };
+ * as launch_select_states does (pbwt_selector.cu:413-456). FIRST_PAIRS is the
+ * reference Imputer's choice without an index or with PBWT selection off:
+ * slot k = haplotypes (2k, 2k+1) at every marker (imputer.cpp:929-942); it
+ * needs no index and N >= 2L. */
+enum { SI_SEL_AUTO = 0, SI_SEL_WARP = 1, SI_SEL_INSERTION = 2, SI_SEL_FIRST_PAIRS = 3 };
 
 /* Transition modes. MATRIX0 reproduces the reference, whose forward-backward
  * reads the first gap's matrix for every gap (forward_backward.cu:108,201,234,269).

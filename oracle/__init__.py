@@ -22,7 +22,7 @@ ORACLE_SO = HERE / "_build" / "libsi_oracle.so"
 REF_PBWT_SO = HERE / "_ref" / "libref_pbwt.so"
 REF_GPU_SO = HERE / "_ref" / "libref_gpu.so"
 
-SEL_AUTO, SEL_WARP, SEL_INSERTION = 0, 1, 2
+SEL_AUTO, SEL_WARP, SEL_INSERTION, SEL_FIRST_PAIRS = 0, 1, 2, 3
 TRANS_MATRIX0, TRANS_PER_GAP = 0, 1
 
 
@@ -231,3 +231,22 @@ def ref_gpu_impute(panel: np.ndarray, pos: np.ndarray, gl: np.ndarray, L: int, n
     if rc != 0:
         raise RuntimeError(f"reference GPU path returned {rc}")
     return slots, lp, haps, ms
+
+
+def ref_gpu_fb_timing(panel: np.ndarray, pos: np.ndarray, gl: np.ndarray, L: int, ne: int, slots: np.ndarray,
+                      rho_rate: float = 4.0, iters: int = 1) -> np.ndarray:
+    """Stage times (ms: emission, forward+backward, sampling) of the reference's
+    plain log-space kernels on a B200 over the given slot table [M][L]."""
+    Lb = ctypes.CDLL(str(REF_GPU_SO))
+    Lb.ref_gpu_fb_timing.restype = c_int
+    Lb.ref_gpu_fb_timing.argtypes = [c_void_p, c_uint32, c_uint32, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32,
+                                     c_float, c_void_p, c_int, c_void_p]
+    panel = np.ascontiguousarray(panel, dtype=np.uint8)
+    M, N = panel.shape
+    gl = np.ascontiguousarray(gl, dtype=np.float32)
+    ms = np.zeros(3, np.float32)
+    rc = Lb.ref_gpu_fb_timing(_p(panel), M, N, _p(np.ascontiguousarray(pos, dtype=np.uint64)), _p(gl), gl.shape[0],
+                              L, ne, rho_rate, _p(np.ascontiguousarray(slots, dtype=np.uint32)), iters, _p(ms))
+    if rc != 0:
+        raise RuntimeError(f"reference GPU timing returned {rc}")
+    return ms

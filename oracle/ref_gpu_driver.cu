@@ -128,3 +128,72 @@ extern "C" int ref_gpu_impute(const uint8_t* panel, uint32_t M, uint32_t N, cons
         return 2;
     }
 }
+
+// Times the reference's plain per-sample log-space path without its selection
+// kernel: EmissionComputer::compute, launch_forward_pass + launch_backward_pass
+// (C = (uint32)sqrtf(M)) and the deterministic HaplotypeSampler, over B
+// samples that share the given slot table slots [M][L] (expanded to pairs
+// (h, (h+1) % N) and replicated per sample as the reference's layout wants).
+// stage_ms[3]: emission, forward+backward, sampling (last iteration).
+extern "C" int ref_gpu_fb_timing(const uint8_t* panel, uint32_t M, uint32_t N, const uint64_t* pos,
+                                 const float* gl, uint32_t B, uint32_t L, uint32_t ne, float rho_rate,
+                                 const uint32_t* slots, int iters, float* stage_ms) {
+    if (N < 2 || M > 65535 || M < 2 || (uint64_t)M * N >= (1ull << 32) || L == 0 || L > 32 || B == 0) return 1;
+    try {
+        Logger::instance().set_level(Logger::ERROR);
+        const size_t cells = (size_t)B * M;
+        DevBuf d_gl, d_states, d_emis, d_post, d_ckpt, d_scale, d_out;
+        const uint32_t C = std::max(1u, (uint32_t)std::sqrt((float)M));
+        const uint32_t n_ckpt = (M + C - 1) / C;
+        RCK(cudaMalloc(&d_gl.p, cells * sizeof(GenotypeLikelihoods)));
+        RCK(cudaMalloc(&d_states.p, cells * L * 2 * sizeof(uint32_t)));
+        RCK(cudaMalloc(&d_emis.p, cells * L * sizeof(float)));
+        RCK(cudaMalloc(&d_post.p, cells * L * sizeof(float)));
+        RCK(cudaMalloc(&d_ckpt.p, (size_t)B * n_ckpt * L * sizeof(float)));
+        RCK(cudaMalloc(&d_scale.p, cells * sizeof(float)));
+        RCK(cudaMalloc(&d_out.p, cells * 2));
+        RCK(cudaMemcpy(d_gl.p, gl, cells * sizeof(GenotypeLikelihoods), cudaMemcpyHostToDevice));
+        std::vector<uint32_t> one((size_t)M * L * 2);
+        for (size_t c = 0; c < (size_t)M * L; ++c) { one[2 * c] = slots[c]; one[2 * c + 1] = (slots[c] + 1) % N; }
+        for (uint32_t b = 0; b < B; ++b)
+            RCK(cudaMemcpy(d_states.as<uint32_t>() + (size_t)b * M * L * 2, one.data(), one.size() * 4,
+                           cudaMemcpyHostToDevice));
+        kernels::EmissionComputer emis(M, N, L, 0);
+        emis.set_reference_panel(panel);
+        kernels::TransitionComputer trans(M, L, 0);
+        std::vector<double> gd(M);
+        for (uint32_t m = 0; m < M; ++m) gd[m] = (double)pos[m] / 1e8;
+        trans.set_genetic_map(gd.data());
+        kernels::HMMParameters hp;
+        hp.ne = ne;
+        hp.rho_rate = rho_rate;
+        hp.theta = 0.001;
+        trans.set_parameters(hp);
+        trans.compute();
+        kernels::HaplotypeSampler sampler(M, N, L, 0);
+        sampler.set_reference_panel(panel);
+        cudaEvent_t ev[4];
+        for (auto& e : ev) RCK(cudaEventCreate(&e));
+        for (int it = 0; it < (iters < 1 ? 1 : iters); ++it) {
+            RCK(cudaEventRecord(ev[0], 0));
+            emis.compute(d_gl.as<GenotypeLikelihoods>(), d_states.as<uint32_t>(), d_emis.as<float>(), B, true);
+            RCK(cudaEventRecord(ev[1], 0));
+            kernels::launch_forward_pass(d_emis.as<float>(), trans.get_transition_matrices(),
+                                         d_states.as<uint32_t>(), B, M, L, C, d_ckpt.as<float>(),
+                                         d_scale.as<float>(), 0);
+            kernels::launch_backward_pass(d_emis.as<float>(), trans.get_transition_matrices(),
+                                          d_states.as<uint32_t>(), d_ckpt.as<float>(), d_scale.as<float>(),
+                                          B, M, L, C, d_post.as<float>(), 0);
+            RCK(cudaEventRecord(ev[2], 0));
+            sampler.sample(d_post.as<float>(), d_states.as<uint32_t>(), d_out.as<uint8_t>(), B, true);
+            RCK(cudaEventRecord(ev[3], 0));
+            RCK(cudaDeviceSynchronize());
+        }
+        if (stage_ms)
+            for (int s = 0; s < 3; ++s) RCK(cudaEventElapsedTime(&stage_ms[s], ev[s], ev[s + 1]));
+        for (auto& e : ev) cudaEventDestroy(e);
+        return 0;
+    } catch (...) {
+        return 2;
+    }
+}

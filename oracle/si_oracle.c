@@ -108,7 +108,10 @@ int sio_select_kind(uint32_t N, uint32_t L) {
  *    strict '>' keeps the first L entries in scan order, rest i % N. */
 void sio_select_row(const uint32_t* prefix_row, uint32_t N, uint32_t L, int kind, uint32_t* slots) {
     if (kind == SIO_SEL_AUTO) kind = sio_select_kind(N, L);
-    if (kind == SIO_SEL_WARP) {
+    if (kind == SIO_SEL_FIRST_PAIRS) {
+        /* Imputer without an index: pairs (2k, 2k+1) (imputer.cpp:929-942) */
+        for (uint32_t i = 0; i < L; ++i) slots[i] = 2 * i;
+    } else if (kind == SIO_SEL_WARP) {
         uint32_t lane0 = (N + 31) / 32;
         if (lane0 > 4) lane0 = 4;
         for (uint32_t i = 0; i < L; ++i)

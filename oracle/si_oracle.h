@@ -22,7 +22,7 @@ extern "C" {
 
 /* Selection patterns the reference kernels produce when every divergence at a
  * marker ties (pbwt_index.cpp:173-191 makes every divergence equal m). */
-enum { SIO_SEL_AUTO = 0, SIO_SEL_WARP = 1, SIO_SEL_INSERTION = 2 };
+enum { SIO_SEL_AUTO = 0, SIO_SEL_WARP = 1, SIO_SEL_INSERTION = 2, SIO_SEL_FIRST_PAIRS = 3 };
 
 /* Transition modes: the reference reads matrix 0 for every gap
  * (forward_backward.cu:108,201,234,269); PER_GAP uses each gap's own matrix. */

@@ -18,7 +18,7 @@ STATUS_NAMES = {
     4: "SI_ERR_UNSUPPORTED", 5: "SI_ERR_STATE", 6: "SI_ERR_TIMEOUT", 7: "SI_ERR_BUDGET",
     8: "SI_ERR_CANCELLED",
 }
-SEL_AUTO, SEL_WARP, SEL_INSERTION = 0, 1, 2
+SEL_AUTO, SEL_WARP, SEL_INSERTION, SEL_FIRST_PAIRS = 0, 1, 2, 3
 TRANS_MATRIX0, TRANS_PER_GAP = 0, 1
 SAMPLE_ARGMAX, SAMPLE_PHILOX = 0, 1
 PBWT_STORE_INDEX, PBWT_ROW_HASHES = 1, 2

@@ -52,8 +52,9 @@ def build(verbose: bool = False, force: bool = False) -> Path:
         if src.suffix == ".cu":
             cmd = [NVCC, *CUFLAGS, "-I", str(PKG.parent / "include"), "-c", str(src), "-o", str(obj)]
         else:
-            cmd = [NVCC, "-x", "c++", "-Xcompiler", ",".join(CXXFLAGS), "-std=c++17",
-                   "-I", str(PKG.parent / "include"), "-c", str(src), "-o", str(obj)]
+            cmd = [os.environ.get("CXX", "g++"), *CXXFLAGS, "-I", str(PKG.parent / "include"),
+                   "-I", str(Path(os.environ.get("CUDA_HOME", "/usr/local/cuda")) / "include"),
+                   "-c", str(src), "-o", str(obj)]
         if verbose:
             print(" ".join(cmd))
         _run(cmd)

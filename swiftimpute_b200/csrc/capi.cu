@@ -134,10 +134,16 @@ si_status ensure_trans(si_ctx* ctx, const si_impute_params* p) {
 
 si_status ensure_selection(si_ctx* ctx, uint32_t L, int kind, SelectionCache** out, bool force = false,
                            cudaStream_t s = nullptr) {
-    if (!ctx->has_index) return fail(ctx, SI_ERR_STATE, "PBWT index not built (si_pbwt_build)");
     if (L == 0 || L > kHead) return fail(ctx, SI_ERR_INVALID_ARG, "L must be in 1..128");
-    if (kind == SI_SEL_AUTO) kind = (L <= 32 && ctx->N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
-    if (kind != SI_SEL_WARP && kind != SI_SEL_INSERTION) return fail(ctx, SI_ERR_INVALID_ARG, "bad selection kind");
+    if (kind == SI_SEL_FIRST_PAIRS) {
+        if ((uint64_t)2 * L > ctx->N)
+            return fail(ctx, SI_ERR_UNSUPPORTED, "first-pairs selection needs N >= 2L haplotypes");
+    } else {
+        if (!ctx->has_index) return fail(ctx, SI_ERR_STATE, "PBWT index not built (si_pbwt_build)");
+        if (kind == SI_SEL_AUTO) kind = (L <= 32 && ctx->N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+        if (kind != SI_SEL_WARP && kind != SI_SEL_INSERTION)
+            return fail(ctx, SI_ERR_INVALID_ARG, "bad selection kind");
+    }
     auto& c = ctx->sel[{L, kind}];
     if (!c.pairs.ptr || force) {
         c.L = L;

@@ -13,7 +13,8 @@
 //              The e^-999 term is the LOG_ZERO seed of every logsumexp2
 //              chain; beta is never rescaled in the reference, so the term
 //              matters once beta decays near e^-999. beta's absolute scale is
-//              therefore tracked exactly as 2^Kb * e^(-999 nb).
+//              therefore tracked exactly as 2^Kb * e^(-999 nb); when the floor
+//              dominates the unit switches to e^-999 itself.
 //   posterior  P_m(k) = softmax(log alpha + log beta)       sampling.cu:80-100
 // FP32 values, exact power-of-two rescaling every marker (no rounding from
 // the rescale), the floor term computed from the integer scale in FP64.
@@ -180,16 +181,31 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
                 float sw = 0.f;
 #pragma unroll
                 for (int k = 0; k < LM; ++k) { w[k] = ((em_next >> k) & 1u) ? be[k] : 0.0f; sw += w[k]; }
-                const int e = exp2_of(sw);
-                const float sc = pow2_neg(e);
-                nb += (int)sh_next;
-                Kb += e;
-                const double farg = 999.0 * (double)(nb - 1) - (double)Kb * 0.69314718055994530942;
-                const float F = farg > -104.0 ? expf((float)fmin(farg, 80.0)) : 0.0f;
-                const float base = fmaf(tr_next.c, sw * sc, F);
-                const float dl = tr_next.delta * sc;
+                // beta_m = e^-999 + U * (c sw + delta w), U = 2^Kb e^(-999 (nb + sh)): the
+                // floor in units of U is exp(farg)
+                const double farg = 999.0 * (double)(nb + (int)sh_next - 1) - (double)Kb * 0.69314718055994530942;
+                if (farg > 0.0) {
+                    // the floor dominates: switch the unit to e^-999 (Kb = 0, nb = 1),
+                    // beta_m = e^-999 (1 + exp(-farg) (c sw + delta w))
+                    const float g = expf(-(float)fmin(farg, 100.0));
+                    const float cs = tr_next.c * sw;
 #pragma unroll
-                for (int k = 0; k < LM; ++k) be[k] = ((lmask >> k) & 1u) ? fmaf(dl, w[k], base) : 0.0f;
+                    for (int k = 0; k < LM; ++k)
+                        be[k] = ((lmask >> k) & 1u) ? fmaf(g, fmaf(tr_next.delta, w[k], cs), 1.0f) : 0.0f;
+                    Kb = 0;
+                    nb = 1;
+                } else {
+                    const float F = farg > -104.0 ? expf((float)farg) : 0.0f;
+                    const float base = fmaf(tr_next.c, sw, F);  // common part of every slot, >= c
+                    const int e = exp2_of(base);
+                    const float sc = pow2_neg(e);
+                    const float b2 = base * sc;
+                    const float dl = tr_next.delta * sc;
+#pragma unroll
+                    for (int k = 0; k < LM; ++k) be[k] = ((lmask >> k) & 1u) ? fmaf(dl, w[k], b2) : 0.0f;
+                    Kb += e;
+                    nb += (int)sh_next;
+                }
             }
             // posterior at m
             const SlotMasks mk = mseg[i];

@@ -22,7 +22,7 @@ __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t*
                               SlotMasks* __restrict__ masks) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    const uint32_t* hrow = head + (uint64_t)m * kHead;
+    const uint32_t* hrow = head ? head + (uint64_t)m * kHead : nullptr;
     const uint32_t* prow = panel + (uint64_t)m * W;
     const uint32_t lane0 = min(4u, (N + 31) / 32);
     const uint32_t top = min(N, L);
@@ -30,6 +30,7 @@ __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t*
     for (uint32_t k = 0; k < L; ++k) {
         uint32_t h;
         if (kind == SI_SEL_WARP) h = (k < lane0) ? hrow[32 * k] : (k % N);
+        else if (kind == SI_SEL_FIRST_PAIRS) h = 2 * k;  // imputer.cpp:938-939, host checks N >= 2L
         else h = (k < top) ? hrow[k] : (k % N);
         const uint32_t h1 = (h + 1) % N;
         if (pairs) {

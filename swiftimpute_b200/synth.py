@@ -147,3 +147,12 @@ def pack_panel(panel: np.ndarray) -> np.ndarray:
     bits = np.packbits(padded.reshape(M, W, 4, 8)[:, :, :, ::-1], axis=-1).reshape(M, W, 4)
     return (bits[..., 0].astype(np.uint32) | (bits[..., 1].astype(np.uint32) << 8)
             | (bits[..., 2].astype(np.uint32) << 16) | (bits[..., 3].astype(np.uint32) << 24))
+
+
+def unpack_panel(words: np.ndarray, N: int) -> np.ndarray:
+    """Inverse of pack_panel: u32 [M][W] -> u8 [M][N]."""
+    words = np.ascontiguousarray(words, dtype=np.uint32)
+    M, W = words.shape
+    b = words.view(np.uint8).reshape(M, W, 4)
+    bits = np.unpackbits(b, axis=-1, bitorder="little").reshape(M, W * 32)
+    return bits[:, :N].astype(np.uint8)

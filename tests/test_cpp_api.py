@@ -1,0 +1,99 @@
+"""The reference-shaped C++ API (include/swiftimpute/imputer.hpp), driven by a
+compiled C++ caller (tests/cpp/api_tool.cpp)."""
+import subprocess
+from pathlib import Path
+
+import numpy as np
+import pytest
+
+import oracle
+from swiftimpute_b200 import synth
+from swiftimpute_b200._native import LIB_PATH
+from vcfutil import write_panel_vcf, write_target_vcf
+
+ROOT = Path(__file__).resolve().parent.parent
+
+
+@pytest.fixture(scope="module")
+def api_tool(tmp_path_factory):
+    exe = tmp_path_factory.mktemp("bin") / "api_tool"
+    subprocess.run(["g++", "-O2", "-std=c++17", "-I", str(ROOT / "include"), str(ROOT / "tests/cpp/api_tool.cpp"),
+                    "-L", str(LIB_PATH.parent), "-lswiftimpute_b200", f"-Wl,-rpath,{LIB_PATH.parent}", "-o", str(exe)],
+                   check=True)
+    return exe
+
+
+@pytest.fixture(scope="module")
+def vcfs(tmp_path_factory):
+    d = tmp_path_factory.mktemp("vcf")
+    panel, pos, _ = synth.make_panel(180, 300, 10, seed=31, spacing=150)
+    typed = synth.typed_every(180, 4)
+    codes, _, _ = synth.make_targets(panel, 17, typed, seed=32)
+    write_panel_vcf(d / "ref.vcf", panel, pos)
+    write_target_vcf(d / "tgt.vcf", codes, pos)
+    return d, panel, pos, codes
+
+
+def test_vcf_parse_binary_roundtrip_and_writer(api_tool, vcfs):
+    d, panel, pos, codes = vcfs
+    r = subprocess.run([str(api_tool), "parse", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "p")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "roundtrip=1" in r.stdout
+    got_panel = np.fromfile(d / "p.panel", np.uint8).reshape(panel.shape)
+    assert np.array_equal(got_panel, panel)
+    gl = np.fromfile(d / "p.gl", np.float32).reshape(codes.shape + (3,))
+    assert np.array_equal(gl, oracle.codes_to_gl(codes))  # hard calls -> {0,-999,-999}, missing -> {0,0,0}
+    lines = (d / "p.out.vcf").read_text().splitlines()
+    assert lines[:3] == ["##fileformat=VCFv4.2", "##source=SwiftImpute", "##contig=<ID=chr1>"]
+    assert lines[8].startswith("#CHROM\tPOS\tID\tREF\tALT\tQUAL\tFILTER\tINFO\tFORMAT\tTARGET1")
+    row = lines[9].split("\t")
+    assert row[:9] == ["chr1", str(int(pos[0])), "rs1", "A", "G", ".", "PASS", "IMP", "GT"]
+    assert row[9] == f"{panel[0, 0]}|{panel[0, 1]}"
+    assert len(lines) == 9 + panel.shape[0]
+
+
+def test_imputer_without_device_raises_cuda_error(api_tool, vcfs):
+    import ctypes
+    from swiftimpute_b200 import _native as N
+    n = ctypes.c_int(0)
+    try:
+        has_gpu = ctypes.CDLL("libcudart.so").cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0
+    except OSError:
+        has_gpu = False
+    if has_gpu:
+        pytest.skip("a device is visible")
+    d, *_ = vcfs
+    r = subprocess.run([str(api_tool), "impute", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "o.vcf"),
+                        str(d / "o"), "1", "8", "10000"], capture_output=True, text=True)
+    assert r.returncode == 10 and "CUDAError" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("deterministic,posteriors", [(1, 0), (0, 1)])
+def test_imputer_end_to_end(api_tool, vcfs, deterministic, posteriors):
+    d, panel, pos, codes = vcfs
+    r = subprocess.run([str(api_tool), "impute", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "o.vcf"),
+                        str(d / "o"), str(deterministic), "8", "10000", str(posteriors)],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "progress_calls=3" in r.stdout  # 17 samples in chunks of 7
+    B, M = codes.shape
+    pairs = oracle.select_pairs(oracle.pbwt_build(panel), 8)
+    want = oracle.fb_batch(codes, pairs, panel, pos, 8, 10000.0, sampled=not deterministic)
+    ds = np.fromfile(d / "o.dosage", np.float32).reshape(B, M)
+    assert np.abs(ds - want["dosage"]).max() <= 1e-4
+    haps = np.fromfile(d / "o.haps", np.uint8).reshape(B, 2, M)
+    if deterministic:
+        assert np.array_equal(haps, want["haps_argmax"])
+    else:
+        assert np.mean(haps != want["haps_sampled"]) <= 1e-3
+    hard = np.fromfile(d / "o.hard", np.float32).reshape(B, M)
+    assert np.array_equal(hard, haps[:, 0] + haps[:, 1])  # get_dosage keeps the reference meaning
+    gp = np.fromfile(d / "o.gp", np.float32).reshape(B, M, 3)
+    p = want["hap_prob"]
+    assert np.abs(gp[..., 2] - p[..., 0] * p[..., 1]).max() <= 2e-4
+    lines = (d / "o.vcf").read_text().splitlines()
+    fmt = lines[9].split("\t")[8]
+    assert fmt == ("GT:DS:GP" if posteriors else "GT")
+    assert len(lines) == 9 + M

@@ -1,0 +1,69 @@
+"""The device kernel's reformulation, emulated in float64 on the CPU: linear
+space, rank-1-plus-diagonal transition, per-marker rescaling, and beta's
+absolute scale carried so the reference's e^-999 logsumexp seed (the floor)
+is reproduced, switching units to e^-999 when the floor dominates. It must
+equal the FP64 log-space oracle (a restatement of the reference's own
+recurrences) to round-off, including deep in the floor regime."""
+import math
+
+import numpy as np
+import pytest
+
+import oracle
+from swiftimpute_b200 import synth
+
+
+def emulate(codes, pairs, panel, pos, L, ne):
+    M = codes.shape[0]
+    td, to = oracle.transitions(pos, ne)
+    c = math.exp(float(to[0])); d = math.exp(float(td[0])); dl = d - c
+    a0 = panel[np.arange(M)[:, None], pairs[:, :, 0]].astype(int)
+    a1 = panel[np.arange(M)[:, None], pairs[:, :, 1]].astype(int)
+
+    def em(m):
+        g = int(codes[m])
+        if g >= 3:
+            return np.ones(L), 0
+        e = ((a0[m] + a1[m]) == g).astype(float)
+        return (np.ones(L), 1) if e.sum() == 0 else (e, 0)
+
+    al = np.zeros((M, L))
+    al[0] = em(0)[0]
+    for m in range(1, M):
+        e, _ = em(m)
+        v = e * (c * al[m - 1].sum() + dl * al[m - 1])
+        al[m] = v / v.sum()
+    be, logs = np.ones(L), 0.0
+    post = np.zeros((M, L))
+    post[M - 1] = al[M - 1]
+    for m in range(M - 2, -1, -1):
+        e, sh = em(m + 1)
+        w = e * be
+        u = c * w.sum() + dl * w
+        logs_u = logs - 999.0 * sh
+        farg = -999.0 - logs_u
+        if farg > 0:
+            v, logs_new = 1.0 + math.exp(-farg) * u, -999.0
+        else:
+            v, logs_new = (math.exp(farg) if farg > -700 else 0.0) + u, logs_u
+        s = v.sum()
+        be, logs = v / s, logs_new + math.log(s)
+        post[m] = al[m] * be
+    return post / post.sum(1, keepdims=True)
+
+
+@pytest.mark.parametrize("spacing,every,M", [(100, 5, 900), (500_000, 5, 400), (30, 50, 1200), (100, 2, 600)])
+def test_scaled_recursion_equals_log_space_oracle(spacing, every, M):
+    panel, pos, _ = synth.make_panel(M, 300, 12, seed=M + every, spacing=spacing)
+    codes, _, _ = synth.make_targets(panel, 2, synth.typed_every(M, every), seed=3)
+    pairs = oracle.select_pairs(oracle.pbwt_build(panel), 8)
+    gl = oracle.codes_to_gl(codes)
+    deep = False
+    for b in range(2):
+        lp = oracle.fb_logpost(gl[b], pairs, panel, pos, 8, 10000.0)
+        P = np.exp(lp - lp.max(1, keepdims=True)); P /= P.sum(1, keepdims=True)
+        Q = emulate(codes[b], pairs, panel, pos, 8, 10000.0)
+        assert np.abs(P - Q).max() < 1e-9
+        deep |= bool(lp.min() < -1500)
+    if spacing == 100 and every == 5:
+        assert deep  # the case reaches the floor regime with unmatched calls on top
