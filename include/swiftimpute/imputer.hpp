@@ -71,6 +71,46 @@ struct HMMParameters {
     bool use_pbwt_selection = true;
 };
 
+// Logger and device queries (core/types.hpp:253-317), used by the reference's CLI.
+class Logger {
+public:
+    enum Level { DEBUG = 0, INFO = 1, WARNING = 2, ERROR = 3 };
+    static Logger& instance();
+    void set_level(Level level) { level_ = level; }
+    Level get_level() const { return level_; }
+    void debug(const std::string& msg);
+    void info(const std::string& msg);
+    void warning(const std::string& msg);
+    void error(const std::string& msg);
+
+private:
+    Logger() = default;
+    Level level_ = INFO;
+    void log(Level level, const std::string& prefix, const std::string& msg);
+};
+
+#define LOG_DEBUG(msg) ::swiftimpute::Logger::instance().debug(msg)
+#define LOG_INFO(msg) ::swiftimpute::Logger::instance().info(msg)
+#define LOG_WARNING(msg) ::swiftimpute::Logger::instance().warning(msg)
+#define LOG_ERROR(msg) ::swiftimpute::Logger::instance().error(msg)
+
+struct DeviceInfo {
+    int device_id = -1;
+    std::string name;
+    size_t total_memory = 0;
+    size_t free_memory = 0;
+    int compute_capability_major = 0;
+    int compute_capability_minor = 0;
+    int multiprocessor_count = 0;
+    int max_threads_per_block = 0;
+    int max_threads_per_multiprocessor = 0;
+};
+
+DeviceInfo get_device_info(int device_id = 0);
+int select_best_device();
+size_t get_available_gpu_memory(int device_id = 0);
+size_t get_total_gpu_memory(int device_id = 0);
+
 class ImputationError : public std::runtime_error {
 public:
     explicit ImputationError(const std::string& msg) : std::runtime_error(msg) {}
@@ -107,6 +147,7 @@ struct ImputationConfig {
     double tie_eps = 1e-4;            // argmax tolerance
     uint64_t hbm_budget_bytes = 0;    // 0 = all free device memory
     bool write_posteriors = false;    // write_vcf emits GT:DS:GP instead of the reference's GT only
+    uint32_t max_samples_per_call = 0; // 0 = as many samples per device pass as the budget allows
 };
 
 class ReferencePanel {

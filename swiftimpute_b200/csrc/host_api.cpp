@@ -12,6 +12,8 @@
 #include <cstring>
 #include <fstream>
 #include <iomanip>
+#include <iostream>
+#include <mutex>
 #include <sstream>
 
 namespace swiftimpute {
@@ -157,6 +159,82 @@ std::string fmt4(double x) {
 }
 
 }  // namespace
+
+// ---------------------------------------------------------------- Logger, devices
+
+Logger& Logger::instance() {
+    static Logger logger;
+    return logger;
+}
+
+void Logger::log(Level level, const std::string& prefix, const std::string& msg) {
+    if (level < level_) return;
+    static std::mutex mu;
+    std::lock_guard<std::mutex> lock(mu);
+    std::cout << prefix << msg << std::endl;
+}
+void Logger::debug(const std::string& msg) { log(DEBUG, "[DEBUG] ", msg); }
+void Logger::info(const std::string& msg) { log(INFO, "[INFO] ", msg); }
+void Logger::warning(const std::string& msg) { log(WARNING, "[WARNING] ", msg); }
+void Logger::error(const std::string& msg) { log(ERROR, "[ERROR] ", msg); }
+
+DeviceInfo get_device_info(int device_id) {
+    DeviceInfo info;
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device_id) != cudaSuccess) {
+        cudaGetLastError();
+        throw CUDAError("cudaGetDeviceProperties", 100);
+    }
+    info.device_id = device_id;
+    info.name = prop.name;
+    info.total_memory = prop.totalGlobalMem;
+    info.compute_capability_major = prop.major;
+    info.compute_capability_minor = prop.minor;
+    info.multiprocessor_count = prop.multiProcessorCount;
+    info.max_threads_per_block = prop.maxThreadsPerBlock;
+    info.max_threads_per_multiprocessor = prop.maxThreadsPerMultiProcessor;
+    int cur = 0;
+    cudaGetDevice(&cur);
+    if (cudaSetDevice(device_id) == cudaSuccess) {
+        size_t f = 0, t = 0;
+        if (cudaMemGetInfo(&f, &t) == cudaSuccess) info.free_memory = f;
+        cudaSetDevice(cur);
+    }
+    return info;
+}
+
+int select_best_device() {  // most free memory (types.cpp:69-90)
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) {
+        cudaGetLastError();
+        throw CUDAError("no CUDA device", 100);
+    }
+    int best = 0;
+    size_t best_free = 0;
+    for (int d = 0; d < n; ++d) {
+        const size_t f = get_available_gpu_memory(d);
+        if (f > best_free) { best_free = f; best = d; }
+    }
+    return best;
+}
+
+size_t get_available_gpu_memory(int device_id) {
+    int cur = 0;
+    cudaGetDevice(&cur);
+    size_t f = 0, t = 0;
+    if (cudaSetDevice(device_id) == cudaSuccess && cudaMemGetInfo(&f, &t) == cudaSuccess) {
+        cudaSetDevice(cur);
+        return f;
+    }
+    cudaGetLastError();
+    return 0;
+}
+
+size_t get_total_gpu_memory(int device_id) {
+    cudaDeviceProp prop;
+    if (cudaGetDeviceProperties(&prop, device_id) != cudaSuccess) { cudaGetLastError(); return 0; }
+    return prop.totalGlobalMem;
+}
 
 // ---------------------------------------------------------------- ReferencePanel
 
@@ -440,18 +518,7 @@ Imputer::Imputer(const ReferencePanel& reference, const ImputationConfig& config
         cudaGetLastError();
         throw CUDAError("no CUDA device", 100);
     }
-    device_id_ = config_.device_id;
-    if (device_id_ < 0) {  // most free memory, as select_best_device (types.cpp:69-90)
-        size_t best = 0;
-        device_id_ = 0;
-        for (int d = 0; d < n; ++d) {
-            size_t f = 0, t = 0;
-            if (cudaSetDevice(d) == cudaSuccess && cudaMemGetInfo(&f, &t) == cudaSuccess && f > best) {
-                best = f;
-                device_id_ = d;
-            }
-        }
-    }
+    device_id_ = config_.device_id < 0 ? select_best_device() : config_.device_id;
     check(si_ctx_create(device_id_, config_.hbm_budget_bytes, &ctx_), "si_ctx_create");
 }
 
@@ -521,6 +588,7 @@ std::unique_ptr<ImputationResult> Imputer::impute_with_progress(
     const uint64_t room = budget > used ? (budget - used) / 2 : 0;
     uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(B, room / per_sample));
     chunk = std::max<uint32_t>(std::min<uint32_t>(chunk, B), std::min<uint32_t>(B, config_.batch_size));
+    if (config_.max_samples_per_call) chunk = std::min<uint32_t>(chunk, config_.max_samples_per_call);
     for (uint32_t s0 = 0; s0 < B; s0 += chunk) {
         const uint32_t n = std::min(chunk, B - s0);
         p.sample_id_base = s0;

@@ -58,11 +58,15 @@ int main(int argc, char** argv) {
             cfg.hmm_params.num_states = (uint32_t)std::atoi(argv[7]);
             cfg.hmm_params.ne = (uint32_t)std::atoi(argv[8]);
             cfg.write_posteriors = argc > 9 && std::atoi(argv[9]) != 0;
-            cfg.batch_size = 7;  // several chunks: results must not depend on it
+            cfg.max_samples_per_call = 7;  // three device passes: results must not depend on it
             Imputer imp(*ref, cfg);
             imp.build_index();
-            uint32_t calls = 0;
-            auto res = imp.impute_with_progress(*tgt, [&](uint32_t done, uint32_t total) { ++calls; });
+            uint32_t calls = 0, last_done = 0, last_total = 0;
+            auto res = imp.impute_with_progress(*tgt, [&](uint32_t done, uint32_t total) {
+                ++calls;
+                last_done = done;
+                last_total = total;
+            });
             res->write_vcf(argv[4], *tgt, *ref, cfg);
             const std::string pre = argv[5];
             const size_t n = (size_t)res->num_samples() * res->num_markers();
@@ -77,8 +81,8 @@ int main(int argc, char** argv) {
             dump(pre + ".dosage", ds.data(), n * 4);
             dump(pre + ".hard", dsh.data(), n * 4);
             dump(pre + ".gp", gp.data(), 3 * n * 4);
-            std::printf("impute ok: B=%u M=%u progress_calls=%u device_bytes=%zu\n", res->num_samples(),
-                        res->num_markers(), calls, imp.device_memory_usage());
+            std::printf("impute ok: B=%u M=%u progress_calls=%u last=%u/%u device_bytes=%zu\n", res->num_samples(),
+                        res->num_markers(), calls, last_done, last_total, imp.device_memory_usage());
             return 0;
         }
     } catch (const CUDAError& e) {

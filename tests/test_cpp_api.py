@@ -77,8 +77,8 @@ def test_imputer_end_to_end(api_tool, vcfs, deterministic, posteriors):
                         str(d / "o"), str(deterministic), "8", "10000", str(posteriors)],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "progress_calls=3" in r.stdout  # 17 samples in chunks of 7
     B, M = codes.shape
+    assert f"progress_calls=3 last={B}/{B}" in r.stdout  # 17 samples in passes of 7
     pairs = oracle.select_pairs(oracle.pbwt_build(panel), 8)
     want = oracle.fb_batch(codes, pairs, panel, pos, 8, 10000.0, sampled=not deterministic)
     ds = np.fromfile(d / "o.dosage", np.float32).reshape(B, M)
@@ -97,3 +97,21 @@ def test_imputer_end_to_end(api_tool, vcfs, deterministic, posteriors):
     fmt = lines[9].split("\t")[8]
     assert fmt == ("GT:DS:GP" if posteriors else "GT")
     assert len(lines) == 9 + M
+
+
+REF_MAIN = Path("/root/reference/src/main.cpp")
+
+
+@pytest.mark.skipif(not REF_MAIN.exists(), reason="reference source tree not present")
+def test_reference_cli_compiles_unchanged(tmp_path):
+    """The reference's own CLI (src/main.cpp), fed to the compiler as-is, builds
+    against include/ (api/imputer.hpp, core/types.hpp forwarders) and links
+    this library: the C++ API is a drop-in."""
+    exe = tmp_path / "swiftimpute_cli"
+    with open(REF_MAIN) as src:
+        r = subprocess.run(["g++", "-std=c++17", "-x", "c++", "-I", str(ROOT / "include"), "-",
+                            "-L", str(LIB_PATH.parent), "-lswiftimpute_b200", f"-Wl,-rpath,{LIB_PATH.parent}",
+                            "-o", str(exe)], stdin=src, cwd=tmp_path, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr[-2000:]
+    out = subprocess.run([str(exe), "--help"], capture_output=True, text=True)
+    assert "Usage" in out.stdout
