@@ -60,7 +60,8 @@ enum {
 
 /* si_impute_params.flags */
 enum {
-    SI_IMPUTE_RESELECT = 1u  /* recompute the per-marker selection tables in this call (else cached per L) */
+    SI_IMPUTE_RESELECT = 1u,   /* recompute the per-marker selection tables in this call (else cached per L) */
+    SI_IMPUTE_FULL_CHAIN = 2u  /* use the marker-by-marker kernel even where the typed-marker kernel applies */
 };
 
 /* Genotype codes for si_impute: 0, 1, 2 = ALT allele count of a hard call,
@@ -79,8 +80,9 @@ typedef struct {
     double tie_eps;               /* argmax picks the first slot with p >= (1 - tie_eps) * max p */
     uint64_t seed;                /* Philox key */
     uint64_t sample_id_base;      /* Philox counter: sample id of row 0 */
-    uint32_t checkpoint_interval; /* markers per forward checkpoint; 0 = autotuned */
-    uint32_t block_threads;       /* chains per CTA; 0 = autotuned */
+    uint32_t checkpoint_interval; /* full-chain kernel: markers per checkpoint segment; typed-marker
+                                     kernel: typed markers per posterior window; 0 = default */
+    uint32_t block_threads;       /* threads per CTA; 0 = default */
     uint64_t reserved[4];
 } si_impute_params;
 
@@ -167,8 +169,10 @@ si_status si_impute_gl(si_ctx* ctx, const si_impute_params* p, const float* gl, 
                        float* dosage, float* hap_prob, uint8_t* haps);
 
 /* Device-pointer variant: all buffers are device memory owned by the caller,
- * work is queued on `stream` (a cudaStream_t, may be NULL) and the call
- * returns without synchronising. Scratch memory comes from the ctx. */
+ * work is queued on `stream` (a cudaStream_t, may be NULL). With the default
+ * transition mode the call waits once on `stream` for a 16-byte count (the
+ * size of the per-sample typed-marker lists) before queueing the rest, then
+ * returns without a further synchronisation. Scratch memory comes from the ctx. */
 si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
                            float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
 

@@ -24,6 +24,7 @@ SAMPLE_ARGMAX, SAMPLE_PHILOX = 0, 1
 PBWT_STORE_INDEX, PBWT_ROW_HASHES = 1, 2
 GENO_MISSING = 3
 IMPUTE_RESELECT = 1
+IMPUTE_FULL_CHAIN = 2
 
 
 class NativeLibraryError(RuntimeError):

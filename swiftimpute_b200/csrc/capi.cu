@@ -1,4 +1,5 @@
 // capi.cu — the C ABI (include/swiftimpute_b200.h) over the device kernels.
+#include "fb_typed.hpp"
 #include "si_internal.hpp"
 
 #include <algorithm>
@@ -172,6 +173,8 @@ si_status check_params(si_ctx* ctx, const si_impute_params* p) {
         return fail(ctx, SI_ERR_INVALID_ARG, "bad sampling mode");
     if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
     if (p->checkpoint_interval > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "checkpoint_interval must be <= 32");
+    if (p->flags & ~(uint32_t)(SI_IMPUTE_RESELECT | SI_IMPUTE_FULL_CHAIN))
+        return fail(ctx, SI_ERR_INVALID_ARG, "unknown flag bits");
     if (p->block_threads && (p->block_threads % 32 || p->block_threads > 128))
         return fail(ctx, SI_ERR_UNSUPPORTED, "block_threads must be a multiple of 32, <= 128");
     if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
@@ -186,6 +189,105 @@ void default_tiles(uint32_t L, uint32_t* T, uint32_t* C) {
     *T = lm <= 8 ? 64 : 32;
 }
 
+constexpr uint32_t kTabN = 4096;
+
+// Closed-form run coefficients for (c, delta, L) in FP64 (fb_typed.hpp).
+si_status ensure_tables(si_ctx* ctx, const LinTrans& t0, uint32_t L) {
+    uint64_t key = 0;
+    std::memcpy(&key, &t0, 8);
+    key = key * 0x9E3779B97F4A7C15ull ^ (uint64_t)L;
+    if (ctx->tab_Q.ptr && ctx->tab_key == key) return SI_OK;
+    const double c = (double)t0.c, dl = (double)t0.delta;
+    const double rho = dl + (double)L * c;
+    const double q = dl / rho;
+    const double lq = q > 0.0 ? std::log(q) : -INFINITY;
+    const double lr = std::log(rho);
+    int regime = std::fabs(rho - 1.0) < 1e-15 ? 2 : (rho < 1.0 ? 0 : 1);
+    const double lgc = regime == 0 ? std::log1p(-rho) : (regime == 1 ? std::log(rho - 1.0) : 0.0);
+    std::vector<float> Q(kTabN), S(kTabN);
+    std::vector<double> G(kTabN);
+    for (uint32_t n = 0; n < kTabN; ++n) {
+        const double qn = (n == 0) ? 1.0 : (q > 0.0 ? std::exp((double)n * lq) : 0.0);
+        const double om = (n == 0) ? 0.0 : (q > 0.0 ? -std::expm1((double)n * lq) : 1.0);
+        Q[n] = (float)qn;
+        S[n] = (float)(om / (double)L);
+        if (n == 0) G[n] = -INFINITY;
+        else if (regime == 0) G[n] = -(double)n * lr + std::log(-std::expm1((double)n * lr)) - lgc;
+        else if (regime == 1) G[n] = std::log(-std::expm1(-(double)n * lr)) - lgc;
+        else G[n] = std::log((double)n);
+    }
+    SI_TRY(dev_reserve(ctx, ctx->tab_Q, kTabN * 4));
+    SI_TRY(dev_reserve(ctx, ctx->tab_S, kTabN * 4));
+    SI_TRY(dev_reserve(ctx, ctx->tab_G, kTabN * 8));
+    SI_CUDA(ctx, cudaMemcpy(ctx->tab_Q.ptr, Q.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
+    SI_CUDA(ctx, cudaMemcpy(ctx->tab_S.ptr, S.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
+    SI_CUDA(ctx, cudaMemcpy(ctx->tab_G.ptr, G.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
+    ctx->tab_consts[0] = q > 0.0 ? std::log2(q) : -INFINITY;
+    ctx->tab_consts[1] = lr;
+    ctx->tab_consts[2] = lgc;
+    ctx->tab_consts[3] = regime;
+    ctx->tab_key = key;
+    return SI_OK;
+}
+
+// Typed-marker forward-backward (default transition mode): anchor lists,
+// chain checkpoints, then the parallel posterior pass.
+si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const SelectionCache* sel, const uint8_t* d_geno,
+                           uint32_t B, float* d_dosage, float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
+    const uint32_t L = p->num_states, M = ctx->M, lm = fb_lmax(L);
+    LinTrans t0;
+    SI_CUDA(ctx, cudaMemcpy(&t0, ctx->trans.ptr, sizeof t0, cudaMemcpyDeviceToHost), "read transition");
+    SI_TRY(ensure_tables(ctx, t0, L));
+    const uint32_t C = p->checkpoint_interval ? p->checkpoint_interval : 8;
+    const uint32_t T = p->block_threads ? p->block_threads : 128;
+    if (typed_post_smem_bytes(L, T, C) > 227u * 1024u)
+        return fail(ctx, SI_ERR_UNSUPPORTED, "posterior tile needs more than 227 KB of shared memory");
+    if (!ctx->pinned_totals)
+        SI_CUDA(ctx, cudaMallocHost(&ctx->pinned_totals, 2 * sizeof(unsigned long long)), "pinned totals");
+    SI_TRY(dev_reserve(ctx, ctx->t_counts, (size_t)B * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_aoff, ((size_t)B + 1) * 8));
+    SI_TRY(dev_reserve(ctx, ctx->t_woff, ((size_t)B + 1) * 8));
+    SI_CUDA(ctx,
+            launch_anchor_lists_count(d_geno, B, M, C, (uint32_t*)ctx->t_counts.ptr,
+                                      (unsigned long long*)ctx->t_aoff.ptr, (unsigned long long*)ctx->t_woff.ptr, s),
+            "anchor count");
+    SI_CUDA(ctx,
+            cudaMemcpyAsync(ctx->pinned_totals, (unsigned long long*)ctx->t_aoff.ptr + B, 8, cudaMemcpyDeviceToHost, s),
+            "read totals");
+    SI_CUDA(ctx,
+            cudaMemcpyAsync(ctx->pinned_totals + 1, (unsigned long long*)ctx->t_woff.ptr + B, 8,
+                            cudaMemcpyDeviceToHost, s),
+            "read totals");
+    SI_CUDA(ctx, cudaStreamSynchronize(s), "anchor count");
+    const unsigned long long NA = ctx->pinned_totals[0], NW = ctx->pinned_totals[1];
+    SI_TRY(dev_reserve(ctx, ctx->t_apos, (size_t)NA * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_acode, (size_t)NA));
+    SI_TRY(dev_reserve(ctx, ctx->t_wsample, (size_t)NW * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_ckF, (size_t)NW * lm * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_ckB, (size_t)NW * lm * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_ckU, (size_t)NW * 8));
+    SI_CUDA(ctx,
+            launch_anchor_lists_fill(d_geno, B, M, (const unsigned long long*)ctx->t_aoff.ptr,
+                                     (const unsigned long long*)ctx->t_woff.ptr, (uint32_t*)ctx->t_apos.ptr,
+                                     (uint8_t*)ctx->t_acode.ptr, (uint32_t*)ctx->t_wsample.ptr, s),
+            "anchor fill");
+    TypedTables tt;
+    tt.Q = (const float*)ctx->tab_Q.ptr; tt.S = (const float*)ctx->tab_S.ptr; tt.G = (const double*)ctx->tab_G.ptr;
+    tt.NT = kTabN; tt.log2q = (float)ctx->tab_consts[0]; tt.invL = 1.0f / (float)L;
+    tt.lr = ctx->tab_consts[1]; tt.lgc = ctx->tab_consts[2]; tt.regime = (int)ctx->tab_consts[3];
+    TypedArgs a;
+    a.masks = (const SlotMasks*)sel->masks.ptr;
+    a.B = B; a.M = M; a.L = L; a.C = C; a.threads = T;
+    a.sampling = p->sampling; a.tie_eps = (float)p->tie_eps; a.seed = p->seed; a.sid_base = p->sample_id_base;
+    a.aoff = (const unsigned long long*)ctx->t_aoff.ptr; a.woff = (const unsigned long long*)ctx->t_woff.ptr;
+    a.apos = (const uint32_t*)ctx->t_apos.ptr; a.acode = (const uint8_t*)ctx->t_acode.ptr;
+    a.wsample = (const uint32_t*)ctx->t_wsample.ptr; a.total_windows = NW;
+    a.ckptF = (float*)ctx->t_ckF.ptr; a.ckptB = (float*)ctx->t_ckB.ptr; a.ckptU = (double*)ctx->t_ckU.ptr;
+    a.dosage = d_dosage; a.hprob = d_hprob; a.haps = d_haps;
+    SI_CUDA(ctx, launch_typed_fb(a, tt, s), "typed forward-backward");
+    return SI_OK;
+}
+
 // Device part of an imputation over B chains whose inputs/outputs are device
 // pointers; queued on stream s.
 si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B, float* d_dosage,
@@ -198,6 +300,13 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
         SI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->ev[3], 0), "stream wait");
     }
     SI_TRY(ensure_trans(ctx, p));
+    if (p->transition_mode == SI_TRANS_MATRIX0 && !(p->flags & SI_IMPUTE_FULL_CHAIN)) {
+        SI_CUDA(ctx, cudaEventRecord(ctx->ev[1], s), "event");
+        SI_TRY(run_device_typed(ctx, p, sel, d_geno, B, d_dosage, d_hprob, d_haps, s));
+        SI_CUDA(ctx, cudaEventRecord(ctx->ev[2], s), "event");
+        ctx->timings_pending = true;
+        return SI_OK;
+    }
     uint32_t T, C;
     default_tiles(p->num_states, &T, &C);
     if (p->checkpoint_interval) C = p->checkpoint_interval;
@@ -272,6 +381,11 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     dev_free(ctx, ctx->io_dosage);
     dev_free(ctx, ctx->io_hprob);
     dev_free(ctx, ctx->io_haps);
+    for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_acode,
+                                &ctx->t_wsample, &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->tab_Q, &ctx->tab_S,
+                                &ctx->tab_G})
+        dev_free(ctx, *b);
+    if (ctx->pinned_totals) cudaFreeHost(ctx->pinned_totals);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;

@@ -79,7 +79,13 @@ struct si_ctx {
     // imputation scratch, grown on demand
     si::DeviceBuffer trans;          // [M] LinTrans
     uint64_t trans_key = ~0ull;
-    si::DeviceBuffer ckpt;           // forward checkpoints
+    si::DeviceBuffer ckpt;           // forward checkpoints (full-chain kernel)
+    // typed-marker kernel scratch and tables
+    si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_wsample, t_ckF, t_ckB, t_ckU;
+    si::DeviceBuffer tab_Q, tab_S, tab_G;
+    uint64_t tab_key = ~0ull;
+    double tab_consts[4] = {0, 0, 0, 0};  // log2q, lr, lgc, regime
+    unsigned long long* pinned_totals = nullptr;
     si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
     float last_ms[3] = {0.f, 0.f, 0.f};
     bool timings_pending = false;
