@@ -181,6 +181,11 @@ si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t
  * calls only). For si_impute_device this waits for the call's kernels. */
 si_status si_last_timings(si_ctx* ctx, float* ms3);
 
+/* Milliseconds of each kernel stage of the last si_impute* call (CUDA events on
+ * its stream): [0] selection, [1] typed-marker lists, [2] anchor chain,
+ * [3] posterior pass (or the whole full-chain kernel). Waits for the call. */
+si_status si_last_kernel_ms(si_ctx* ctx, float* ms4);
+
 #ifdef __cplusplus
 }
 #endif

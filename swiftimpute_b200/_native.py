@@ -79,6 +79,7 @@ SIGNATURES = [
     ("si_impute_device", c_int,
      [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("si_last_timings", c_int, [c_void_p, POINTER(c_float)]),
+    ("si_last_kernel_ms", c_int, [c_void_p, POINTER(c_float)]),
 ]
 
 _lib = None

@@ -129,6 +129,7 @@ si_status ensure_trans(si_ctx* ctx, const si_impute_params* p) {
     }
     SI_TRY(dev_reserve(ctx, ctx->trans, sizeof(LinTrans) * M));
     SI_CUDA(ctx, cudaMemcpy(ctx->trans.ptr, t.data(), sizeof(LinTrans) * M, cudaMemcpyHostToDevice), "copy trans");
+    ctx->trans0 = t0;
     ctx->trans_key = key;
     return SI_OK;
 }
@@ -235,9 +236,7 @@ si_status ensure_tables(si_ctx* ctx, const LinTrans& t0, uint32_t L) {
 si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const SelectionCache* sel, const uint8_t* d_geno,
                            uint32_t B, float* d_dosage, float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
     const uint32_t L = p->num_states, M = ctx->M, lm = fb_lmax(L);
-    LinTrans t0;
-    SI_CUDA(ctx, cudaMemcpy(&t0, ctx->trans.ptr, sizeof t0, cudaMemcpyDeviceToHost), "read transition");
-    SI_TRY(ensure_tables(ctx, t0, L));
+    SI_TRY(ensure_tables(ctx, ctx->trans0, L));
     const uint32_t C = p->checkpoint_interval ? p->checkpoint_interval : 8;
     const uint32_t T = p->block_threads ? p->block_threads : 128;
     if (typed_post_smem_bytes(L, T, C) > 227u * 1024u)
@@ -271,6 +270,7 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
                                      (const unsigned long long*)ctx->t_woff.ptr, (uint32_t*)ctx->t_apos.ptr,
                                      (uint8_t*)ctx->t_acode.ptr, (uint32_t*)ctx->t_wsample.ptr, s),
             "anchor fill");
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[2], s), "event");
     TypedTables tt;
     tt.Q = (const float*)ctx->tab_Q.ptr; tt.S = (const float*)ctx->tab_S.ptr; tt.G = (const double*)ctx->tab_G.ptr;
     tt.NT = kTabN; tt.log2q = (float)ctx->tab_consts[0]; tt.invL = 1.0f / (float)L;
@@ -284,7 +284,9 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
     a.wsample = (const uint32_t*)ctx->t_wsample.ptr; a.total_windows = NW;
     a.ckptF = (float*)ctx->t_ckF.ptr; a.ckptB = (float*)ctx->t_ckB.ptr; a.ckptU = (double*)ctx->t_ckU.ptr;
     a.dosage = d_dosage; a.hprob = d_hprob; a.haps = d_haps;
+    a.ev_chain_done = ctx->kev[3];
     SI_CUDA(ctx, launch_typed_fb(a, tt, s), "typed forward-backward");
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[4], s), "event");
     return SI_OK;
 }
 
@@ -293,7 +295,10 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
 si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B, float* d_dosage,
                      float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
     SelectionCache* sel = nullptr;
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[0], s), "event");
     SI_TRY(ensure_selection(ctx, p->num_states, p->selection_kind, &sel, (p->flags & SI_IMPUTE_RESELECT) != 0, s));
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[1], s), "event");
+    ctx->kernel_pending = true;
     if (s != ctx->stream && !(p->flags & SI_IMPUTE_RESELECT)) {
         // a cached table may have been built on the ctx stream: order it before s
         SI_CUDA(ctx, cudaEventRecord(ctx->ev[3], ctx->stream), "event");
@@ -322,7 +327,10 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
     l.sampling = p->sampling; l.tie_eps = (float)p->tie_eps; l.seed = p->seed; l.sample_id_base = p->sample_id_base;
     l.ckpt = (float*)ctx->ckpt.ptr; l.dosage = d_dosage; l.hprob = d_hprob; l.haps = d_haps;
     SI_CUDA(ctx, cudaEventRecord(ctx->ev[1], s), "event");
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[2], s), "event");
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[3], s), "event");
     SI_CUDA(ctx, launch_fb(l, s), "forward-backward kernel");
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[4], s), "event");
     SI_CUDA(ctx, cudaEventRecord(ctx->ev[2], s), "event");
     ctx->timings_pending = true;
     return SI_OK;
@@ -365,6 +373,8 @@ si_status si_ctx_create(int device, uint64_t hbm_budget_bytes, si_ctx** out) {
     if (cudaStreamCreateWithFlags(&ctx->stream, cudaStreamNonBlocking) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
     for (auto& e : ctx->ev)
         if (cudaEventCreate(&e) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
+    for (auto& e : ctx->kev)
+        if (cudaEventCreate(&e) != cudaSuccess) { delete ctx; return SI_ERR_CUDA; }
     *out = ctx;
     return SI_OK;
 }
@@ -387,6 +397,7 @@ si_status si_ctx_destroy(si_ctx* ctx) {
         dev_free(ctx, *b);
     if (ctx->pinned_totals) cudaFreeHost(ctx->pinned_totals);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
+    for (auto& e : ctx->kev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
     delete ctx;
     return SI_OK;
@@ -653,6 +664,17 @@ si_status si_last_timings(si_ctx* ctx, float* ms3) {
         ctx->timings_pending = false;
     }
     for (int i = 0; i < 3; ++i) ms3[i] = ctx->last_ms[i];
+    return SI_OK;
+}
+
+si_status si_last_kernel_ms(si_ctx* ctx, float* ms4) {
+    if (!ctx || !ms4) return SI_ERR_INVALID_ARG;
+    if (ctx->kernel_pending) {
+        SI_CUDA(ctx, cudaEventSynchronize(ctx->kev[4]), "wait for kernels");
+        for (int i = 0; i < 4; ++i) cudaEventElapsedTime(&ctx->kernel_ms[i], ctx->kev[i], ctx->kev[i + 1]);
+        ctx->kernel_pending = false;
+    }
+    for (int i = 0; i < 4; ++i) ms4[i] = ctx->kernel_ms[i];
     return SI_OK;
 }
 

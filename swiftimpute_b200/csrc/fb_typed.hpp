@@ -37,6 +37,7 @@ struct TypedArgs {
     float* dosage;
     float* hprob;
     uint8_t* haps;
+    cudaEvent_t ev_chain_done;       // recorded between the chain and the posterior kernel (may be null)
 };
 
 cudaError_t launch_anchor_lists_count(const uint8_t* geno, uint32_t B, uint32_t M, uint32_t C, uint32_t* counts,

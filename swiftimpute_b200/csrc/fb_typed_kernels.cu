@@ -427,6 +427,7 @@ cudaError_t launch_typed_lm(const TypedArgs& a, const Tabs& tb, cudaStream_t s) 
     anchor_chain_kernel<LM><<<(a.B + 127) / 128, 128, 0, s>>>(a, tb);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
+    if (a.ev_chain_done && (e = cudaEventRecord(a.ev_chain_done, s)) != cudaSuccess) return e;
     const uint32_t T = a.threads;
     const size_t sm = post_smem<LM>(T, a.C);
     e = cudaFuncSetAttribute(anchor_posterior_kernel<LM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);

@@ -58,6 +58,9 @@ struct si_ctx {
     std::string err;
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+    cudaEvent_t kev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // per-kernel timing of the last call
+    float kernel_ms[4] = {0.f, 0.f, 0.f, 0.f};
+    bool kernel_pending = false;
 
     // panel
     uint32_t M = 0, N = 0, W = 0;
@@ -79,6 +82,7 @@ struct si_ctx {
     // imputation scratch, grown on demand
     si::DeviceBuffer trans;          // [M] LinTrans
     uint64_t trans_key = ~0ull;
+    si::LinTrans trans0{1.f, 0.f};  // host copy of the first gap's transition
     si::DeviceBuffer ckpt;           // forward checkpoints (full-chain kernel)
     // typed-marker kernel scratch and tables
     si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_wsample, t_ckF, t_ckB, t_ckU;

@@ -133,6 +133,12 @@ class Engine:
                                               c_void_p(d_haps) if d_haps else None,
                                               c_void_p(stream) if stream else None))
 
+    def last_kernel_ms(self) -> tuple[float, float, float, float]:
+        """(selection, typed-marker lists, anchor chain, posterior or full-chain kernel) in ms."""
+        ms = (c_float * 4)()
+        self._check(self.lib.si_last_kernel_ms(self.h, ms))
+        return tuple(ms)
+
     def last_timings(self) -> tuple[float, float, float]:
         ms = (c_float * 3)()
         self._check(self.lib.si_last_timings(self.h, ms))

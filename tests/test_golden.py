@@ -59,8 +59,9 @@ def test_selection_matches_reference_kernels(name):
 def test_posteriors_match_reference_kernels(name):
     """The reference's FP32 log-space kernels against the FP64 oracle: the
     posterior each samples from (softmax of its normalised log posterior).
-    The reference's unscaled FP32 beta carries absolute errors up to ~1e-2 in
-    log space near the e^-999 floor, so the bar here is 2e-2 per probability."""
+    The reference's own FP32 rounding (unscaled beta near the e^-999 floor)
+    measures up to ~1.2e-4 per probability on these cases (0 under the
+    uniform map); the bar is 5e-4."""
     g = _ref_gpu()
     panel, pos, codes, L, ne = _case(g, name)
     pairs = oracle.select_pairs(oracle.pbwt_build(panel), L)
@@ -72,7 +73,7 @@ def test_posteriors_match_reference_kernels(name):
         P = np.exp(lp - lp.max(1, keepdims=True)); P /= P.sum(1, keepdims=True)
         R = np.exp(ref[b] - ref[b].max(1, keepdims=True)); R /= R.sum(1, keepdims=True)
         worst = max(worst, float(np.abs(P - R).max()))
-    assert worst <= 2e-2, worst
+    assert worst <= 5e-4, worst
 
 
 def test_argmax_haplotypes_match_reference_under_exact_ties():

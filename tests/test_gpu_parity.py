@@ -146,10 +146,14 @@ def test_fb_tiles_do_not_change_results(engine):
     panel, pos, codes, _ = workload(300, 400, 100, synth.typed_every(300, 5), 100, 13)
     load(engine, panel, pos, store=False)
     base = engine.impute(codes, N.default_params(), hap_prob=True)
-    for C, T in [(8, 32), (17, 96), (32, 128), (1, 32)]:
-        alt = engine.impute(codes, N.default_params(checkpoint_interval=C, block_threads=T), hap_prob=True)
-        assert np.array_equal(alt["haps"], base["haps"])
-        assert np.abs(alt["dosage"] - base["dosage"]).max() <= 1e-5
+    for flags in (0, N.IMPUTE_FULL_CHAIN):
+        for C, T in [(8, 32), (17, 96), (32, 128), (1, 32)]:
+            alt = engine.impute(codes, N.default_params(checkpoint_interval=C, block_threads=T, flags=flags),
+                                hap_prob=True)
+            assert np.array_equal(alt["haps"], base["haps"])
+            assert np.abs(alt["dosage"] - base["dosage"]).max() <= 2e-5
+    ms = engine.last_kernel_ms()
+    assert len(ms) == 4 and ms[3] > 0
 
 
 def test_fb_philox_sampling_and_batch_invariance(engine):
@@ -209,3 +213,40 @@ def test_budget_is_enforced():
         with pytest.raises(N.SIError) as e:
             eng.upload_panel(panel)
         assert e.value.status == 7
+
+
+def test_ragged_missingness_per_sample(engine):
+    """Each sample has its own typed set (random dropouts and extra calls), so
+    the typed-marker kernel's anchor lists differ in length per sample."""
+    panel, pos, codes, truth = workload(1200, 500, 45, synth.typed_every(1200, 6), 100, 18)
+    rng = np.random.default_rng(19)
+    codes = codes.copy()
+    drop = rng.random(codes.shape) < 0.3
+    codes[drop] = 3
+    extra = rng.random(codes.shape) < 0.02
+    codes[extra] = truth[extra]
+    codes[3, :] = 3          # a sample with no calls at all
+    codes[4, :] = truth[4]   # a sample typed everywhere
+    codes[5, 0] = 3          # marker 0 missing
+    compare(engine, panel, pos, codes, 8, 10000)
+    compare(engine, panel, pos, codes, 16, 10000, sampling=N.SAMPLE_PHILOX)
+
+
+@pytest.mark.parametrize("spacing,every", [(100, 5), (500_000, 5), (20, 97), (100, 1)])
+def test_typed_kernel_agrees_with_full_chain(engine, spacing, every):
+    panel, pos, codes, _ = workload(1500, 600, 64, synth.typed_every(1500, every), spacing, 20)
+    load(engine, panel, pos, store=False)
+    typed = engine.impute(codes, N.default_params(), hap_prob=True)
+    full = engine.impute(codes, N.default_params(flags=N.IMPUTE_FULL_CHAIN), hap_prob=True)
+    assert np.abs(typed["dosage"] - full["dosage"]).max() <= 2e-5
+    assert np.abs(typed["hap_prob"] - full["hap_prob"]).max() <= 2e-5
+    assert np.mean(typed["haps"] != full["haps"]) <= 1e-4
+
+
+def test_long_untyped_gaps_beyond_tables(engine):
+    """Gaps longer than the 4,096-entry closed-form tables use the on-the-fly
+    formulas."""
+    panel, pos, codes, _ = workload(9000, 200, 6, np.array([0, 5, 4700, 8999]), 30, 21)
+    compare(engine, panel, pos, codes, 8, 10000)
+    panel, pos, codes, _ = workload(9000, 200, 6, np.array([3, 4500]), 500_000, 22)
+    compare(engine, panel, pos, codes, 4, 10000)
