@@ -270,11 +270,6 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A, Tabs tb)
 // ---------------------------------------------------------------- posterior
 
 template <int LM>
-struct Epi {
-    float p[LM];
-};
-
-template <int LM>
 __global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A, Tabs tb) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t T = blockDim.x, t = threadIdx.x, C = A.C;
