@@ -176,6 +176,45 @@ si_status si_impute_gl(si_ctx* ctx, const si_impute_params* p, const float* gl, 
 si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
                            float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
 
+/* Uneven batches ----------------------------------------------------------
+ * One launch sequence over targets that cover different marker ranges
+ * (regions) with different slot counts. A region is a contiguous panel slice
+ * [m_begin, m_end) imputed with num_states slots. Its selection comes either
+ * from the resident index (SI_INDEX_GLOBAL: the PBWT swept from marker 0, as
+ * the serving loop uses it) or from a sweep restarted at m_begin
+ * (SI_INDEX_REGION: what the reference computes when run on the sliced panel,
+ * ReferencePanel::load_vcf(filename, region), imputer.cpp:27-44, including
+ * the slice's own first-gap transition matrix). A GLOBAL region uses the
+ * panel's first-gap matrix, like a full-panel imputation. Each job is one target of one region: its codes are the
+ * (m_end - m_begin) bytes at geno + geno_offset; its outputs are packed at
+ * out_offset: dosage[out_offset + i], hap_prob[2 (out_offset + i) + phase],
+ * haps[2 out_offset + i] (hap0) and haps[2 out_offset + len + i] (hap1).
+ * Philox draws are keyed by (seed, sample_id, absolute marker), so a job's
+ * draws do not depend on the rest of the batch. */
+enum { SI_INDEX_GLOBAL = 0, SI_INDEX_REGION = 1 };
+
+typedef struct {
+    uint32_t m_begin;
+    uint32_t m_end;
+    uint32_t num_states;   /* 1..32 */
+    int32_t index_origin;  /* SI_INDEX_* */
+} si_region;
+
+typedef struct {
+    uint32_t region;
+    uint32_t reserved;
+    uint64_t geno_offset;
+    uint64_t out_offset;
+    uint64_t sample_id;
+} si_job;
+
+/* Device buffers; regions and jobs are host arrays. params->num_states is
+ * ignored (each region has its own); params->transition_mode must be
+ * SI_TRANS_MATRIX0. */
+si_status si_impute_jobs_device(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
+                                const si_job* jobs, uint32_t n_jobs, const uint8_t* d_geno, float* d_dosage,
+                                float* d_hap_prob, uint8_t* d_haps, void* stream);
+
 /* Milliseconds of the last si_impute* device work (CUDA events): [0] selection,
  * [1] forward-backward kernel, [2] whole call including copies (host-buffer
  * calls only). For si_impute_device this waits for the call's kernels. */

@@ -57,6 +57,20 @@ class ImputeParams(ctypes.Structure):
     ]
 
 
+INDEX_GLOBAL, INDEX_REGION = 0, 1
+
+
+class Region(ctypes.Structure):
+    """Mirror of ``si_region``."""
+    _fields_ = [("m_begin", c_uint32), ("m_end", c_uint32), ("num_states", c_uint32), ("index_origin", c_int32)]
+
+
+class Job(ctypes.Structure):
+    """Mirror of ``si_job``."""
+    _fields_ = [("region", c_uint32), ("reserved", c_uint32), ("geno_offset", c_uint64), ("out_offset", c_uint64),
+                ("sample_id", c_uint64)]
+
+
 # (name, restype, argtypes) for every symbol the header declares.
 SIGNATURES = [
     ("si_abi_version", c_int, []),
@@ -78,6 +92,9 @@ SIGNATURES = [
     ("si_impute_gl", c_int, [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p]),
     ("si_impute_device", c_int,
      [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
+    ("si_impute_jobs_device", c_int,
+     [c_void_p, POINTER(ImputeParams), POINTER(Region), c_uint32, POINTER(Job), c_uint32, c_void_p, c_void_p,
+      c_void_p, c_void_p, c_void_p]),
     ("si_last_timings", c_int, [c_void_p, POINTER(c_float)]),
     ("si_last_kernel_ms", c_int, [c_void_p, POINTER(c_float)]),
 ]

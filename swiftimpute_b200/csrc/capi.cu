@@ -80,6 +80,8 @@ void reset_index(si_ctx* ctx) {
         dev_free(ctx, kv.second.masks);
     }
     ctx->sel.clear();
+    for (auto& kv : ctx->region_sel) dev_free(ctx, kv.second.masks);
+    ctx->region_sel.clear();
     ctx->has_index = false;
     ctx->pbwt_flags = 0;
 }
@@ -192,102 +194,120 @@ void default_tiles(uint32_t L, uint32_t* T, uint32_t* C) {
 
 constexpr uint32_t kTabN = 4096;
 
-// Closed-form run coefficients for (c, delta, L) in FP64 (fb_typed.hpp).
-si_status ensure_tables(si_ctx* ctx, const LinTrans& t0, uint32_t L) {
+// Closed-form run coefficients for (c, delta, L) in FP64 (fb_typed.hpp),
+// cached per (transition, L).
+si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* out) {
     uint64_t key = 0;
     std::memcpy(&key, &t0, 8);
     key = key * 0x9E3779B97F4A7C15ull ^ (uint64_t)L;
-    if (ctx->tab_Q.ptr && ctx->tab_key == key) return SI_OK;
-    const double c = (double)t0.c, dl = (double)t0.delta;
-    const double rho = dl + (double)L * c;
-    const double q = dl / rho;
-    const double lq = q > 0.0 ? std::log(q) : -INFINITY;
-    const double lr = std::log(rho);
-    int regime = std::fabs(rho - 1.0) < 1e-15 ? 2 : (rho < 1.0 ? 0 : 1);
-    const double lgc = regime == 0 ? std::log1p(-rho) : (regime == 1 ? std::log(rho - 1.0) : 0.0);
-    std::vector<float> Q(kTabN), S(kTabN);
-    std::vector<double> G(kTabN);
-    for (uint32_t n = 0; n < kTabN; ++n) {
-        const double qn = (n == 0) ? 1.0 : (q > 0.0 ? std::exp((double)n * lq) : 0.0);
-        const double om = (n == 0) ? 0.0 : (q > 0.0 ? -std::expm1((double)n * lq) : 1.0);
-        Q[n] = (float)qn;
-        S[n] = (float)(om / (double)L);
-        if (n == 0) G[n] = -INFINITY;
-        else if (regime == 0) G[n] = -(double)n * lr + std::log(-std::expm1((double)n * lr)) - lgc;
-        else if (regime == 1) G[n] = std::log(-std::expm1(-(double)n * lr)) - lgc;
-        else G[n] = std::log((double)n);
+    auto& ts = ctx->tables[key];
+    if (!ts.Q.ptr) {
+        const double c = (double)t0.c, dl = (double)t0.delta;
+        const double rho = dl + (double)L * c;
+        const double q = dl / rho;
+        const double lq = q > 0.0 ? std::log(q) : -INFINITY;
+        const double lr = std::log(rho);
+        const int regime = std::fabs(rho - 1.0) < 1e-15 ? 2 : (rho < 1.0 ? 0 : 1);
+        const double lgc = regime == 0 ? std::log1p(-rho) : (regime == 1 ? std::log(rho - 1.0) : 0.0);
+        std::vector<float> Q(kTabN), S(kTabN);
+        std::vector<double> G(kTabN);
+        for (uint32_t n = 0; n < kTabN; ++n) {
+            const double qn = (n == 0) ? 1.0 : (q > 0.0 ? std::exp((double)n * lq) : 0.0);
+            const double om = (n == 0) ? 0.0 : (q > 0.0 ? -std::expm1((double)n * lq) : 1.0);
+            Q[n] = (float)qn;
+            S[n] = (float)(om / (double)L);
+            if (n == 0) G[n] = -INFINITY;
+            else if (regime == 0) G[n] = -(double)n * lr + std::log(-std::expm1((double)n * lr)) - lgc;
+            else if (regime == 1) G[n] = std::log(-std::expm1(-(double)n * lr)) - lgc;
+            else G[n] = std::log((double)n);
+        }
+        si_status st = dev_alloc(ctx, ts.Q, kTabN * 4);
+        if (st == SI_OK) st = dev_alloc(ctx, ts.S, kTabN * 4);
+        if (st == SI_OK) st = dev_alloc(ctx, ts.G, kTabN * 8);
+        if (st != SI_OK) {
+            dev_free(ctx, ts.Q); dev_free(ctx, ts.S); dev_free(ctx, ts.G);
+            ctx->tables.erase(key);
+            return st;
+        }
+        SI_CUDA(ctx, cudaMemcpy(ts.Q.ptr, Q.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
+        SI_CUDA(ctx, cudaMemcpy(ts.S.ptr, S.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
+        SI_CUDA(ctx, cudaMemcpy(ts.G.ptr, G.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
+        ts.consts[0] = q > 0.0 ? std::log2(q) : -INFINITY;
+        ts.consts[1] = lr;
+        ts.consts[2] = lgc;
+        ts.consts[3] = regime;
     }
-    SI_TRY(dev_reserve(ctx, ctx->tab_Q, kTabN * 4));
-    SI_TRY(dev_reserve(ctx, ctx->tab_S, kTabN * 4));
-    SI_TRY(dev_reserve(ctx, ctx->tab_G, kTabN * 8));
-    SI_CUDA(ctx, cudaMemcpy(ctx->tab_Q.ptr, Q.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
-    SI_CUDA(ctx, cudaMemcpy(ctx->tab_S.ptr, S.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
-    SI_CUDA(ctx, cudaMemcpy(ctx->tab_G.ptr, G.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
-    ctx->tab_consts[0] = q > 0.0 ? std::log2(q) : -INFINITY;
-    ctx->tab_consts[1] = lr;
-    ctx->tab_consts[2] = lgc;
-    ctx->tab_consts[3] = regime;
-    ctx->tab_key = key;
+    out->Q = (const float*)ts.Q.ptr; out->S = (const float*)ts.S.ptr; out->G = (const double*)ts.G.ptr;
+    out->NT = kTabN; out->log2q = (float)ts.consts[0]; out->invL = 1.0f / (float)L;
+    out->lr = ts.consts[1]; out->lgc = ts.consts[2]; out->regime = (int)ts.consts[3];
     return SI_OK;
 }
 
-// Typed-marker forward-backward (default transition mode): anchor lists,
-// chain checkpoints, then the parallel posterior pass.
-si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const SelectionCache* sel, const uint8_t* d_geno,
-                           uint32_t B, float* d_dosage, float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
-    const uint32_t L = p->num_states, M = ctx->M, lm = fb_lmax(L);
-    SI_TRY(ensure_tables(ctx, ctx->trans0, L));
-    const uint32_t C = p->checkpoint_interval ? p->checkpoint_interval : 8;
-    const uint32_t T = p->block_threads ? p->block_threads : 128;
-    if (typed_post_smem_bytes(L, T, C) > 227u * 1024u)
+// The typed-marker pipeline once the per-sample views are set in `a`
+// (geno, B, M, regions/samples or reg0, sampling, outputs): anchor lists,
+// chain, posterior. Waits once on `s` for the 16-byte list totals.
+si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32_t lmax, bool all_full,
+                    cudaStream_t s) {
+    a.C = p->checkpoint_interval ? p->checkpoint_interval : 8;
+    a.threads = p->block_threads ? p->block_threads : 128;
+    if (typed_post_smem_bytes(lmax, a.threads, a.C) > 227u * 1024u)
         return fail(ctx, SI_ERR_UNSUPPORTED, "posterior tile needs more than 227 KB of shared memory");
     if (!ctx->pinned_totals)
         SI_CUDA(ctx, cudaMallocHost(&ctx->pinned_totals, 2 * sizeof(unsigned long long)), "pinned totals");
+    const uint32_t B = a.B;
     SI_TRY(dev_reserve(ctx, ctx->t_counts, (size_t)B * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_aoff, ((size_t)B + 1) * 8));
     SI_TRY(dev_reserve(ctx, ctx->t_woff, ((size_t)B + 1) * 8));
-    SI_CUDA(ctx,
-            launch_anchor_lists_count(d_geno, B, M, C, (uint32_t*)ctx->t_counts.ptr,
-                                      (unsigned long long*)ctx->t_aoff.ptr, (unsigned long long*)ctx->t_woff.ptr, s),
-            "anchor count");
-    SI_CUDA(ctx,
-            cudaMemcpyAsync(ctx->pinned_totals, (unsigned long long*)ctx->t_aoff.ptr + B, 8, cudaMemcpyDeviceToHost, s),
-            "read totals");
-    SI_CUDA(ctx,
-            cudaMemcpyAsync(ctx->pinned_totals + 1, (unsigned long long*)ctx->t_woff.ptr + B, 8,
-                            cudaMemcpyDeviceToHost, s),
-            "read totals");
+    a.counts = (uint32_t*)ctx->t_counts.ptr;
+    a.aoff = (unsigned long long*)ctx->t_aoff.ptr;
+    a.woff = (unsigned long long*)ctx->t_woff.ptr;
+    SI_CUDA(ctx, launch_anchor_lists_count(a, s), "anchor count");
+    SI_CUDA(ctx, cudaMemcpyAsync(ctx->pinned_totals, a.aoff + B, 8, cudaMemcpyDeviceToHost, s), "read totals");
+    SI_CUDA(ctx, cudaMemcpyAsync(ctx->pinned_totals + 1, a.woff + B, 8, cudaMemcpyDeviceToHost, s), "read totals");
     SI_CUDA(ctx, cudaStreamSynchronize(s), "anchor count");
     const unsigned long long NA = ctx->pinned_totals[0], NW = ctx->pinned_totals[1];
     SI_TRY(dev_reserve(ctx, ctx->t_apos, (size_t)NA * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_aem, (size_t)NA * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_acode, (size_t)NA));
     SI_TRY(dev_reserve(ctx, ctx->t_wsample, (size_t)NW * 4));
-    SI_TRY(dev_reserve(ctx, ctx->t_ckF, (size_t)NW * lm * 4));
-    SI_TRY(dev_reserve(ctx, ctx->t_ckB, (size_t)NW * lm * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_ckF, (size_t)NW * lmax * 4));
+    SI_TRY(dev_reserve(ctx, ctx->t_ckB, (size_t)NW * lmax * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_ckU, (size_t)NW * 8));
-    SI_CUDA(ctx,
-            launch_anchor_lists_fill(d_geno, B, M, (const unsigned long long*)ctx->t_aoff.ptr,
-                                     (const unsigned long long*)ctx->t_woff.ptr, (uint32_t*)ctx->t_apos.ptr,
-                                     (uint8_t*)ctx->t_acode.ptr, (uint32_t*)ctx->t_wsample.ptr, s),
-            "anchor fill");
+    a.apos = (uint32_t*)ctx->t_apos.ptr;
+    a.aem = (uint32_t*)ctx->t_aem.ptr;
+    a.ashift = (uint8_t*)ctx->t_acode.ptr;
+    a.wsample = (uint32_t*)ctx->t_wsample.ptr;
+    a.total_windows = NW;
+    a.ckptF = (float*)ctx->t_ckF.ptr;
+    a.ckptB = (float*)ctx->t_ckB.ptr;
+    a.ckptU = (double*)ctx->t_ckU.ptr;
+    SI_CUDA(ctx, launch_anchor_lists_fill(a, s), "anchor fill");
     SI_CUDA(ctx, cudaEventRecord(ctx->kev[2], s), "event");
-    TypedTables tt;
-    tt.Q = (const float*)ctx->tab_Q.ptr; tt.S = (const float*)ctx->tab_S.ptr; tt.G = (const double*)ctx->tab_G.ptr;
-    tt.NT = kTabN; tt.log2q = (float)ctx->tab_consts[0]; tt.invL = 1.0f / (float)L;
-    tt.lr = ctx->tab_consts[1]; tt.lgc = ctx->tab_consts[2]; tt.regime = (int)ctx->tab_consts[3];
-    TypedArgs a;
-    a.masks = (const SlotMasks*)sel->masks.ptr;
-    a.B = B; a.M = M; a.L = L; a.C = C; a.threads = T;
-    a.sampling = p->sampling; a.tie_eps = (float)p->tie_eps; a.seed = p->seed; a.sid_base = p->sample_id_base;
-    a.aoff = (const unsigned long long*)ctx->t_aoff.ptr; a.woff = (const unsigned long long*)ctx->t_woff.ptr;
-    a.apos = (const uint32_t*)ctx->t_apos.ptr; a.acode = (const uint8_t*)ctx->t_acode.ptr;
-    a.wsample = (const uint32_t*)ctx->t_wsample.ptr; a.total_windows = NW;
-    a.ckptF = (float*)ctx->t_ckF.ptr; a.ckptB = (float*)ctx->t_ckB.ptr; a.ckptU = (double*)ctx->t_ckU.ptr;
-    a.dosage = d_dosage; a.hprob = d_hprob; a.haps = d_haps;
     a.ev_chain_done = ctx->kev[3];
-    SI_CUDA(ctx, launch_typed_fb(a, tt, s), "typed forward-backward");
+    SI_CUDA(ctx, launch_typed_fb(a, lmax, all_full, s), "typed forward-backward");
     SI_CUDA(ctx, cudaEventRecord(ctx->kev[4], s), "event");
     return SI_OK;
+}
+
+// Typed-marker forward-backward for a plain batch (every sample over all M markers).
+si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const SelectionCache* sel, const uint8_t* d_geno,
+                           uint32_t B, float* d_dosage, float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
+    TypedArgs a{};
+    a.geno = d_geno;
+    a.B = B;
+    a.M = ctx->M;
+    a.sampling = p->sampling;
+    a.tie_eps = (float)p->tie_eps;
+    a.seed = p->seed;
+    a.sid_base = p->sample_id_base;
+    a.reg0.masks = (const SlotMasks*)sel->masks.ptr;
+    a.reg0.L = p->num_states;
+    SI_TRY(tables_for(ctx, ctx->trans0, p->num_states, &a.reg0.tabs));
+    a.dosage = d_dosage;
+    a.hprob = d_hprob;
+    a.haps = d_haps;
+    const uint32_t lmax = fb_lmax(p->num_states);
+    return run_typed(ctx, p, a, lmax, lmax == p->num_states, s);
 }
 
 // Device part of an imputation over B chains whose inputs/outputs are device
@@ -391,10 +411,16 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     dev_free(ctx, ctx->io_dosage);
     dev_free(ctx, ctx->io_hprob);
     dev_free(ctx, ctx->io_haps);
-    for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_acode,
-                                &ctx->t_wsample, &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->tab_Q, &ctx->tab_S,
-                                &ctx->tab_G})
+    for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_acode, &ctx->t_aem,
+                                &ctx->t_wsample, &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->job_regions,
+                                &ctx->job_samples})
         dev_free(ctx, *b);
+    for (auto& kv : ctx->tables) {
+        dev_free(ctx, kv.second.Q);
+        dev_free(ctx, kv.second.S);
+        dev_free(ctx, kv.second.G);
+    }
+    for (auto& kv : ctx->region_sel) dev_free(ctx, kv.second.masks);
     if (ctx->pinned_totals) cudaFreeHost(ctx->pinned_totals);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->kev) if (e) cudaEventDestroy(e);
@@ -515,17 +541,21 @@ si_status si_pbwt_build(si_ctx* ctx, uint32_t flags) {
         SI_TRY(dev_alloc(ctx, ctx->row_hash, (size_t)M * 8));
         SI_CUDA(ctx, cudaMemsetAsync(ctx->row_hash.ptr, 0, (size_t)M * 8, ctx->stream), "memset hash");
     }
-    DeviceBuffer perm;
+    DeviceBuffer perm, jobbuf;
     SI_TRY(dev_alloc(ctx, perm, (size_t)2 * N * 4));
-    cudaError_t e = cudaEventRecord(ctx->ev[0], ctx->stream);
+    SI_TRY(dev_alloc(ctx, jobbuf, sizeof(SweepJob)));
+    const SweepJob job{0, M, 0};
+    cudaError_t e = cudaMemcpy(jobbuf.ptr, &job, sizeof job, cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
     if (e == cudaSuccess)
-        e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, M, N, ctx->W, (uint32_t*)ctx->head.ptr,
-                              (uint32_t*)ctx->prefix.ptr, (unsigned long long*)ctx->row_hash.ptr, (uint32_t*)perm.ptr,
-                              ctx->stream);
+        e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, (const SweepJob*)jobbuf.ptr, 1, N, ctx->W,
+                              (uint32_t*)ctx->head.ptr, (uint32_t*)ctx->prefix.ptr,
+                              (unsigned long long*)ctx->row_hash.ptr, (uint32_t*)perm.ptr, ctx->stream);
     if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
     if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
     if (e == cudaSuccess) e = cudaEventElapsedTime(&ctx->pbwt_ms, ctx->ev[0], ctx->ev[1]);
     dev_free(ctx, perm);
+    dev_free(ctx, jobbuf);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "PBWT sweep");
     ctx->has_index = true;
     ctx->pbwt_flags = flags;
@@ -664,6 +694,163 @@ si_status si_last_timings(si_ctx* ctx, float* ms3) {
         ctx->timings_pending = false;
     }
     for (int i = 0; i < 3; ++i) ms3[i] = ctx->last_ms[i];
+    return SI_OK;
+}
+
+si_status si_impute_jobs_device(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
+                                const si_job* jobs, uint32_t n_jobs, const uint8_t* d_geno, float* d_dosage,
+                                float* d_hap_prob, uint8_t* d_haps, void* stream) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!p || !regions || !jobs || !d_geno || n_regions == 0 || n_jobs == 0)
+        return fail(ctx, SI_ERR_INVALID_ARG, "NULL argument or empty batch");
+    if (p->transition_mode != SI_TRANS_MATRIX0)
+        return fail(ctx, SI_ERR_UNSUPPORTED, "uneven batches use the first-gap transition (SI_TRANS_MATRIX0)");
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    if (!ctx->has_map) return fail(ctx, SI_ERR_STATE, "marker positions not set (si_panel_set_map)");
+    if (p->sampling != SI_SAMPLE_ARGMAX && p->sampling != SI_SAMPLE_PHILOX)
+        return fail(ctx, SI_ERR_INVALID_ARG, "bad sampling mode");
+    if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
+    if (p->checkpoint_interval > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "checkpoint_interval must be <= 32");
+    if (p->block_threads && (p->block_threads % 32 || p->block_threads > 128))
+        return fail(ctx, SI_ERR_UNSUPPORTED, "block_threads must be a multiple of 32, <= 128");
+    SI_TRY(set_device(ctx));
+    cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[0], s), "event");
+    const uint32_t N = ctx->N, W = ctx->W;
+    uint32_t lmax = 4;
+    bool need_global = false;
+    for (uint32_t r = 0; r < n_regions; ++r) {
+        const si_region& g = regions[r];
+        if (g.m_begin >= g.m_end || g.m_end > ctx->M)
+            return fail(ctx, SI_ERR_INVALID_ARG, "region " + std::to_string(r) + " is empty or outside the panel");
+        if (g.num_states == 0 || g.num_states > 32)
+            return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) + ": num_states must be 1..32");
+        if (g.index_origin != SI_INDEX_GLOBAL && g.index_origin != SI_INDEX_REGION)
+            return fail(ctx, SI_ERR_INVALID_ARG, "bad index_origin");
+        lmax = std::max(lmax, fb_lmax(g.num_states));
+        need_global |= g.index_origin == SI_INDEX_GLOBAL;
+    }
+    bool all_full = true;
+    for (uint32_t r = 0; r < n_regions; ++r) all_full &= regions[r].num_states == lmax;
+    if (need_global) SI_TRY(ensure_trans(ctx, p));  // panel-wide first-gap transition (trans0)
+    std::vector<TypedRegion> tr(n_regions);
+    // region-local sweeps that are not cached yet, all in one launch
+    std::vector<SweepJob> sweeps;
+    std::vector<uint32_t> sweep_region;
+    uint64_t head_rows = 0;
+    for (uint32_t r = 0; r < n_regions; ++r) {
+        const si_region& g = regions[r];
+        if (g.index_origin != SI_INDEX_REGION) continue;
+        const uint32_t L = g.num_states;
+        const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+        auto key = std::make_tuple(g.m_begin, g.m_end, L, kind);
+        if (ctx->region_sel.count(key)) continue;
+        bool dup = false;
+        for (uint32_t q : sweep_region)
+            if (regions[q].m_begin == g.m_begin && regions[q].m_end == g.m_end) dup = true;
+        if (dup) continue;
+        sweeps.push_back(SweepJob{g.m_begin, g.m_end - g.m_begin, head_rows * kHead});
+        sweep_region.push_back(r);
+        head_rows += g.m_end - g.m_begin;
+    }
+    if (!sweeps.empty()) {
+        DeviceBuffer head, perm, jb;
+        SI_TRY(dev_alloc(ctx, head, head_rows * kHead * 4));
+        si_status st = dev_alloc(ctx, perm, (size_t)sweeps.size() * 2 * N * 4);
+        if (st == SI_OK) st = dev_alloc(ctx, jb, sweeps.size() * sizeof(SweepJob));
+        cudaError_t e = cudaSuccess;
+        if (st == SI_OK) e = cudaMemsetAsync(head.ptr, 0, head_rows * kHead * 4, s);
+        if (st == SI_OK && e == cudaSuccess)
+            e = cudaMemcpyAsync(jb.ptr, sweeps.data(), sweeps.size() * sizeof(SweepJob), cudaMemcpyHostToDevice, s);
+        if (st == SI_OK && e == cudaSuccess)
+            e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, (const SweepJob*)jb.ptr, (uint32_t)sweeps.size(),
+                                  N, W, (uint32_t*)head.ptr, nullptr, nullptr, (uint32_t*)perm.ptr, s);
+        // selection tables of every region (and slot count) that uses these sweeps
+        for (uint32_t r = 0; st == SI_OK && e == cudaSuccess && r < n_regions; ++r) {
+            const si_region& g = regions[r];
+            if (g.index_origin != SI_INDEX_REGION) continue;
+            const uint32_t L = g.num_states;
+            const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+            auto key = std::make_tuple(g.m_begin, g.m_end, L, kind);
+            if (ctx->region_sel.count(key)) continue;
+            size_t j = 0;
+            while (j < sweeps.size() && !(sweeps[j].m0 == g.m_begin && sweeps[j].len == g.m_end - g.m_begin)) ++j;
+            if (j == sweeps.size()) continue;  // cached already under another slot count? swept above
+            auto& rs = ctx->region_sel[key];
+            st = dev_alloc(ctx, rs.masks, (size_t)(g.m_end - g.m_begin) * sizeof(SlotMasks));
+            if (st != SI_OK) { ctx->region_sel.erase(key); break; }
+            e = launch_select((const uint32_t*)head.ptr + sweeps[j].head_off,
+                              (const uint32_t*)ctx->panel.ptr + (size_t)g.m_begin * W, g.m_end - g.m_begin, N, W, L,
+                              kind, nullptr, (SlotMasks*)rs.masks.ptr, s);
+        }
+        if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);  // scratch reuse below
+        dev_free(ctx, head);
+        dev_free(ctx, perm);
+        dev_free(ctx, jb);
+        if (st != SI_OK) return st;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "region sweep");
+    }
+    for (uint32_t r = 0; r < n_regions; ++r) {
+        const si_region& g = regions[r];
+        const uint32_t L = g.num_states;
+        tr[r].L = L;
+        if (g.index_origin == SI_INDEX_GLOBAL) {
+            SelectionCache* sel = nullptr;
+            SI_TRY(ensure_selection(ctx, L, p->selection_kind, &sel, false, s));
+            tr[r].masks = (const SlotMasks*)sel->masks.ptr + g.m_begin;
+            SI_TRY(tables_for(ctx, ctx->trans0, L, &tr[r].tabs));
+        } else {
+            const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+            tr[r].masks = (const SlotMasks*)ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)].masks.ptr;
+            const LinTrans t0 = (g.m_end - g.m_begin >= 2)
+                                    ? lin_trans(ctx->morgans[g.m_begin], ctx->morgans[g.m_begin + 1], (double)p->ne,
+                                                p->rho_rate)
+                                    : LinTrans{1.f, 0.f};
+            if (g.m_end - g.m_begin >= 2 && !(t0.c >= 1e-30f))
+                return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
+                                                         ": zero genetic distance in its first gap");
+            SI_TRY(tables_for(ctx, t0, L, &tr[r].tabs));
+        }
+    }
+    std::vector<TypedSample> ts(n_jobs);
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        if (jobs[j].region >= n_regions) return fail(ctx, SI_ERR_INVALID_ARG, "job region out of range");
+        const si_region& g = regions[jobs[j].region];
+        ts[j].geno_off = jobs[j].geno_offset;
+        ts[j].out_off = jobs[j].out_offset;
+        ts[j].sample_id = jobs[j].sample_id;
+        ts[j].m0 = g.m_begin;
+        ts[j].len = g.m_end - g.m_begin;
+        ts[j].region = jobs[j].region;
+        ts[j].pad = 0;
+    }
+    SI_TRY(dev_reserve(ctx, ctx->job_regions, tr.size() * sizeof(TypedRegion)));
+    SI_TRY(dev_reserve(ctx, ctx->job_samples, ts.size() * sizeof(TypedSample)));
+    SI_CUDA(ctx, cudaMemcpyAsync(ctx->job_regions.ptr, tr.data(), tr.size() * sizeof(TypedRegion),
+                                 cudaMemcpyHostToDevice, s), "copy regions");
+    SI_CUDA(ctx, cudaMemcpyAsync(ctx->job_samples.ptr, ts.data(), ts.size() * sizeof(TypedSample),
+                                 cudaMemcpyHostToDevice, s), "copy jobs");
+    SI_CUDA(ctx, cudaEventRecord(ctx->kev[1], s), "event");
+    ctx->kernel_pending = true;
+    TypedArgs a{};
+    a.geno = d_geno;
+    a.B = n_jobs;
+    a.M = 0;
+    a.sampling = p->sampling;
+    a.tie_eps = (float)p->tie_eps;
+    a.seed = p->seed;
+    a.sid_base = 0;
+    a.regions = (const TypedRegion*)ctx->job_regions.ptr;
+    a.samples = (const TypedSample*)ctx->job_samples.ptr;
+    a.dosage = d_dosage;
+    a.hprob = d_hap_prob;
+    a.haps = d_haps;
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[1], s), "event");
+    SI_TRY(run_typed(ctx, p, a, lmax, all_full, s));
+    SI_CUDA(ctx, cudaEventRecord(ctx->ev[2], s), "event");
+    ctx->timings_pending = true;
+    // host copies of tr/ts must outlive the async copies: wait before returning
+    SI_CUDA(ctx, cudaStreamSynchronize(s), "uneven batch");
     return SI_OK;
 }
 

@@ -19,17 +19,43 @@ struct TypedTables {
     int regime;  // 0: rho < 1, 1: rho > 1, 2: rho == 1
 };
 
-struct TypedArgs {
+// A panel slice imputed with L slots: its slot masks (index 0 = the slice's
+// first marker) and the closed-form tables of its transition.
+struct TypedRegion {
     const SlotMasks* masks;
-    uint32_t B, M, L, C, threads;
+    uint32_t L;
+    TypedTables tabs;
+};
+
+// One target of an uneven batch.
+struct TypedSample {
+    uint64_t geno_off;   // codes at geno + geno_off, len bytes
+    uint64_t out_off;    // outputs packed at out_off (dosage), 2 out_off (haps)
+    uint64_t sample_id;  // Philox counter
+    uint32_t m0;         // absolute panel marker of the slice's first marker
+    uint32_t len;
+    uint32_t region;
+    uint32_t pad;
+};
+
+struct TypedArgs {
+    const uint8_t* geno;
+    uint32_t B;                      // samples
+    uint32_t M;                      // markers per sample of a plain batch
+    uint32_t C, threads;
     int sampling;
     float tie_eps;
     uint64_t seed, sid_base;
-    const unsigned long long* aoff;  // [B+1] anchor offsets
-    const unsigned long long* woff;  // [B+1] window offsets
-    const uint32_t* apos;            // anchor marker positions
-    const uint8_t* acode;            // anchor genotype codes
-    const uint32_t* wsample;         // window -> sample
+    TypedRegion reg0;                // the region of a plain batch
+    const TypedRegion* regions;      // device array, uneven batches (else null)
+    const TypedSample* samples;      // device array, uneven batches (else null)
+    unsigned long long* aoff;        // [B+1] anchor offsets
+    unsigned long long* woff;        // [B+1] window offsets
+    uint32_t* counts;                // [B]
+    uint32_t* apos;                  // anchor positions (within the slice)
+    uint32_t* aem;                   // anchor emission masks over the slots
+    uint8_t* ashift;                 // 1 where no slot matches the call (every slot scaled by e^-999)
+    uint32_t* wsample;               // window -> sample
     unsigned long long total_windows;
     float* ckptF;                    // [windows][Lmax] forward anchor at each window's first anchor
     float* ckptB;                    // [windows][Lmax] backward anchor (E . beta, scaled)
@@ -40,12 +66,9 @@ struct TypedArgs {
     cudaEvent_t ev_chain_done;       // recorded between the chain and the posterior kernel (may be null)
 };
 
-cudaError_t launch_anchor_lists_count(const uint8_t* geno, uint32_t B, uint32_t M, uint32_t C, uint32_t* counts,
-                                      unsigned long long* aoff, unsigned long long* woff, cudaStream_t s);
-cudaError_t launch_anchor_lists_fill(const uint8_t* geno, uint32_t B, uint32_t M, const unsigned long long* aoff,
-                                     const unsigned long long* woff, uint32_t* apos, uint8_t* acode, uint32_t* wsample,
-                                     cudaStream_t s);
-cudaError_t launch_typed_fb(const TypedArgs& a, const TypedTables& t, cudaStream_t s);
+cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s);
+cudaError_t launch_anchor_lists_fill(const TypedArgs& a, cudaStream_t s);
+cudaError_t launch_typed_fb(const TypedArgs& a, uint32_t lmax, bool all_full, cudaStream_t s);
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C);
 
 }  // namespace si

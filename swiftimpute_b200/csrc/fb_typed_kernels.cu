@@ -40,17 +40,40 @@ __device__ __forceinline__ uint32_t emission_mask(uint32_t g, SlotMasks mk, uint
     return mg ? mg : lmask;
 }
 
-struct Tabs {
-    const float* Q;   // q^n
-    const float* S;   // (1 - q^n) / L
-    const double* G;  // log G(n)
-    uint32_t NT;
-    float log2q;
-    float invL;
-    double lr;        // log rho
-    double lgc;       // log(1 - rho) (rho < 1) or log(rho - 1) (rho > 1)
-    int regime;       // 0: rho < 1, 1: rho > 1, 2: rho == 1
+using Tabs = TypedTables;
+
+// Per-sample view: a plain batch is B rows of M codes sharing reg0; an uneven
+// batch reads its sample and region descriptors.
+struct View {
+    const uint8_t* geno;
+    uint64_t out;
+    uint64_t sid;
+    uint32_t m0, len;
+    TypedRegion r;
 };
+
+__device__ __forceinline__ View view_of(const TypedArgs& A, uint32_t s) {
+    View v;
+    if (A.samples) {
+        const TypedSample d = A.samples[s];
+        v.geno = A.geno + d.geno_off;
+        v.out = d.out_off;
+        v.sid = d.sample_id;
+        v.m0 = d.m0;
+        v.len = d.len;
+        v.r = A.regions[d.region];
+    } else {
+        v.geno = A.geno + (uint64_t)s * A.M;
+        v.out = (uint64_t)s * A.M;
+        v.sid = A.sid_base + s;
+        v.m0 = 0;
+        v.len = A.M;
+        v.r = A.reg0;
+    }
+    return v;
+}
+
+__device__ __forceinline__ uint32_t lmask_of(uint32_t L) { return L >= 32 ? 0xffffffffu : ((1u << L) - 1u); }
 
 __device__ __forceinline__ float tabQ(const Tabs& t, uint32_t n) {
     return n < t.NT ? __ldg(t.Q + n) : exp2f((float)n * t.log2q);
@@ -69,17 +92,16 @@ __device__ __forceinline__ double tabG(const Tabs& t, uint32_t n) {
 
 constexpr uint32_t kWarpsPerBlock = 8;
 
-__global__ void anchor_count_kernel(const uint8_t* __restrict__ geno, uint32_t B, uint32_t M,
-                                    uint32_t* __restrict__ counts) {
+__global__ void anchor_count_kernel(TypedArgs A) {
     const uint32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31;
-    if (s >= B) return;
-    const uint8_t* row = geno + (uint64_t)s * M;
+    if (s >= A.B) return;
+    const View v = view_of(A, s);
     uint32_t n = 0;
-    for (uint32_t m = lane; m < M; m += 32) n += (m == 0 || row[m] < 3) ? 1u : 0u;
+    for (uint32_t m = lane; m < v.len; m += 32) n += (m == 0 || v.geno[m] < 3) ? 1u : 0u;
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-    if (lane == 0) counts[s] = n;
+    if (lane == 0) A.counts[s] = n;
 }
 
 // Exclusive scans of anchor counts and window counts (ceil(count / C)) in one
@@ -123,32 +145,35 @@ __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __res
     if (t == T - 1) { aoff[B] = ra; woff[B] = rw; }
 }
 
-__global__ void anchor_fill_kernel(const uint8_t* __restrict__ geno, uint32_t B, uint32_t M,
-                                   const unsigned long long* __restrict__ aoff,
-                                   const unsigned long long* __restrict__ woff, uint32_t* __restrict__ apos,
-                                   uint8_t* __restrict__ acode, uint32_t* __restrict__ wsample) {
+// Anchor lists: marker position, emission mask over the slots and the
+// "no slot matches" flag (which scales every slot by e^-999, counted in
+// beta's unit), in marker order; marker 0 is always an anchor.
+__global__ void anchor_fill_kernel(TypedArgs A) {
     const uint32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31;
-    if (s >= B) return;
-    const uint8_t* row = geno + (uint64_t)s * M;
-    unsigned long long o = aoff[s];
-    for (uint32_t m0 = 0; m0 < M; m0 += 32) {
+    if (s >= A.B) return;
+    const View v = view_of(A, s);
+    const uint32_t lmask = lmask_of(v.r.L);
+    unsigned long long o = A.aoff[s];
+    for (uint32_t m0 = 0; m0 < v.len; m0 += 32) {
         const uint32_t m = m0 + lane;
         uint8_t g = 3;
         bool a = false;
-        if (m < M) {
-            g = row[m];
+        if (m < v.len) {
+            g = v.geno[m];
             a = (m == 0) || g < 3;
         }
         const uint32_t bal = __ballot_sync(0xffffffffu, a);
         if (a) {
             const unsigned long long at = o + __popc(bal & ((1u << lane) - 1u));
-            apos[at] = m;
-            acode[at] = g > 3 ? 3 : g;
+            uint32_t sh;
+            A.apos[at] = m;
+            A.aem[at] = emission_mask(g, v.r.masks[m], lmask, &sh);
+            A.ashift[at] = (uint8_t)sh;
         }
         o += __popc(bal);
     }
-    for (unsigned long long w = woff[s] + lane; w < woff[s + 1]; w += 32) wsample[w] = s;
+    for (unsigned long long w = A.woff[s] + lane; w < A.woff[s + 1]; w += 32) A.wsample[w] = s;
 }
 
 // ---------------------------------------------------------------- chain
@@ -218,122 +243,177 @@ __device__ __forceinline__ void init_forward(float (&a)[LM], uint32_t em) {
     for (int k = 0; k < LM; ++k) a[k] = ((em >> k) & 1u) ? 1.f : 0.f;
 }
 
+constexpr int kPrefetch = 8;  // anchors whose list entries are loaded ahead of the chain step
+
 template <int LM>
-__global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A, Tabs tb) {
+__global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
     const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
     if (s >= A.B) return;
-    const uint32_t lmask = A.L >= 32 ? 0xffffffffu : ((1u << A.L) - 1u);
+    const View v = view_of(A, s);
+    const Tabs& tb = v.r.tabs;
     const unsigned long long base = A.aoff[s], NA = A.aoff[s + 1] - base, wb = A.woff[s];
     const uint32_t* pos = A.apos + base;
-    const uint8_t* code = A.acode + base;
+    const uint32_t* aem = A.aem + base;
+    const uint8_t* ash = A.ashift + base;
     const uint32_t C = A.C;
-    uint32_t sh;
-    // forward
+    // forward: the list entries of kPrefetch anchors are loaded before their steps run
     float a[LM];
-    init_forward<LM>(a, emission_mask(code[0], A.masks[0], lmask, &sh));
-    forward_step<LM>(tb, 0, a, lmask);  // normalise (n = 0: q^0 = 1, S = 0)
+    init_forward<LM>(a, aem[0]);
+    forward_step<LM>(tb, 0, a, 0xffffffffu);  // normalise
 #pragma unroll
     for (int k = 0; k < LM; ++k) A.ckptF[wb * LM + k] = a[k];
-    for (unsigned long long k = 1; k < NA; ++k) {
-        const uint32_t p = pos[k];
-        forward_step<LM>(tb, p - pos[k - 1], a, emission_mask(code[k], A.masks[p], lmask, &sh));
-        if (k % C == 0)
+    uint32_t prev = pos[0];
+    for (unsigned long long k0 = 1; k0 < NA; k0 += kPrefetch) {
+        uint32_t pp[kPrefetch], ee[kPrefetch];
 #pragma unroll
-            for (int l = 0; l < LM; ++l) A.ckptF[(wb + k / C) * LM + l] = a[l];
+        for (int j = 0; j < kPrefetch; ++j) {
+            const unsigned long long k = k0 + j;
+            pp[j] = k < NA ? pos[k] : 0u;
+            ee[j] = k < NA ? aem[k] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kPrefetch; ++j) {
+            const unsigned long long k = k0 + j;
+            if (k < NA) {
+                forward_step<LM>(tb, pp[j] - prev, a, ee[j]);
+                prev = pp[j];
+                if (k % C == 0)
+#pragma unroll
+                    for (int l = 0; l < LM; ++l) A.ckptF[(wb + k / C) * LM + l] = a[l];
+            }
+        }
     }
     // backward
     float w[LM];
-    const uint32_t plast = pos[NA - 1];
-    double logU = chain_end_logU(tb, A.M - 1 - plast);
-    {
-        const uint32_t em = emission_mask(code[NA - 1], A.masks[plast], lmask, &sh);
-        init_forward<LM>(w, em);
-        logU -= 999.0 * (double)sh;
-    }
+    uint32_t nextp = pos[NA - 1];
+    double logU = chain_end_logU(tb, v.len - 1 - nextp);
+    init_forward<LM>(w, aem[NA - 1]);
+    logU -= 999.0 * (double)ash[NA - 1];
     if ((NA - 1) % C == 0) {
 #pragma unroll
         for (int l = 0; l < LM; ++l) A.ckptB[(wb + (NA - 1) / C) * LM + l] = w[l];
         A.ckptU[wb + (NA - 1) / C] = logU;
     }
-    for (long long k = (long long)NA - 2; k >= 0; --k) {
-        const uint32_t p = pos[k];
-        const uint32_t em = emission_mask(code[k], A.masks[p], lmask, &sh);
-        backward_step<LM>(tb, pos[k + 1] - p, w, logU, em, sh, lmask);
-        if (k % C == 0) {
+    for (long long k0 = (long long)NA - 2; k0 >= 0; k0 -= kPrefetch) {
+        uint32_t pp[kPrefetch], ee[kPrefetch], hh[kPrefetch];
 #pragma unroll
-            for (int l = 0; l < LM; ++l) A.ckptB[(wb + k / C) * LM + l] = w[l];
-            A.ckptU[wb + k / C] = logU;
+        for (int j = 0; j < kPrefetch; ++j) {
+            const long long k = k0 - j;
+            pp[j] = k >= 0 ? pos[k] : 0u;
+            ee[j] = k >= 0 ? aem[k] : 0u;
+            hh[j] = k >= 0 ? ash[k] : 0u;
+        }
+#pragma unroll
+        for (int j = 0; j < kPrefetch; ++j) {
+            const long long k = k0 - j;
+            if (k >= 0) {
+                backward_step<LM>(tb, nextp - pp[j], w, logU, ee[j], hh[j], 0u);
+                nextp = pp[j];
+                if (k % C == 0) {
+#pragma unroll
+                    for (int l = 0; l < LM; ++l) A.ckptB[(wb + k / C) * LM + l] = w[l];
+                    A.ckptU[wb + k / C] = logU;
+                }
+            }
         }
     }
 }
 
 // ---------------------------------------------------------------- posterior
 
-template <int LM>
-__global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A, Tabs tb) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t T = blockDim.x, t = threadIdx.x, C = A.C;
-    float* bw = reinterpret_cast<float*>(smem);                                  // [C][LM][T]
-    double* bu = reinterpret_cast<double*>(smem + (size_t)C * LM * T * 4);      // [C][T]
-    const unsigned long long g = (unsigned long long)blockIdx.x * T + t;
-    if (g >= A.total_windows) return;
-    const uint32_t s = A.wsample[g];
-    const unsigned long long base = A.aoff[s], NA = A.aoff[s + 1] - base, wb = A.woff[s];
-    const unsigned long long w = g - wb;
-    const uint32_t* pos = A.apos + base;
-    const uint8_t* code = A.acode + base;
-    const unsigned long long k0 = w * C, k1 = min(k0 + C, NA);
-    const uint32_t lmask = A.L >= 32 ? 0xffffffffu : ((1u << A.L) - 1u);
-    const uint32_t M = A.M;
-    uint32_t sh;
+// Per-warp output staging: each thread computes 32 consecutive cells of its
+// window into shared memory, then the warp writes every thread's 32 cells as
+// one coalesced row segment (128 B of dosage, 2 x 32 B of alleles).
+constexpr uint32_t kStageD = 33;  // floats per staged dosage row (32 + pad)
+constexpr uint32_t kStageH = 36;  // bytes per staged allele row (32 + pad)
 
-    // backward anchors k in (k0, k1], stored at slot k - k0 - 1
-    {
-        float v[LM];
+// nibble of slot bits -> four 0/1 floats (shared-memory table)
+__device__ __forceinline__ float4 nib(const float4* lut, uint32_t bits, int j) { return lut[(bits >> (4 * j)) & 15u]; }
+
+// kFull: every sample of the launch uses all LM slots (no active-slot masking).
+template <int LM, bool kFull>
+__global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    const uint32_t T = blockDim.x, t = threadIdx.x, C = A.C, lane = t & 31, warp = t >> 5;
+    float4* lut = reinterpret_cast<float4*>(smem);                                  // [16]
+    float* bw = reinterpret_cast<float*>(smem + 256);                               // [C][LM][T]
+    double* bu = reinterpret_cast<double*>(smem + 256 + (size_t)C * LM * T * 4);   // [C][T]
+    unsigned char* stage = smem + 256 + (size_t)C * LM * T * 4 + (size_t)C * T * 8;
+    float* sd = reinterpret_cast<float*>(stage) + (size_t)warp * 32 * kStageD;      // [32][kStageD] of this warp
+    uint8_t* sh8 = stage + (size_t)(T / 32) * 32 * kStageD * 4 + (size_t)warp * 64 * kStageH;  // [32][2][kStageH]
+    if (t < 16) lut[t] = make_float4((float)(t & 1), (float)((t >> 1) & 1), (float)((t >> 2) & 1), (float)(t >> 3));
+    __syncthreads();
+
+    const unsigned long long g = (unsigned long long)blockIdx.x * T + t;
+    const bool live = g < A.total_windows;
+
+    uint32_t s = 0, cstart = 0, ncells = 0;
+    View v{};
+    unsigned long long NA = 0, k0 = 0, k1 = 0;
+    const uint32_t* pos = nullptr;
+    const uint32_t* aem = nullptr;
+    float a[LM];
+#pragma unroll
+    for (int l = 0; l < LM; ++l) a[l] = 0.f;
+    if (live) {
+        s = A.wsample[g];
+        v = view_of(A, s);
+        const Tabs& tb = v.r.tabs;
+        const unsigned long long base = A.aoff[s], wb = A.woff[s], w = g - wb;
+        NA = A.aoff[s + 1] - base;
+        pos = A.apos + base;
+        aem = A.aem + base;
+        const uint8_t* ash = A.ashift + base;
+        k0 = w * C;
+        k1 = min(k0 + C, NA);
+        // backward anchors k in (k0, k1], at slot k - k0 - 1
+        float bv[LM];
         double logU;
         long long kstart;
         if (k1 < NA) {
 #pragma unroll
-            for (int l = 0; l < LM; ++l) v[l] = A.ckptB[(wb + w + 1) * LM + l];
+            for (int l = 0; l < LM; ++l) bv[l] = A.ckptB[(wb + w + 1) * LM + l];
             logU = A.ckptU[wb + w + 1];
             kstart = (long long)k1;
         } else {
-            const uint32_t plast = pos[NA - 1];
-            logU = chain_end_logU(tb, M - 1 - plast);
-            const uint32_t em = emission_mask(code[NA - 1], A.masks[plast], lmask, &sh);
-            init_forward<LM>(v, em);
-            logU -= 999.0 * (double)sh;
+            logU = chain_end_logU(tb, v.len - 1 - pos[NA - 1]) - 999.0 * (double)ash[NA - 1];
+            init_forward<LM>(bv, aem[NA - 1]);
             kstart = (long long)NA - 1;
         }
         for (long long k = kstart;; --k) {
             if (k > (long long)k0) {
                 const uint32_t slot = (uint32_t)(k - (long long)k0 - 1);
 #pragma unroll
-                for (int l = 0; l < LM; ++l) bw[((size_t)slot * LM + l) * T + t] = v[l];
+                for (int l = 0; l < LM; ++l) bw[((size_t)slot * LM + l) * T + t] = bv[l];
                 bu[(size_t)slot * T + t] = logU;
             }
             if (k - 1 <= (long long)k0) break;
-            const uint32_t p = pos[k - 1];
-            const uint32_t em = emission_mask(code[k - 1], A.masks[p], lmask, &sh);
-            backward_step<LM>(tb, pos[k] - p, v, logU, em, sh, lmask);
+            backward_step<LM>(tb, pos[k] - pos[k - 1], bv, logU, aem[k - 1], ash[k - 1], 0u);
         }
-    }
-
-    // forward sweep over the window's intervals with the fused epilogue
-    float a[LM];
 #pragma unroll
-    for (int l = 0; l < LM; ++l) a[l] = A.ckptF[(wb + w) * LM + l];
-    const float keep = 1.0f - A.tie_eps;
-    for (unsigned long long k = k0; k < k1; ++k) {
-        const uint32_t p0 = pos[k];
+        for (int l = 0; l < LM; ++l) a[l] = A.ckptF[(wb + w) * LM + l];
+        cstart = pos[k0];
+        ncells = (k1 < NA ? pos[k1] : v.len) - cstart;
+    }
+    const Tabs& tb = v.r.tabs;
+    const uint32_t lmask = lmask_of(v.r.L);
+    float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
+#pragma unroll
+    for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
+
+    // interval state (current anchor k, cells [p0, p1))
+    unsigned long long k = k0;
+    uint32_t p0 = cstart, p1 = 0, n = 0;
+    float Sa = 0.f, Sw = 0.f;
+    double farg = 0.0;
+    int mode = 2;  // 0: exact floor per cell, 1: floor negligible, 2: beta uniform
+    float wv[LM];
+    auto open_interval = [&]() {
         const bool has_next = k + 1 < NA;
-        const uint32_t p1 = has_next ? pos[k + 1] : M;
-        const uint32_t n = p1 - p0;
-        const float Sa = vsum<LM>(a);
-        float wv[LM];
-        float Sw = 0.f;
-        double farg = 0.0;
-        int mode = 2;  // 0: exact floor per cell, 1: floor negligible, 2: beta uniform
+        p1 = has_next ? pos[k + 1] : v.len;
+        n = p1 - p0;
+        Sa = vsum<LM>(a);
+        mode = 2;
         if (has_next) {
             const uint32_t slot = (uint32_t)(k - k0);
 #pragma unroll
@@ -343,13 +423,31 @@ __global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A, Tabs
             if (farg + tabG(tb, n) < -104.0) mode = 1;
             else if (farg + tabG(tb, 1) > 60.0) mode = 2;
             else mode = 0;
+        } else {
+#pragma unroll
+            for (int l = 0; l < LM; ++l) wv[l] = 0.f;
         }
-        for (uint32_t i = 0; i < n; ++i) {
-            const uint32_t m = p0 + i;
+    };
+    if (live) open_interval();
+
+    const float keep = 1.0f - A.tie_eps;
+    const uint32_t max_cells = __reduce_max_sync(0xffffffffu, ncells);
+    for (uint32_t cb = 0; cb < max_cells; cb += 32) {
+        for (uint32_t c = 0; c < 32; ++c) {
+            const uint32_t idx = cb + c;
+            if (idx >= ncells) break;
+            const uint32_t m = cstart + idx;
+            if (m == p1) {  // next anchor: forward step with its emission, open its interval
+                forward_step<LM>(tb, n, a, aem[k + 1]);
+                ++k;
+                p0 = p1;
+                open_interval();
+            }
+            const uint32_t i = m - p0;
             const float xf = tabQ(tb, i), yf = Sa * tabS(tb, i);
             float xb = 0.f, yb = 1.f;
             if (mode != 2) {
-                const uint32_t j1 = n - i;  // j + 1
+                const uint32_t j1 = n - i;
                 const float Qj = tabQ(tb, j1), Sj = tabS(tb, j1);
                 if (mode == 1) {
                     xb = Qj;
@@ -366,28 +464,44 @@ __global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A, Tabs
                     }
                 }
             }
-            const SlotMasks mk = A.masks[m];
+            const SlotMasks mk = v.r.masks[m];
+            // p_l = (xf a_l + yf)(xb w_l + yb), two slots per packed FP32x2 op
             float pr[LM];
-            float tot = 0.f, q0 = 0.f, q1 = 0.f, pmax = 0.f;
+            const float2 XF = make_float2(xf, xf), YF = make_float2(yf, yf);
+            const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
+            float2 tot2 = make_float2(0.f, 0.f), q02 = tot2, q12 = tot2;
 #pragma unroll
-            for (int l = 0; l < LM; ++l) {
-                const float al = fmaf(xf, a[l], yf);
-                const float be = fmaf(xb, has_next ? wv[l] : 0.f, yb);
-                pr[l] = ((lmask >> l) & 1u) ? al * be : 0.f;
-                tot += pr[l];
-                q0 += ((mk.a0 >> l) & 1u) ? pr[l] : 0.f;
-                q1 += ((mk.a1 >> l) & 1u) ? pr[l] : 0.f;
-                pmax = fmaxf(pmax, pr[l]);
+            for (int l = 0; l < LM; l += 2) {
+                const float2 al = __ffma2_rn(XF, make_float2(a[l], a[l + 1]), YF);
+                const float2 be = __ffma2_rn(XB, make_float2(wv[l], wv[l + 1]), YB);
+                float2 pp = __fmul2_rn(al, be);
+                if (!kFull) pp = __fmul2_rn(pp, make_float2(act[l], act[l + 1]));
+                pr[l] = pp.x;
+                pr[l + 1] = pp.y;
+                tot2 = __fadd2_rn(tot2, pp);
             }
+#pragma unroll
+            for (int j = 0; j < LM / 4; ++j) {
+                const float4 m0 = nib(lut, mk.a0, j), m1 = nib(lut, mk.a1, j);
+                const float2 p01 = make_float2(pr[4 * j], pr[4 * j + 1]), p23 = make_float2(pr[4 * j + 2], pr[4 * j + 3]);
+                q02 = __ffma2_rn(p01, make_float2(m0.x, m0.y), q02);
+                q02 = __ffma2_rn(p23, make_float2(m0.z, m0.w), q02);
+                q12 = __ffma2_rn(p01, make_float2(m1.x, m1.y), q12);
+                q12 = __ffma2_rn(p23, make_float2(m1.z, m1.w), q12);
+            }
+            const float tot = tot2.x + tot2.y, q0 = q02.x + q02.y, q1 = q12.x + q12.y;
             uint32_t pick;
             if (A.sampling == SI_SAMPLE_ARGMAX) {
-                const float thr = pmax * keep;
-                pick = LM;
+                float pmax = pr[0];
 #pragma unroll
-                for (int l = LM - 1; l >= 0; --l) pick = (pr[l] >= thr) ? (uint32_t)l : pick;
-                if (pick >= LM) pick = 0;
+                for (int l = 1; l < LM; ++l) pmax = fmaxf(pmax, pr[l]);
+                const float thr = pmax * keep;
+                pick = 0;
+#pragma unroll
+                for (int l = LM - 1; l >= 1; --l) pick = (pr[l] >= thr) ? (uint32_t)l : pick;
+                if (pr[0] >= thr) pick = 0;
             } else {
-                const float target = cell_uniform(A.seed, A.sid_base + s, m) * tot;
+                const float target = cell_uniform(A.seed, v.sid, v.m0 + m) * tot;
                 float cum = 0.f;
                 uint32_t last_nz = 0;
                 pick = LM;
@@ -399,39 +513,60 @@ __global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A, Tabs
                 }
                 if (pick == LM) pick = last_nz;
             }
-            const float inv = 1.0f / tot;
-            const uint64_t cell = (uint64_t)s * M + m;
-            if (A.dosage) A.dosage[cell] = (q0 + q1) * inv;
-            if (A.hprob) reinterpret_cast<float2*>(A.hprob)[cell] = make_float2(q0 * inv, q1 * inv);
-            if (A.haps) {
-                A.haps[(uint64_t)s * 2 * M + m] = (uint8_t)((mk.a0 >> pick) & 1u);
-                A.haps[(uint64_t)s * 2 * M + M + m] = (uint8_t)((mk.a1 >> pick) & 1u);
+            const float inv = __frcp_rn(tot);
+            sd[lane * kStageD + c] = (q0 + q1) * inv;
+            sh8[(lane * 2 + 0) * kStageH + c] = (uint8_t)((mk.a0 >> pick) & 1u);
+            sh8[(lane * 2 + 1) * kStageH + c] = (uint8_t)((mk.a1 >> pick) & 1u);
+            if (A.hprob) reinterpret_cast<float2*>(A.hprob)[v.out + m] = make_float2(q0 * inv, q1 * inv);
+        }
+        __syncwarp();
+        // flush: row r = the 32 cells thread r just staged
+        const int mine = (int)min(32u, ncells > cb ? ncells - cb : 0u);
+        for (int r = 0; r < 32; ++r) {
+            const int cnt = __shfl_sync(0xffffffffu, mine, r);
+            if (cnt <= 0) continue;
+            const unsigned long long out = __shfl_sync(0xffffffffu, (unsigned long long)v.out, r);
+            const uint32_t len = __shfl_sync(0xffffffffu, v.len, r);
+            const uint32_t m0 = __shfl_sync(0xffffffffu, cstart + cb, r);
+            if ((int)lane < cnt) {
+                if (A.dosage) A.dosage[out + m0 + lane] = sd[r * kStageD + lane];
+                if (A.haps) {
+                    A.haps[2 * out + m0 + lane] = sh8[(r * 2 + 0) * kStageH + lane];
+                    A.haps[2 * out + len + m0 + lane] = sh8[(r * 2 + 1) * kStageH + lane];
+                }
             }
         }
-        if (has_next) forward_step<LM>(tb, n, a, emission_mask(code[k + 1], A.masks[p1], lmask, &sh));
+        __syncwarp();
     }
 }
 
 template <int LM>
 size_t post_smem(uint32_t T, uint32_t C) {
-    return (size_t)C * LM * T * 4 + (size_t)C * T * 8;
+    return 256 + (size_t)C * LM * T * 4 + (size_t)C * T * 8 + (size_t)(T / 32) * 32 * kStageD * 4 +
+           (size_t)(T / 32) * 64 * kStageH;
 }
 
-template <int LM>
-cudaError_t launch_typed_lm(const TypedArgs& a, const Tabs& tb, cudaStream_t s) {
-    anchor_chain_kernel<LM><<<(a.B + 127) / 128, 128, 0, s>>>(a, tb);
-    cudaError_t e = cudaGetLastError();
-    if (e != cudaSuccess) return e;
-    if (a.ev_chain_done && (e = cudaEventRecord(a.ev_chain_done, s)) != cudaSuccess) return e;
+template <int LM, bool kFull>
+cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
     const uint32_t T = a.threads;
     const size_t sm = post_smem<LM>(T, a.C);
-    e = cudaFuncSetAttribute(anchor_posterior_kernel<LM>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    cudaError_t e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull>,
+                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
     if (e != cudaSuccess) return e;
     const unsigned long long grid = (a.total_windows + T - 1) / T;
     if (grid == 0) return cudaSuccess;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    anchor_posterior_kernel<LM><<<(uint32_t)grid, T, sm, s>>>(a, tb);
+    anchor_posterior_kernel<LM, kFull><<<(uint32_t)grid, T, sm, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int LM>
+cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
+    anchor_chain_kernel<LM><<<(a.B + 127) / 128, 128, 0, s>>>(a);
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return e;
+    if (a.ev_chain_done && (e = cudaEventRecord(a.ev_chain_done, s)) != cudaSuccess) return e;
+    return full ? launch_post<LM, true>(a, s) : launch_post<LM, false>(a, s);
 }
 
 }  // namespace
@@ -445,32 +580,27 @@ size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C) {
     }
 }
 
-cudaError_t launch_anchor_lists_count(const uint8_t* geno, uint32_t B, uint32_t M, uint32_t C, uint32_t* counts,
-                                      unsigned long long* aoff, unsigned long long* woff, cudaStream_t s) {
-    anchor_count_kernel<<<(B + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, s>>>(geno, B, M, counts);
+cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s) {
+    anchor_count_kernel<<<(a.B + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    anchor_scan_kernel<<<1, 1024, 0, s>>>(counts, B, C, aoff, woff);
+    anchor_scan_kernel<<<1, 1024, 0, s>>>(a.counts, a.B, a.C, a.aoff, a.woff);
     return cudaGetLastError();
 }
 
-cudaError_t launch_anchor_lists_fill(const uint8_t* geno, uint32_t B, uint32_t M, const unsigned long long* aoff,
-                                     const unsigned long long* woff, uint32_t* apos, uint8_t* acode, uint32_t* wsample,
-                                     cudaStream_t s) {
-    anchor_fill_kernel<<<(B + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, s>>>(
-        geno, B, M, aoff, woff, apos, acode, wsample);
+cudaError_t launch_anchor_lists_fill(const TypedArgs& a, cudaStream_t s) {
+    anchor_fill_kernel<<<(a.B + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
 
-cudaError_t launch_typed_fb(const TypedArgs& a, const TypedTables& t, cudaStream_t s) {
-    Tabs tb;
-    tb.Q = t.Q; tb.S = t.S; tb.G = t.G; tb.NT = t.NT; tb.log2q = t.log2q; tb.invL = t.invL;
-    tb.lr = t.lr; tb.lgc = t.lgc; tb.regime = t.regime;
-    switch (fb_lmax(a.L)) {
-        case 4: return launch_typed_lm<4>(a, tb, s);
-        case 8: return launch_typed_lm<8>(a, tb, s);
-        case 16: return launch_typed_lm<16>(a, tb, s);
-        default: return launch_typed_lm<32>(a, tb, s);
+// lmax: slots held per thread (every region's L <= lmax); the fast variant
+// runs when every region uses exactly lmax slots.
+cudaError_t launch_typed_fb(const TypedArgs& a, uint32_t lmax, bool all_full, cudaStream_t s) {
+    switch (lmax) {
+        case 4: return launch_typed_lm<4>(a, all_full, s);
+        case 8: return launch_typed_lm<8>(a, all_full, s);
+        case 16: return launch_typed_lm<16>(a, all_full, s);
+        default: return launch_typed_lm<32>(a, all_full, s);
     }
 }
 

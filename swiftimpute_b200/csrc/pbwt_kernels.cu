@@ -49,12 +49,21 @@ constexpr int kSweepThreads = 1024;
 //      pbwt_index.cpp:176-207 — and emit the row's outputs.
 // Two barriers per marker. perm arrays live in shared memory when they fit,
 // otherwise in the global scratch (L2-resident at these sizes).
+// Block b sweeps its own slice jobs[b] = {m0, len, head_off}: the order
+// restarts from iota at m0 (a region swept on its own, as the reference does
+// on a sliced panel). The whole-panel build is one job {0, M, 0}; only it may
+// also write the full prefix rows and row hashes.
 template <bool kSmemPerm>
 __global__ void __launch_bounds__(kSweepThreads, 1)
-pbwt_sweep_kernel(const uint32_t* __restrict__ panel, uint32_t M, uint32_t N, uint32_t W, uint32_t E,
-                  uint32_t* __restrict__ head, uint32_t* __restrict__ prefix,
-                  unsigned long long* __restrict__ row_hash, uint32_t* __restrict__ gperm) {
+pbwt_sweep_kernel(const uint32_t* __restrict__ panel_all, const SweepJob* __restrict__ jobs, uint32_t N, uint32_t W,
+                  uint32_t E, uint32_t* __restrict__ head_all, uint32_t* __restrict__ prefix,
+                  unsigned long long* __restrict__ row_hash, uint32_t* __restrict__ gperm_all) {
     extern __shared__ __align__(16) uint32_t smem[];
+    const SweepJob job = jobs[blockIdx.x];
+    const uint32_t* panel = panel_all + (uint64_t)job.m0 * W;
+    const uint32_t M = job.len;
+    uint32_t* head = head_all + job.head_off;
+    uint32_t* gperm = kSmemPerm ? nullptr : gperm_all + (uint64_t)blockIdx.x * 2 * N;
     uint32_t* rows = smem;                       // [2][W]
     uint32_t* wsum = rows + 2 * W;               // [2][32]
     uint32_t* perm_base = kSmemPerm ? (wsum + 64) : gperm;
@@ -69,11 +78,22 @@ pbwt_sweep_kernel(const uint32_t* __restrict__ panel, uint32_t M, uint32_t N, ui
     for (uint32_t i = t; i < W; i += blockDim.x) rows[i] = panel[i];
     __syncthreads();
 
+    // the next marker's row is loaded into registers at the top of a step and
+    // written to the other shared buffer after the scatter, so the load's
+    // latency overlaps the step instead of stalling it
+    constexpr uint32_t kRowRegs = 4;
     for (uint32_t m = 0; m < M; ++m) {
         const uint32_t* row = rows + (m & 1) * W;
-        // prefetch the next marker's row into the other buffer
-        if (m + 1 < M)
-            for (uint32_t i = t; i < W; i += blockDim.x) rows[((m + 1) & 1) * W + i] = panel[(uint64_t)(m + 1) * W + i];
+        uint32_t nxt_words[kRowRegs];
+        if (m + 1 < M) {
+#pragma unroll
+            for (uint32_t r = 0; r < kRowRegs; ++r) {
+                const uint32_t i = t + r * blockDim.x;
+                nxt_words[r] = (i < W) ? __ldg(panel + (uint64_t)(m + 1) * W + i) : 0u;
+            }
+            for (uint32_t i = t + kRowRegs * blockDim.x; i < W; i += blockDim.x)  // rows wider than the registers
+                rows[((m + 1) & 1) * W + i] = panel[(uint64_t)(m + 1) * W + i];
+        }
 
         uint32_t n_own = 0;
         if (beg < N) n_own = min(E, N - beg);
@@ -124,6 +144,13 @@ pbwt_sweep_kernel(const uint32_t* __restrict__ panel, uint32_t M, uint32_t N, ui
             for (int o = 16; o > 0; o >>= 1) hacc += __shfl_xor_sync(0xffffffffu, hacc, o);
             if (lane == 0) atomicAdd(row_hash + m, hacc);
         }
+        if (m + 1 < M) {
+#pragma unroll
+            for (uint32_t r = 0; r < kRowRegs; ++r) {
+                const uint32_t i = t + r * blockDim.x;
+                if (i < W) rows[((m + 1) & 1) * W + i] = nxt_words[r];
+            }
+        }
         __syncthreads();
         uint32_t* tmp = cur; cur = nxt; nxt = tmp;
     }
@@ -145,11 +172,13 @@ size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W) {
     return (size_t)(2 * W + 64) * 4 + (size_t)2 * N * 4;
 }
 
-// Single-CTA sweep; head must be zero-filled for rows shorter than kHead.
-cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_head,
-                              uint32_t* d_prefix, unsigned long long* d_hash, uint32_t* d_perm_scratch,
-                              cudaStream_t s) {
-    const uint32_t T = kSweepThreads;
+// One CTA per job (device array d_jobs[n_jobs]); head must be zero-filled for
+// rows shorter than kHead; d_perm_scratch holds 2 N words per job.
+cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, uint32_t n_jobs, uint32_t N,
+                              uint32_t W, uint32_t* d_head, uint32_t* d_prefix, unsigned long long* d_hash,
+                              uint32_t* d_perm_scratch, cudaStream_t s) {
+    uint32_t T = ((N + 8 * 32 - 1) / (8 * 32)) * 32;  // ~8 entries per thread
+    T = T < 128 ? 128 : (T > kSweepThreads ? kSweepThreads : T);
     const uint32_t E = (N + T - 1) / T;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
@@ -159,13 +188,14 @@ cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, uint32_t M, uint32_t N, u
         cudaError_t e = cudaFuncSetAttribute(pbwt_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)full);
         if (e != cudaSuccess) return e;
-        pbwt_sweep_kernel<true><<<1, T, full, s>>>(d_panel, M, N, W, E, d_head, d_prefix, d_hash, nullptr);
+        pbwt_sweep_kernel<true><<<n_jobs, T, full, s>>>(d_panel, d_jobs, N, W, E, d_head, d_prefix, d_hash, nullptr);
     } else {
         const size_t small = (size_t)(2 * W + 64) * 4;
         cudaError_t e = cudaFuncSetAttribute(pbwt_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              (int)small);
         if (e != cudaSuccess) return e;
-        pbwt_sweep_kernel<false><<<1, T, small, s>>>(d_panel, M, N, W, E, d_head, d_prefix, d_hash, d_perm_scratch);
+        pbwt_sweep_kernel<false><<<n_jobs, T, small, s>>>(d_panel, d_jobs, N, W, E, d_head, d_prefix, d_hash,
+                                                           d_perm_scratch);
     }
     return cudaGetLastError();
 }

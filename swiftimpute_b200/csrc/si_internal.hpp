@@ -7,6 +7,7 @@
 
 #include <cstdint>
 #include <map>
+#include <tuple>
 #include <string>
 #include <utility>
 #include <vector>
@@ -35,6 +36,13 @@ struct SlotMasks {
 struct LinTrans {
     float c;
     float delta;
+};
+
+// A PBWT sweep over panel rows [m0, m0 + len), head rows written at head + head_off.
+struct SweepJob {
+    uint32_t m0;
+    uint32_t len;
+    uint64_t head_off;
 };
 
 struct DeviceBuffer {
@@ -85,10 +93,18 @@ struct si_ctx {
     si::LinTrans trans0{1.f, 0.f};  // host copy of the first gap's transition
     si::DeviceBuffer ckpt;           // forward checkpoints (full-chain kernel)
     // typed-marker kernel scratch and tables
-    si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_wsample, t_ckF, t_ckB, t_ckU;
-    si::DeviceBuffer tab_Q, tab_S, tab_G;
-    uint64_t tab_key = ~0ull;
-    double tab_consts[4] = {0, 0, 0, 0};  // log2q, lr, lgc, regime
+    si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_aem, t_wsample, t_ckF, t_ckB, t_ckU;
+    struct TableSet {
+        si::DeviceBuffer Q, S, G;
+        double consts[4] = {0, 0, 0, 0};  // log2q, lr, lgc, regime
+    };
+    std::map<uint64_t, TableSet> tables;  // closed-form run tables per (transition, L)
+    // region-local selection tables (index restarted at the region start), per (m_begin, m_end, L, kind)
+    struct RegionSel {
+        si::DeviceBuffer masks;
+    };
+    std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, RegionSel> region_sel;
+    si::DeviceBuffer job_regions, job_samples;  // uploaded descriptors of the last uneven batch
     unsigned long long* pinned_totals = nullptr;
     si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
     float last_ms[3] = {0.f, 0.f, 0.f};
@@ -108,9 +124,9 @@ si_status cuda_fail(si_ctx* ctx, cudaError_t e, const char* what);
 // Kernel launchers (pbwt_kernels.cu, select_kernels.cu, fb_kernels.cu).
 cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,
                               uint32_t* d_bad, cudaStream_t s);
-cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_head,
-                              uint32_t* d_prefix, unsigned long long* d_hash, uint32_t* d_perm_scratch,
-                              cudaStream_t s);
+cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, uint32_t n_jobs, uint32_t N,
+                              uint32_t W, uint32_t* d_head, uint32_t* d_prefix, unsigned long long* d_hash,
+                              uint32_t* d_perm_scratch, cudaStream_t s);
 size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W);
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
                           uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, cudaStream_t s);

@@ -133,6 +133,44 @@ class Engine:
                                               c_void_p(d_haps) if d_haps else None,
                                               c_void_p(stream) if stream else None))
 
+    def impute_jobs(self, regions, jobs, params: N.ImputeParams | None = None, *, hap_prob: bool = False,
+                    stream: int | None = None):
+        """Uneven batch. ``regions``: list of (m_begin, m_end, L, index_origin);
+        ``jobs``: list of (region, codes[len] u8, sample_id). Outputs are packed per
+        job; returns a list of dicts (dosage [len], haps [2][len], hap_prob [len][2]).
+        Device buffers are allocated with torch (plumbing only)."""
+        import torch
+        params = params or N.default_params()
+        R = (N.Region * len(regions))(*[N.Region(a, b, L, o) for a, b, L, o in regions])
+        lens = [max(0, regions[r][1] - regions[r][0]) if 0 <= r < len(regions) else 0 for r, _, _ in jobs]
+        offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        J = (N.Job * len(jobs))(*[N.Job(r, 0, int(offs[i]), int(offs[i]), int(sid))
+                                  for i, (r, _, sid) in enumerate(jobs)])
+        total = max(1, int(offs[-1]))
+        geno = np.concatenate([np.asarray(c, dtype=np.uint8) for _, c, _ in jobs] + [np.zeros(1, np.uint8)])
+        dev = torch.device("cuda", 0)
+        d_geno = torch.from_numpy(geno).to(dev)
+        d_dos = torch.empty(total, dtype=torch.float32, device=dev)
+        d_haps = torch.empty(2 * total, dtype=torch.uint8, device=dev)
+        d_hp = torch.empty(2 * total, dtype=torch.float32, device=dev) if hap_prob else None
+        torch.cuda.synchronize(dev)
+        self._check(self.lib.si_impute_jobs_device(self.h, byref(params), R, len(regions), J, len(jobs),
+                                                   c_void_p(d_geno.data_ptr()), c_void_p(d_dos.data_ptr()),
+                                                   c_void_p(d_hp.data_ptr()) if hap_prob else None,
+                                                   c_void_p(d_haps.data_ptr()),
+                                                   c_void_p(stream) if stream else None))
+        torch.cuda.synchronize(dev)
+        dos, haps = d_dos.cpu().numpy(), d_haps.cpu().numpy()
+        hp = d_hp.cpu().numpy() if hap_prob else None
+        out = []
+        for i in range(len(jobs)):
+            a, n = int(offs[i]), lens[i]
+            o = {"dosage": dos[a:a + n], "haps": haps[2 * a:2 * a + 2 * n].reshape(2, n)}
+            if hap_prob:
+                o["hap_prob"] = hp[2 * a:2 * a + 2 * n].reshape(n, 2)
+            out.append(o)
+        return out
+
     def last_kernel_ms(self) -> tuple[float, float, float, float]:
         """(selection, typed-marker lists, anchor chain, posterior or full-chain kernel) in ms."""
         ms = (c_float * 4)()
