@@ -176,6 +176,25 @@ si_status si_impute_gl(si_ctx* ctx, const si_impute_params* p, const float* gl, 
 si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
                            float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
 
+/* Allocation-free variant of si_impute_device for callers that cannot call
+ * cudaMalloc while they impute: code inside CUDA stream capture, where an
+ * allocation synchronises the device and breaks the capture, and programs
+ * whose device memory belongs to another allocator (a framework's pool). It
+ * has no counterpart in the reference. The caller passes device inputs and
+ * outputs; the forward checkpoints live in a fixed 16 MiB array inside the
+ * library (held by every GPU that loads it, until exit). Needs B * ceil(M/C - 1)
+ * * Lmax * 4 bytes of checkpoints (C = 32 markers, 16 for L > 16; Lmax = L
+ * rounded up to 4/8/16/32) within that limit, else SI_ERR_UNSUPPORTED. The
+ * ctx must hold the slot and transition tables for these parameters: make one
+ * allocating call (si_impute or si_impute_device) with them first, and let it
+ * complete. Its first call on a device is its set-up: it looks up the
+ * array's device address (with lazy module loading, that is also when the
+ * driver commits the array's memory); make that call before any stream
+ * capture. Calls share the array, so calls
+ * whose kernels overlap on the GPU race; serialise them on one stream. */
+si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
+                                   float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
+
 /* Uneven batches ----------------------------------------------------------
  * One launch sequence over targets that cover different marker ranges
  * (regions) with different slot counts. A region is a contiguous panel slice

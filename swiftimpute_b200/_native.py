@@ -95,6 +95,8 @@ SIGNATURES = [
     ("si_impute_jobs_device", c_int,
      [c_void_p, POINTER(ImputeParams), POINTER(Region), c_uint32, POINTER(Job), c_uint32, c_void_p, c_void_p,
       c_void_p, c_void_p, c_void_p]),
+    ("si_impute_device_noalloc", c_int,
+     [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("si_last_timings", c_int, [c_void_p, POINTER(c_float)]),
     ("si_last_kernel_ms", c_int, [c_void_p, POINTER(c_float)]),
 ]
