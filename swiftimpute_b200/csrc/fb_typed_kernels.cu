@@ -92,13 +92,36 @@ __device__ __forceinline__ double tabG(const Tabs& t, uint32_t n) {
 
 constexpr uint32_t kWarpsPerBlock = 8;
 
+// 16 consecutive codes per lane: bit j set when code j < 3 (typed).
+__device__ __forceinline__ uint32_t typed_bits16(const uint8_t* g, uint32_t base, uint32_t len, bool vec) {
+    uint32_t bits = 0;
+    if (vec && base + 16 <= len) {
+        const uint4 w = *reinterpret_cast<const uint4*>(g + base);
+        const uint32_t ww[4] = {w.x, w.y, w.z, w.w};
+#pragma unroll
+        for (int q = 0; q < 4; ++q) {
+            const uint32_t lt = __vcmpltu4(ww[q], 0x03030303u);  // 0xff in each byte below 3
+#pragma unroll
+            for (int b = 0; b < 4; ++b) bits |= ((lt >> (8 * b + 7)) & 1u) << (4 * q + b);
+        }
+    } else {
+        for (uint32_t j = 0; j < 16 && base + j < len; ++j) bits |= (g[base + j] < 3 ? 1u : 0u) << j;
+    }
+    return bits;
+}
+
 __global__ void anchor_count_kernel(TypedArgs A) {
     const uint32_t s = blockIdx.x * kWarpsPerBlock + (threadIdx.x >> 5);
     const uint32_t lane = threadIdx.x & 31;
     if (s >= A.B) return;
     const View v = view_of(A, s);
+    const bool vec = (reinterpret_cast<uintptr_t>(v.geno) & 15u) == 0;
     uint32_t n = 0;
-    for (uint32_t m = lane; m < v.len; m += 32) n += (m == 0 || v.geno[m] < 3) ? 1u : 0u;
+    for (uint32_t base = lane * 16; base < v.len; base += 512) {
+        uint32_t bits = typed_bits16(v.geno, base, v.len, vec);
+        if (base == 0) bits |= 1u;  // marker 0 is always an anchor
+        n += __popc(bits);
+    }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
     if (lane == 0) A.counts[s] = n;
@@ -154,24 +177,31 @@ __global__ void anchor_fill_kernel(TypedArgs A) {
     if (s >= A.B) return;
     const View v = view_of(A, s);
     const uint32_t lmask = lmask_of(v.r.L);
+    const bool vec = (reinterpret_cast<uintptr_t>(v.geno) & 15u) == 0;
     unsigned long long o = A.aoff[s];
-    for (uint32_t m0 = 0; m0 < v.len; m0 += 32) {
-        const uint32_t m = m0 + lane;
-        uint8_t g = 3;
-        bool a = false;
-        if (m < v.len) {
-            g = v.geno[m];
-            a = (m == 0) || g < 3;
+    for (uint32_t b0 = 0; b0 < v.len; b0 += 512) {
+        const uint32_t base = b0 + lane * 16;
+        uint32_t bits = base < v.len ? typed_bits16(v.geno, base, v.len, vec) : 0u;
+        if (base == 0) bits |= 1u;
+        const uint32_t cnt = __popc(bits);
+        uint32_t incl = cnt;
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            const uint32_t y = __shfl_up_sync(0xffffffffu, incl, d);
+            if (lane >= (uint32_t)d) incl += y;
         }
-        const uint32_t bal = __ballot_sync(0xffffffffu, a);
-        if (a) {
-            const unsigned long long at = o + __popc(bal & ((1u << lane) - 1u));
+        unsigned long long at = o + incl - cnt;
+        while (bits) {
+            const uint32_t j = __ffs(bits) - 1;
+            bits &= bits - 1;
+            const uint32_t m = base + j;
             uint32_t sh;
             A.apos[at] = m;
-            A.aem[at] = emission_mask(g, v.r.masks[m], lmask, &sh);
+            A.aem[at] = emission_mask(v.geno[m], v.r.masks[m], lmask, &sh);
             A.ashift[at] = (uint8_t)sh;
+            ++at;
         }
-        o += __popc(bal);
+        o += __shfl_sync(0xffffffffu, incl, 31);
     }
     for (unsigned long long w = A.woff[s] + lane; w < A.woff[s + 1]; w += 32) A.wsample[w] = s;
 }
@@ -245,9 +275,13 @@ __device__ __forceinline__ void init_forward(float (&a)[LM], uint32_t em) {
 
 constexpr int kPrefetch = 8;  // anchors whose list entries are loaded ahead of the chain step
 
+// A CTA of 128 threads serves 64 samples: warps 0-1 run their forward chains
+// and warps 2-3 their backward chains at the same time (the two directions
+// are independent). Anchor entries are loaded one group of kPrefetch ahead.
 template <int LM>
 __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
-    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t s = blockIdx.x * 64 + (threadIdx.x & 63);
+    const bool forward = threadIdx.x < 64;
     if (s >= A.B) return;
     const View v = view_of(A, s);
     const Tabs& tb = v.r.tabs;
@@ -256,65 +290,85 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
     const uint32_t* aem = A.aem + base;
     const uint8_t* ash = A.ashift + base;
     const uint32_t C = A.C;
-    // forward: the list entries of kPrefetch anchors are loaded before their steps run
-    float a[LM];
-    init_forward<LM>(a, aem[0]);
-    forward_step<LM>(tb, 0, a, 0xffffffffu);  // normalise
+    if (forward) {
+        float a[LM];
+        init_forward<LM>(a, aem[0]);
+        forward_step<LM>(tb, 0, a, 0xffffffffu);  // normalise
 #pragma unroll
-    for (int k = 0; k < LM; ++k) A.ckptF[wb * LM + k] = a[k];
-    uint32_t prev = pos[0];
-    for (unsigned long long k0 = 1; k0 < NA; k0 += kPrefetch) {
+        for (int k = 0; k < LM; ++k) A.ckptF[wb * LM + k] = a[k];
+        uint32_t prev = pos[0];
         uint32_t pp[kPrefetch], ee[kPrefetch];
 #pragma unroll
         for (int j = 0; j < kPrefetch; ++j) {
-            const unsigned long long k = k0 + j;
+            const unsigned long long k = 1 + j;
             pp[j] = k < NA ? pos[k] : 0u;
             ee[j] = k < NA ? aem[k] : 0u;
         }
+        for (unsigned long long k0 = 1; k0 < NA; k0 += kPrefetch) {
+            uint32_t pn[kPrefetch], en[kPrefetch];
 #pragma unroll
-        for (int j = 0; j < kPrefetch; ++j) {
-            const unsigned long long k = k0 + j;
-            if (k < NA) {
-                forward_step<LM>(tb, pp[j] - prev, a, ee[j]);
-                prev = pp[j];
-                if (k % C == 0)
-#pragma unroll
-                    for (int l = 0; l < LM; ++l) A.ckptF[(wb + k / C) * LM + l] = a[l];
+            for (int j = 0; j < kPrefetch; ++j) {  // next group, in flight during this one
+                const unsigned long long k = k0 + kPrefetch + j;
+                pn[j] = k < NA ? pos[k] : 0u;
+                en[j] = k < NA ? aem[k] : 0u;
             }
-        }
-    }
-    // backward
-    float w[LM];
-    uint32_t nextp = pos[NA - 1];
-    double logU = chain_end_logU(tb, v.len - 1 - nextp);
-    init_forward<LM>(w, aem[NA - 1]);
-    logU -= 999.0 * (double)ash[NA - 1];
-    if ((NA - 1) % C == 0) {
 #pragma unroll
-        for (int l = 0; l < LM; ++l) A.ckptB[(wb + (NA - 1) / C) * LM + l] = w[l];
-        A.ckptU[wb + (NA - 1) / C] = logU;
-    }
-    for (long long k0 = (long long)NA - 2; k0 >= 0; k0 -= kPrefetch) {
+            for (int j = 0; j < kPrefetch; ++j) {
+                const unsigned long long k = k0 + j;
+                if (k < NA) {
+                    forward_step<LM>(tb, pp[j] - prev, a, ee[j]);
+                    prev = pp[j];
+                    if (k % C == 0)
+#pragma unroll
+                        for (int l = 0; l < LM; ++l) A.ckptF[(wb + k / C) * LM + l] = a[l];
+                }
+            }
+#pragma unroll
+            for (int j = 0; j < kPrefetch; ++j) { pp[j] = pn[j]; ee[j] = en[j]; }
+        }
+    } else {
+        float w[LM];
+        uint32_t nextp = pos[NA - 1];
+        double logU = chain_end_logU(tb, v.len - 1 - nextp);
+        init_forward<LM>(w, aem[NA - 1]);
+        logU -= 999.0 * (double)ash[NA - 1];
+        if ((NA - 1) % C == 0) {
+#pragma unroll
+            for (int l = 0; l < LM; ++l) A.ckptB[(wb + (NA - 1) / C) * LM + l] = w[l];
+            A.ckptU[wb + (NA - 1) / C] = logU;
+        }
         uint32_t pp[kPrefetch], ee[kPrefetch], hh[kPrefetch];
 #pragma unroll
         for (int j = 0; j < kPrefetch; ++j) {
-            const long long k = k0 - j;
+            const long long k = (long long)NA - 2 - j;
             pp[j] = k >= 0 ? pos[k] : 0u;
             ee[j] = k >= 0 ? aem[k] : 0u;
             hh[j] = k >= 0 ? ash[k] : 0u;
         }
+        for (long long k0 = (long long)NA - 2; k0 >= 0; k0 -= kPrefetch) {
+            uint32_t pn[kPrefetch], en[kPrefetch], hn[kPrefetch];
 #pragma unroll
-        for (int j = 0; j < kPrefetch; ++j) {
-            const long long k = k0 - j;
-            if (k >= 0) {
-                backward_step<LM>(tb, nextp - pp[j], w, logU, ee[j], hh[j], 0u);
-                nextp = pp[j];
-                if (k % C == 0) {
+            for (int j = 0; j < kPrefetch; ++j) {
+                const long long k = k0 - kPrefetch - j;
+                pn[j] = k >= 0 ? pos[k] : 0u;
+                en[j] = k >= 0 ? aem[k] : 0u;
+                hn[j] = k >= 0 ? ash[k] : 0u;
+            }
 #pragma unroll
-                    for (int l = 0; l < LM; ++l) A.ckptB[(wb + k / C) * LM + l] = w[l];
-                    A.ckptU[wb + k / C] = logU;
+            for (int j = 0; j < kPrefetch; ++j) {
+                const long long k = k0 - j;
+                if (k >= 0) {
+                    backward_step<LM>(tb, nextp - pp[j], w, logU, ee[j], hh[j], 0u);
+                    nextp = pp[j];
+                    if (k % C == 0) {
+#pragma unroll
+                        for (int l = 0; l < LM; ++l) A.ckptB[(wb + k / C) * LM + l] = w[l];
+                        A.ckptU[wb + k / C] = logU;
+                    }
                 }
             }
+#pragma unroll
+            for (int j = 0; j < kPrefetch; ++j) { pp[j] = pn[j]; ee[j] = en[j]; hh[j] = hn[j]; }
         }
     }
 }
@@ -562,7 +616,7 @@ cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
 
 template <int LM>
 cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
-    anchor_chain_kernel<LM><<<(a.B + 127) / 128, 128, 0, s>>>(a);
+    anchor_chain_kernel<LM><<<(a.B + 63) / 64, 128, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (a.ev_chain_done && (e = cudaEventRecord(a.ev_chain_done, s)) != cudaSuccess) return e;

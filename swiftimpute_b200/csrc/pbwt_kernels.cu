@@ -53,7 +53,10 @@ constexpr int kSweepThreads = 1024;
 // restarts from iota at m0 (a region swept on its own, as the reference does
 // on a sliced panel). The whole-panel build is one job {0, M, 0}; only it may
 // also write the full prefix rows and row hashes.
-template <bool kSmemPerm>
+// kE > 0: each thread holds its (at most kE) entries and their bits in
+// registers, loaded with independent shared-memory reads; kE = 0: any number
+// of entries, re-read in the scatter pass.
+template <bool kSmemPerm, int kE>
 __global__ void __launch_bounds__(kSweepThreads, 1)
 pbwt_sweep_kernel(const uint32_t* __restrict__ panel_all, const SweepJob* __restrict__ jobs, uint32_t N, uint32_t W,
                   uint32_t E, uint32_t* __restrict__ head_all, uint32_t* __restrict__ prefix,
@@ -99,9 +102,20 @@ pbwt_sweep_kernel(const uint32_t* __restrict__ panel_all, const SweepJob* __rest
         if (beg < N) n_own = min(E, N - beg);
         // pass 1: zero count of the owned entries
         uint32_t z = 0;
-        for (uint32_t i = 0; i < n_own; ++i) {
-            const uint32_t v = cur[beg + i];
-            z += ((row[v >> 5] >> (v & 31)) & 1u) ^ 1u;
+        uint32_t hv[kE > 0 ? kE : 1];
+        uint32_t ones = 0;
+        if (kE > 0) {
+#pragma unroll
+            for (int i = 0; i < kE; ++i) hv[i] = (uint32_t)i < n_own ? cur[beg + i] : 0u;
+#pragma unroll
+            for (int i = 0; i < kE; ++i)
+                if ((uint32_t)i < n_own) ones |= ((row[hv[i] >> 5] >> (hv[i] & 31)) & 1u) << i;
+            z = n_own - __popc(ones);
+        } else {
+            for (uint32_t i = 0; i < n_own; ++i) {
+                const uint32_t v = cur[beg + i];
+                z += ((row[v >> 5] >> (v & 31)) & 1u) ^ 1u;
+            }
         }
 
         // warp inclusive scan of zero counts
@@ -131,13 +145,27 @@ pbwt_sweep_kernel(const uint32_t* __restrict__ panel_all, const SweepJob* __rest
         uint32_t* out_row = prefix ? prefix + (uint64_t)m * N : nullptr;
         uint32_t* head_row = head + (uint64_t)m * kHead;
         // pass 2: stable scatter
-        for (uint32_t i = 0; i < n_own; ++i) {
-            const uint32_t v = cur[beg + i];
-            const uint32_t pos = ((row[v >> 5] >> (v & 31)) & 1u) ? (total_zeros + ob++) : zb++;
-            nxt[pos] = v;
-            if (out_row) out_row[pos] = v;
-            if (pos < kHead) head_row[pos] = v;
-            if (row_hash) hacc += mix_entry(v, pos);
+        if (kE > 0) {
+#pragma unroll
+            for (int i = 0; i < kE; ++i) {
+                if ((uint32_t)i < n_own) {
+                    const uint32_t v = hv[i];
+                    const uint32_t pos = ((ones >> i) & 1u) ? (total_zeros + ob++) : zb++;
+                    nxt[pos] = v;
+                    if (out_row) out_row[pos] = v;
+                    if (pos < kHead) head_row[pos] = v;
+                    if (row_hash) hacc += mix_entry(v, pos);
+                }
+            }
+        } else {
+            for (uint32_t i = 0; i < n_own; ++i) {
+                const uint32_t v = cur[beg + i];
+                const uint32_t pos = ((row[v >> 5] >> (v & 31)) & 1u) ? (total_zeros + ob++) : zb++;
+                nxt[pos] = v;
+                if (out_row) out_row[pos] = v;
+                if (pos < kHead) head_row[pos] = v;
+                if (row_hash) hacc += mix_entry(v, pos);
+            }
         }
         if (row_hash) {
 #pragma unroll
@@ -177,26 +205,31 @@ size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W) {
 cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, uint32_t n_jobs, uint32_t N,
                               uint32_t W, uint32_t* d_head, uint32_t* d_prefix, unsigned long long* d_hash,
                               uint32_t* d_perm_scratch, cudaStream_t s) {
-    uint32_t T = ((N + 8 * 32 - 1) / (8 * 32)) * 32;  // ~8 entries per thread
+    uint32_t T = ((N + 4 * 32 - 1) / (4 * 32)) * 32;  // ~4 entries per thread, 128..1024 threads
     T = T < 128 ? 128 : (T > kSweepThreads ? kSweepThreads : T);
     const uint32_t E = (N + T - 1) / T;
     int dev = 0, max_optin = 0;
     cudaGetDevice(&dev);
     cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, dev);
     const size_t full = pbwt_sweep_smem_bytes(N, W);
-    if (full <= (size_t)max_optin) {
-        cudaError_t e = cudaFuncSetAttribute(pbwt_sweep_kernel<true>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)full);
+    auto go = [&](auto kernel, size_t smem, uint32_t* gp) -> cudaError_t {
+        cudaError_t e = cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
         if (e != cudaSuccess) return e;
-        pbwt_sweep_kernel<true><<<n_jobs, T, full, s>>>(d_panel, d_jobs, N, W, E, d_head, d_prefix, d_hash, nullptr);
+        kernel<<<n_jobs, T, smem, s>>>(d_panel, d_jobs, N, W, E, d_head, d_prefix, d_hash, gp);
+        return cudaSuccess;
+    };
+    cudaError_t e;
+    if (full <= (size_t)max_optin) {
+        e = E <= 4 ? go(pbwt_sweep_kernel<true, 4>, full, nullptr)
+          : E <= 8 ? go(pbwt_sweep_kernel<true, 8>, full, nullptr)
+          : E <= 16 ? go(pbwt_sweep_kernel<true, 16>, full, nullptr)
+                    : go(pbwt_sweep_kernel<true, 0>, full, nullptr);
     } else {
         const size_t small = (size_t)(2 * W + 64) * 4;
-        cudaError_t e = cudaFuncSetAttribute(pbwt_sweep_kernel<false>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             (int)small);
-        if (e != cudaSuccess) return e;
-        pbwt_sweep_kernel<false><<<n_jobs, T, small, s>>>(d_panel, d_jobs, N, W, E, d_head, d_prefix, d_hash,
-                                                           d_perm_scratch);
+        e = E <= 16 ? go(pbwt_sweep_kernel<false, 16>, small, d_perm_scratch)
+                    : go(pbwt_sweep_kernel<false, 0>, small, d_perm_scratch);
     }
+    if (e != cudaSuccess) return e;
     return cudaGetLastError();
 }
 
