@@ -201,7 +201,7 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
     std::memcpy(&key, &t0, 8);
     key = key * 0x9E3779B97F4A7C15ull ^ (uint64_t)L;
     auto& ts = ctx->tables[key];
-    if (!ts.Q.ptr) {
+    if (!ts.QS.ptr) {
         const double c = (double)t0.c, dl = (double)t0.delta;
         const double rho = dl + (double)L * c;
         const double q = dl / rho;
@@ -209,35 +209,33 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
         const double lr = std::log(rho);
         const int regime = std::fabs(rho - 1.0) < 1e-15 ? 2 : (rho < 1.0 ? 0 : 1);
         const double lgc = regime == 0 ? std::log1p(-rho) : (regime == 1 ? std::log(rho - 1.0) : 0.0);
-        std::vector<float> Q(kTabN), S(kTabN);
+        std::vector<float> QS(2 * kTabN);
         std::vector<double> G(kTabN);
         for (uint32_t n = 0; n < kTabN; ++n) {
             const double qn = (n == 0) ? 1.0 : (q > 0.0 ? std::exp((double)n * lq) : 0.0);
             const double om = (n == 0) ? 0.0 : (q > 0.0 ? -std::expm1((double)n * lq) : 1.0);
-            Q[n] = (float)qn;
-            S[n] = (float)(om / (double)L);
+            QS[2 * n] = (float)qn;
+            QS[2 * n + 1] = (float)(om / (double)L);
             if (n == 0) G[n] = -INFINITY;
             else if (regime == 0) G[n] = -(double)n * lr + std::log(-std::expm1((double)n * lr)) - lgc;
             else if (regime == 1) G[n] = std::log(-std::expm1(-(double)n * lr)) - lgc;
             else G[n] = std::log((double)n);
         }
-        si_status st = dev_alloc(ctx, ts.Q, kTabN * 4);
-        if (st == SI_OK) st = dev_alloc(ctx, ts.S, kTabN * 4);
+        si_status st = dev_alloc(ctx, ts.QS, kTabN * 8);
         if (st == SI_OK) st = dev_alloc(ctx, ts.G, kTabN * 8);
         if (st != SI_OK) {
-            dev_free(ctx, ts.Q); dev_free(ctx, ts.S); dev_free(ctx, ts.G);
+            dev_free(ctx, ts.QS); dev_free(ctx, ts.G);
             ctx->tables.erase(key);
             return st;
         }
-        SI_CUDA(ctx, cudaMemcpy(ts.Q.ptr, Q.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
-        SI_CUDA(ctx, cudaMemcpy(ts.S.ptr, S.data(), kTabN * 4, cudaMemcpyHostToDevice), "copy tables");
+        SI_CUDA(ctx, cudaMemcpy(ts.QS.ptr, QS.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
         SI_CUDA(ctx, cudaMemcpy(ts.G.ptr, G.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
         ts.consts[0] = q > 0.0 ? std::log2(q) : -INFINITY;
         ts.consts[1] = lr;
         ts.consts[2] = lgc;
         ts.consts[3] = regime;
     }
-    out->Q = (const float*)ts.Q.ptr; out->S = (const float*)ts.S.ptr; out->G = (const double*)ts.G.ptr;
+    out->QS = (const float2*)ts.QS.ptr; out->G = (const double*)ts.G.ptr;
     out->NT = kTabN; out->log2q = (float)ts.consts[0]; out->invL = 1.0f / (float)L;
     out->lr = ts.consts[1]; out->lgc = ts.consts[2]; out->regime = (int)ts.consts[3];
     return SI_OK;
@@ -248,8 +246,8 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
 // chain, posterior. Waits once on `s` for the 16-byte list totals.
 si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32_t lmax, bool all_full,
                     cudaStream_t s) {
-    a.C = p->checkpoint_interval ? p->checkpoint_interval : 8;
-    a.threads = p->block_threads ? p->block_threads : 128;
+    a.C = p->checkpoint_interval ? p->checkpoint_interval : typed_default_window(lmax);
+    a.threads = p->block_threads ? p->block_threads : typed_default_threads(lmax);
     if (typed_post_smem_bytes(lmax, a.threads, a.C) > 227u * 1024u)
         return fail(ctx, SI_ERR_UNSUPPORTED, "posterior tile needs more than 227 KB of shared memory");
     if (!ctx->pinned_totals)
@@ -416,8 +414,7 @@ si_status si_ctx_destroy(si_ctx* ctx) {
                                 &ctx->job_samples})
         dev_free(ctx, *b);
     for (auto& kv : ctx->tables) {
-        dev_free(ctx, kv.second.Q);
-        dev_free(ctx, kv.second.S);
+        dev_free(ctx, kv.second.QS);
         dev_free(ctx, kv.second.G);
     }
     for (auto& kv : ctx->region_sel) dev_free(ctx, kv.second.masks);

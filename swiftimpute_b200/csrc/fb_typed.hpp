@@ -6,10 +6,9 @@ namespace si {
 
 // Closed-form coefficients for runs of untyped markers under one transition
 // (c, delta), computed in FP64 on the host: q = delta / rho, rho = delta + L c,
-// Q[n] = q^n, S[n] = (1 - q^n) / L, G[n] = log sum_{k=1..n} rho^-k.
+// QS[n] = {Q[n], S[n]} = {q^n, (1 - q^n) / L}, G[n] = log sum_{k=1..n} rho^-k.
 struct TypedTables {
-    const float* Q;
-    const float* S;
+    const float2* QS;
     const double* G;
     uint32_t NT;
     float log2q;
@@ -70,5 +69,7 @@ cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s);
 cudaError_t launch_anchor_lists_fill(const TypedArgs& a, cudaStream_t s);
 cudaError_t launch_typed_fb(const TypedArgs& a, uint32_t lmax, bool all_full, cudaStream_t s);
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C);
+uint32_t typed_default_window(uint32_t lmax);   // anchors per window when the caller gives none
+uint32_t typed_default_threads(uint32_t lmax);  // posterior CTA size when the caller gives none
 
 }  // namespace si

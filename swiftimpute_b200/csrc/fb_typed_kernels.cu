@@ -15,11 +15,11 @@
 // per-cell work runs in parallel. Kernels:
 //   anchor_count / anchor_scan / anchor_fill   per-sample anchor lists (marker 0
 //                                              is always an anchor)
-//   anchor_chain     one thread per sample: forward and backward over anchors,
-//                    checkpoints every C anchors
-//   anchor_posterior one thread per (sample, window of C anchors): rebuilds the
-//                    window's anchors from the checkpoints and writes dosage,
-//                    P(hap=1) and haplotypes for every cell of the window.
+//   anchor_chain     one group of L lanes per sample and direction: forward and
+//                    backward over anchors, checkpoints every C anchors
+//   anchor_posterior one thread per (sample, window of C anchors) rebuilds the
+//                    window's anchors from the checkpoints; then one lane per
+//                    marker writes dosage, P(hap=1) and haplotypes.
 #include "fb_typed.hpp"
 #include "philox.cuh"
 
@@ -75,11 +75,11 @@ __device__ __forceinline__ View view_of(const TypedArgs& A, uint32_t s) {
 
 __device__ __forceinline__ uint32_t lmask_of(uint32_t L) { return L >= 32 ? 0xffffffffu : ((1u << L) - 1u); }
 
-__device__ __forceinline__ float tabQ(const Tabs& t, uint32_t n) {
-    return n < t.NT ? __ldg(t.Q + n) : exp2f((float)n * t.log2q);
-}
-__device__ __forceinline__ float tabS(const Tabs& t, uint32_t n) {
-    return n < t.NT ? __ldg(t.S + n) : (1.0f - exp2f((float)n * t.log2q)) * t.invL;
+// {Q[n], S[n]}: table entry, or the closed form past the table
+__device__ __forceinline__ float2 tabQS(const Tabs& t, uint32_t n) {
+    if (n < t.NT) return __ldg(t.QS + n);
+    const float qn = exp2f((float)n * t.log2q);
+    return make_float2(qn, (1.0f - qn) * t.invL);
 }
 __device__ __forceinline__ double tabG(const Tabs& t, uint32_t n) {
     if (n < t.NT) return __ldg(t.G + n);
@@ -227,7 +227,8 @@ __device__ __forceinline__ double chain_end_logU(const Tabs& tb, uint32_t n) {
 template <int LM>
 __device__ __forceinline__ void backward_step(const Tabs& tb, uint32_t n, float (&w)[LM], double& logU, uint32_t em,
                                               uint32_t sh, uint32_t lmask) {
-    const float Qn = tabQ(tb, n), Sn = tabS(tb, n);
+    const float2 qs = tabQS(tb, n);
+    const float Qn = qs.x, Sn = qs.y;
     const float sw = vsum<LM>(w);
     const double fterm = -999.0 - logU + tabG(tb, n);
     if (fterm > 0.0) {
@@ -257,7 +258,8 @@ __device__ __forceinline__ void backward_step(const Tabs& tb, uint32_t n, float 
 
 template <int LM>
 __device__ __forceinline__ void forward_step(const Tabs& tb, uint32_t n, float (&a)[LM], uint32_t em) {
-    const float Qn = tabQ(tb, n), Sn = tabS(tb, n);
+    const float2 qs = tabQS(tb, n);
+    const float Qn = qs.x, Sn = qs.y;
     const float base = vsum<LM>(a) * Sn;
 #pragma unroll
     for (int k = 0; k < LM; ++k) a[k] = ((em >> k) & 1u) ? fmaf(Qn, a[k], base) : 0.f;
@@ -273,271 +275,368 @@ __device__ __forceinline__ void init_forward(float (&a)[LM], uint32_t em) {
     for (int k = 0; k < LM; ++k) a[k] = ((em >> k) & 1u) ? 1.f : 0.f;
 }
 
-constexpr int kPrefetch = 8;  // anchors whose list entries are loaded ahead of the chain step
+// Sum over a chain's group of G lanes (aligned runs of G lanes; xor offsets
+// below G stay inside the group). Full-warp mask: every lane of the warp calls
+// it at the same step.
+template <int G>
+__device__ __forceinline__ float group_sum(float v) {
+#pragma unroll
+    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    return v;
+}
 
-// A CTA of 128 threads serves 64 samples: warps 0-1 run their forward chains
-// and warps 2-3 their backward chains at the same time (the two directions
-// are independent). Anchor entries are loaded one group of kPrefetch ahead.
+// One chain per group of LM lanes, one slot per lane. Even warps run forward
+// chains, odd warps the backward chains of the same samples. The warp steps
+// in lockstep to the longest of its chains (a finished chain holds its state),
+// in blocks of LM anchors: lane k holds the list entry of the block's k-th
+// anchor, loaded one block ahead, and the group reads it by shuffle.
+// Checkpoints: forward vector at anchors k % C == 0; backward vector and the
+// log of its unit at the same anchors.
 template <int LM>
 __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
-    const uint32_t s = blockIdx.x * 64 + (threadIdx.x & 63);
-    const bool forward = threadIdx.x < 64;
-    if (s >= A.B) return;
-    const View v = view_of(A, s);
+    constexpr uint32_t G = LM, GPW = 32 / G;
+    const uint32_t lane = threadIdx.x & 31;
+    const uint32_t wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+    const bool forward = (wg & 1u) == 0;
+    const uint32_t gl = lane / G, kl = lane % G, g0 = gl * G;
+    const uint32_t s = (wg >> 1) * GPW + gl;
+    const bool live = s < A.B;
+    View v{};
+    uint32_t NA = 0;
+    unsigned long long base = 0, wb = 0;
+    if (live) {
+        v = view_of(A, s);
+        base = A.aoff[s];
+        wb = A.woff[s];
+        NA = (uint32_t)(A.aoff[s + 1] - base);
+    }
+    const uint32_t NAw = __reduce_max_sync(0xffffffffu, NA);
+    if (NAw == 0) return;  // whole warp
     const Tabs& tb = v.r.tabs;
-    const unsigned long long base = A.aoff[s], NA = A.aoff[s + 1] - base, wb = A.woff[s];
     const uint32_t* pos = A.apos + base;
     const uint32_t* aem = A.aem + base;
     const uint8_t* ash = A.ashift + base;
     const uint32_t C = A.C;
     if (forward) {
-        float a[LM];
-        init_forward<LM>(a, aem[0]);
-        forward_step<LM>(tb, 0, a, 0xffffffffu);  // normalise
-#pragma unroll
-        for (int k = 0; k < LM; ++k) A.ckptF[wb * LM + k] = a[k];
-        uint32_t prev = pos[0];
-        uint32_t pp[kPrefetch], ee[kPrefetch];
-#pragma unroll
-        for (int j = 0; j < kPrefetch; ++j) {
-            const unsigned long long k = 1 + j;
-            pp[j] = k < NA ? pos[k] : 0u;
-            ee[j] = k < NA ? aem[k] : 0u;
+        float a = 0.f, sa = 0.f;
+        uint32_t prev = 0;
+        if (NA > 0) {
+            a = ((aem[0] >> kl) & 1u) ? 1.f : 0.f;
+            prev = pos[0];
         }
-        for (unsigned long long k0 = 1; k0 < NA; k0 += kPrefetch) {
-            uint32_t pn[kPrefetch], en[kPrefetch];
+        sa = group_sum<G>(a);
+        {
+            const float sc = NA > 0 ? pow2_neg(exp2_of(sa)) : 1.f;
+            a *= sc;
+            sa *= sc;
+        }
+        if (NA > 0) A.ckptF[wb * LM + kl] = a;
+        uint32_t cc = C, ci = 1;  // anchors to the next checkpoint, its window
+        uint32_t pv = 1 + kl < NA ? pos[1 + kl] : 0u, ev = 1 + kl < NA ? aem[1 + kl] : 0u;
+        for (uint32_t k0 = 1; k0 < NAw; k0 += G) {
+            const uint32_t kn = k0 + G + kl;  // next block, in flight during this one
+            const uint32_t pn = kn < NA ? pos[kn] : 0u, en = kn < NA ? aem[kn] : 0u;
 #pragma unroll
-            for (int j = 0; j < kPrefetch; ++j) {  // next group, in flight during this one
-                const unsigned long long k = k0 + kPrefetch + j;
-                pn[j] = k < NA ? pos[k] : 0u;
-                en[j] = k < NA ? aem[k] : 0u;
-            }
-#pragma unroll
-            for (int j = 0; j < kPrefetch; ++j) {
-                const unsigned long long k = k0 + j;
-                if (k < NA) {
-                    forward_step<LM>(tb, pp[j] - prev, a, ee[j]);
-                    prev = pp[j];
-                    if (k % C == 0)
-#pragma unroll
-                        for (int l = 0; l < LM; ++l) A.ckptF[(wb + k / C) * LM + l] = a[l];
+            for (uint32_t j = 0; j < G; ++j) {
+                const uint32_t p = __shfl_sync(0xffffffffu, pv, g0 + j);
+                const uint32_t em = __shfl_sync(0xffffffffu, ev, g0 + j);
+                const bool act = k0 + j < NA;
+                const float2 qs = tabQS(tb, act ? p - prev : 0u);
+                float an = ((em >> kl) & 1u) ? fmaf(qs.x, a, sa * qs.y) : 0.f;
+                an = act ? an : a;
+                const float s2 = group_sum<G>(an);
+                const float sc = act ? pow2_neg(exp2_of(s2)) : 1.f;
+                a = an * sc;
+                sa = act ? s2 * sc : sa;
+                prev = act ? p : prev;
+                cc = act ? cc - 1 : cc;
+                if (act && cc == 0) {
+                    A.ckptF[(wb + ci) * LM + kl] = a;
+                    ++ci;
+                    cc = C;
                 }
             }
-#pragma unroll
-            for (int j = 0; j < kPrefetch; ++j) { pp[j] = pn[j]; ee[j] = en[j]; }
+            pv = pn;
+            ev = en;
         }
     } else {
-        float w[LM];
-        uint32_t nextp = pos[NA - 1];
-        double logU = chain_end_logU(tb, v.len - 1 - nextp);
-        init_forward<LM>(w, aem[NA - 1]);
-        logU -= 999.0 * (double)ash[NA - 1];
-        if ((NA - 1) % C == 0) {
-#pragma unroll
-            for (int l = 0; l < LM; ++l) A.ckptB[(wb + (NA - 1) / C) * LM + l] = w[l];
-            A.ckptU[wb + (NA - 1) / C] = logU;
+        // step t handles anchor k = NA - 2 - t (t = 0 .. NA - 2)
+        float w = 0.f, sw = 0.f;
+        uint32_t nextp = 0;
+        double logU = 0.0;
+        if (NA > 0) {
+            nextp = pos[NA - 1];
+            logU = chain_end_logU(tb, v.len - 1 - nextp) - 999.0 * (double)ash[NA - 1];
+            w = ((aem[NA - 1] >> kl) & 1u) ? 1.f : 0.f;
         }
-        uint32_t pp[kPrefetch], ee[kPrefetch], hh[kPrefetch];
-#pragma unroll
-        for (int j = 0; j < kPrefetch; ++j) {
-            const long long k = (long long)NA - 2 - j;
-            pp[j] = k >= 0 ? pos[k] : 0u;
-            ee[j] = k >= 0 ? aem[k] : 0u;
-            hh[j] = k >= 0 ? ash[k] : 0u;
+        sw = group_sum<G>(w);
+        if (NA > 0 && (NA - 1) % C == 0) {
+            A.ckptB[(wb + (NA - 1) / C) * LM + kl] = w;
+            if (kl == 0) A.ckptU[wb + (NA - 1) / C] = logU;
         }
-        for (long long k0 = (long long)NA - 2; k0 >= 0; k0 -= kPrefetch) {
-            uint32_t pn[kPrefetch], en[kPrefetch], hn[kPrefetch];
+        uint32_t cc = NA >= 2 ? (NA - 2) % C + 1 : 0u;  // anchors to the next checkpoint (k % C == 0)
+        uint32_t ci = NA >= 2 ? (NA - 2) / C : 0u;      // its window
+        auto load = [&](uint32_t t, uint32_t& p, uint32_t& e, uint32_t& h) {
+            const bool ok = t + 2 <= NA;
+            const uint32_t k = NA - 2 - t;
+            p = ok ? pos[k] : 0u;
+            e = ok ? aem[k] : 0u;
+            h = ok ? ash[k] : 0u;
+        };
+        uint32_t pv, ev, hv;
+        load(kl, pv, ev, hv);
+        for (uint32_t t0 = 0; t0 + 1 < NAw; t0 += G) {
+            uint32_t pn, en, hn;
+            load(t0 + G + kl, pn, en, hn);
 #pragma unroll
-            for (int j = 0; j < kPrefetch; ++j) {
-                const long long k = k0 - kPrefetch - j;
-                pn[j] = k >= 0 ? pos[k] : 0u;
-                en[j] = k >= 0 ? aem[k] : 0u;
-                hn[j] = k >= 0 ? ash[k] : 0u;
-            }
-#pragma unroll
-            for (int j = 0; j < kPrefetch; ++j) {
-                const long long k = k0 - j;
-                if (k >= 0) {
-                    backward_step<LM>(tb, nextp - pp[j], w, logU, ee[j], hh[j], 0u);
-                    nextp = pp[j];
-                    if (k % C == 0) {
-#pragma unroll
-                        for (int l = 0; l < LM; ++l) A.ckptB[(wb + k / C) * LM + l] = w[l];
-                        A.ckptU[wb + k / C] = logU;
-                    }
+            for (uint32_t j = 0; j < G; ++j) {
+                const uint32_t p = __shfl_sync(0xffffffffu, pv, g0 + j);
+                const uint32_t em = __shfl_sync(0xffffffffu, ev, g0 + j);
+                const uint32_t sh = __shfl_sync(0xffffffffu, hv, g0 + j);
+                const bool act = t0 + j + 2 <= NA;
+                const uint32_t n = act ? nextp - p : 0u;
+                const float2 qs = tabQS(tb, n);
+                const double fterm = act ? -999.0 - logU + tabG(tb, n) : -1000.0;
+                const bool on = (em >> kl) & 1u;
+                float wn;
+                double lu = logU + (double)n * tb.lr;
+                if (fterm > 0.0) {
+                    // the floor dominates: unit becomes U rho^n e^fterm
+                    const float g = expf(-(float)fmin(fterm, 100.0));
+                    const float b = fmaf(g * sw, qs.y, 1.0f);
+                    wn = on ? fmaf(g * qs.x, w, b) : 0.f;
+                    lu += fterm;
+                } else {
+                    const float F = fterm > -104.0 ? expf((float)fterm) : 0.f;
+                    const float b = fmaf(sw, qs.y, F);
+                    wn = on ? fmaf(qs.x, w, b) : 0.f;
+                }
+                lu -= 999.0 * (double)sh;
+                wn = act ? wn : w;
+                const float s2 = group_sum<G>(wn);
+                const int e = act ? exp2_of(s2) : 0;
+                const float sc = pow2_neg(e);
+                w = wn * sc;
+                sw = act ? s2 * sc : sw;
+                logU = act ? lu + (double)e * 0.69314718055994530942 : logU;
+                nextp = act ? p : nextp;
+                cc = act ? cc - 1 : cc;
+                if (act && cc == 0) {
+                    A.ckptB[(wb + ci) * LM + kl] = w;
+                    if (kl == 0) A.ckptU[wb + ci] = logU;
+                    --ci;
+                    cc = C;
                 }
             }
-#pragma unroll
-            for (int j = 0; j < kPrefetch; ++j) { pp[j] = pn[j]; ee[j] = en[j]; hh[j] = hn[j]; }
+            pv = pn;
+            ev = en;
+            hv = hn;
         }
     }
 }
 
 // ---------------------------------------------------------------- posterior
+//
+// Phase 1, one thread per window (C consecutive anchors of one sample): from
+// the window's checkpoints, rebuild for every anchor k of the window the
+// interval record of the run [pos[k], pos[k+1]):
+//   a'  forward vector after the emission at k, divided by its sum
+//   w'  backward vector of anchor k+1 (E . beta), divided by its sum
+//   {p0, p1, farg'} with farg' = -999 - logU - ln(sum w) the log of beta's
+//       e^-999 floor in units of w'; -inf when the floor is negligible over
+//       the whole run, +inf when beta is uniform (the chain's last run, or a
+//       floor that dominates everywhere).
+// With a' and w' of unit sum, a cell i markers after p0 and j = p1 - m before
+// p1 has
+//   alpha_l ~ Q[i] a'_l + S[i]      beta_l ~ Q[j] w'_l + S[j] (+ floor)
+//   p_l = alpha_l beta_l.
+// Phase 2, one warp per run of windows of the same sample: lane = marker, so
+// each warp step covers 32 consecutive markers and writes them coalesced. A
+// lane finds its record by counting anchors (typed markers and marker 0) up
+// to its marker with a ballot over the codes.
 
-// Per-warp output staging: each thread computes 32 consecutive cells of its
-// window into shared memory, then the warp writes every thread's 32 cells as
-// one coalesced row segment (128 B of dosage, 2 x 32 B of alleles).
-constexpr uint32_t kStageD = 33;  // floats per staged dosage row (32 + pad)
-constexpr uint32_t kStageH = 36;  // bytes per staged allele row (32 + pad)
+// mode of a record from the high word of farg'
+constexpr uint32_t kInfHi = 0x7ff00000u;
 
-// nibble of slot bits -> four 0/1 floats (shared-memory table)
-__device__ __forceinline__ float4 nib(const float4* lut, uint32_t bits, int j) { return lut[(bits >> (4 * j)) & 15u]; }
+__device__ __forceinline__ float rcp_approx(float x) {
+    float r;
+    asm("rcp.approx.ftz.f32 %0, %1;" : "=f"(r) : "f"(x));
+    return r;
+}
+
+template <int LM>
+__host__ __device__ constexpr uint32_t post_record_bytes() { return 2u * LM * 4u + 16u; }
 
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
 template <int LM, bool kFull>
-__global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A) {
+__global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kernel(TypedArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t T = blockDim.x, t = threadIdx.x, C = A.C, lane = t & 31, warp = t >> 5;
-    float4* lut = reinterpret_cast<float4*>(smem);                                  // [16]
-    float* bw = reinterpret_cast<float*>(smem + 256);                               // [C][LM][T]
-    double* bu = reinterpret_cast<double*>(smem + 256 + (size_t)C * LM * T * 4);   // [C][T]
-    unsigned char* stage = smem + 256 + (size_t)C * LM * T * 4 + (size_t)C * T * 8;
-    float* sd = reinterpret_cast<float*>(stage) + (size_t)warp * 32 * kStageD;      // [32][kStageD] of this warp
-    uint8_t* sh8 = stage + (size_t)(T / 32) * 32 * kStageD * 4 + (size_t)warp * 64 * kStageH;  // [32][2][kStageH]
-    if (t < 16) lut[t] = make_float4((float)(t & 1), (float)((t >> 1) & 1), (float)((t >> 2) & 1), (float)(t >> 3));
+    const uint32_t t = threadIdx.x, C = A.C, lane = t & 31, warp = t >> 5;
+    // nibble -> four 0/1 floats, 8 copies so that the 8 lanes of a quarter warp
+    // read distinct banks: entry e, copy j at float4 index 8 e + j
+    float4* lut = reinterpret_cast<float4*>(smem);
+    const size_t per_warp = (size_t)32 * C * post_record_bytes<LM>();
+    unsigned char* wbase = smem + 2048 + (size_t)warp * per_warp;
+    float* recA = reinterpret_cast<float*>(wbase);                            // [32 C][LM]
+    float* recW = recA + (size_t)32 * C * LM;                                  // [32 C][LM]
+    uint4* recM = reinterpret_cast<uint4*>(recW + (size_t)32 * C * LM);        // [32 C] {p0, p1, farg' lo, hi}
+    for (uint32_t e = t; e < 128; e += blockDim.x) {
+        const uint32_t n = e >> 3;
+        lut[e] = make_float4((float)(n & 1), (float)((n >> 1) & 1), (float)((n >> 2) & 1), (float)(n >> 3));
+    }
     __syncthreads();
 
-    const unsigned long long g = (unsigned long long)blockIdx.x * T + t;
+    // ---- phase 1
+    const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + t;
     const bool live = g < A.total_windows;
-
-    uint32_t s = 0, cstart = 0, ncells = 0;
-    View v{};
-    unsigned long long NA = 0, k0 = 0, k1 = 0;
-    const uint32_t* pos = nullptr;
-    const uint32_t* aem = nullptr;
-    float a[LM];
-#pragma unroll
-    for (int l = 0; l < LM; ++l) a[l] = 0.f;
+    uint32_t s = 0xffffffffu, cstart = 0, cend = 0;
     if (live) {
         s = A.wsample[g];
-        v = view_of(A, s);
+        const View v = view_of(A, s);
         const Tabs& tb = v.r.tabs;
         const unsigned long long base = A.aoff[s], wb = A.woff[s], w = g - wb;
-        NA = A.aoff[s + 1] - base;
-        pos = A.apos + base;
-        aem = A.aem + base;
+        const unsigned long long NA = A.aoff[s + 1] - base;
+        const uint32_t* pos = A.apos + base;
+        const uint32_t* aem = A.aem + base;
         const uint8_t* ash = A.ashift + base;
-        k0 = w * C;
-        k1 = min(k0 + C, NA);
-        // backward anchors k in (k0, k1], at slot k - k0 - 1
+        const unsigned long long k0 = w * C, k1 = min(k0 + C, NA);
+        const uint32_t u0 = lane * C;  // this window's first record
+        cstart = pos[k0];
+        cend = k1 < NA ? pos[k1] : v.len;
+        // backward: records k0 .. k1-1 take w' from anchor k+1
         float bv[LM];
         double logU;
-        long long kstart;
+        unsigned long long kstart;
         if (k1 < NA) {
 #pragma unroll
             for (int l = 0; l < LM; ++l) bv[l] = A.ckptB[(wb + w + 1) * LM + l];
             logU = A.ckptU[wb + w + 1];
-            kstart = (long long)k1;
+            kstart = k1;
         } else {
             logU = chain_end_logU(tb, v.len - 1 - pos[NA - 1]) - 999.0 * (double)ash[NA - 1];
             init_forward<LM>(bv, aem[NA - 1]);
-            kstart = (long long)NA - 1;
-        }
-        for (long long k = kstart;; --k) {
-            if (k > (long long)k0) {
-                const uint32_t slot = (uint32_t)(k - (long long)k0 - 1);
+            kstart = NA - 1;
+            const uint32_t u = u0 + (uint32_t)(NA - 1 - k0);
 #pragma unroll
-                for (int l = 0; l < LM; ++l) bw[((size_t)slot * LM + l) * T + t] = bv[l];
-                bu[(size_t)slot * T + t] = logU;
-            }
-            if (k - 1 <= (long long)k0) break;
-            backward_step<LM>(tb, pos[k] - pos[k - 1], bv, logU, aem[k - 1], ash[k - 1], 0u);
+            for (int l = 0; l < LM; ++l) recW[(size_t)u * LM + l] = 0.f;
+            recM[u] = make_uint4(pos[NA - 1], v.len, 0u, kInfHi);  // beta uniform
         }
+        for (unsigned long long k = kstart; k > k0; --k) {
+            const uint32_t p0 = pos[k - 1], p1 = pos[k], n = p1 - p0;
+            const float sw = vsum<LM>(bv);
+            const double farg = -999.0 - logU;
+            uint32_t lo = 0u, hi;
+            if (farg + tabG(tb, n) < -104.0) hi = kInfHi | 0x80000000u;  // floor negligible: -inf
+            else if (farg + tabG(tb, 1) > 60.0) hi = kInfHi;               // floor dominates: uniform
+            else {
+                const double f = farg - log((double)sw);
+                lo = (uint32_t)__double_as_longlong(f);
+                hi = (uint32_t)((unsigned long long)__double_as_longlong(f) >> 32);
+            }
+            const uint32_t u = u0 + (uint32_t)(k - 1 - k0);
+            const float inv = rcp_approx(sw);
+#pragma unroll
+            for (int l = 0; l < LM; ++l) recW[(size_t)u * LM + l] = bv[l] * inv;
+            recM[u] = make_uint4(p0, p1, lo, hi);
+            if (k - 1 > k0) backward_step<LM>(tb, n, bv, logU, aem[k - 1], ash[k - 1], 0u);
+        }
+        // forward: records take a' at anchor k
+        float a[LM];
 #pragma unroll
         for (int l = 0; l < LM; ++l) a[l] = A.ckptF[(wb + w) * LM + l];
-        cstart = pos[k0];
-        ncells = (k1 < NA ? pos[k1] : v.len) - cstart;
-    }
-    const Tabs& tb = v.r.tabs;
-    const uint32_t lmask = lmask_of(v.r.L);
-    float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
+        for (unsigned long long k = k0; k < k1; ++k) {
+            const uint32_t u = u0 + (uint32_t)(k - k0);
+            const float inv = rcp_approx(vsum<LM>(a));
 #pragma unroll
-    for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
-
-    // interval state (current anchor k, cells [p0, p1))
-    unsigned long long k = k0;
-    uint32_t p0 = cstart, p1 = 0, n = 0;
-    float Sa = 0.f, Sw = 0.f;
-    double farg = 0.0;
-    int mode = 2;  // 0: exact floor per cell, 1: floor negligible, 2: beta uniform
-    float wv[LM];
-    auto open_interval = [&]() {
-        const bool has_next = k + 1 < NA;
-        p1 = has_next ? pos[k + 1] : v.len;
-        n = p1 - p0;
-        Sa = vsum<LM>(a);
-        mode = 2;
-        if (has_next) {
-            const uint32_t slot = (uint32_t)(k - k0);
-#pragma unroll
-            for (int l = 0; l < LM; ++l) wv[l] = bw[((size_t)slot * LM + l) * T + t];
-            Sw = vsum<LM>(wv);
-            farg = -999.0 - bu[(size_t)slot * T + t];
-            if (farg + tabG(tb, n) < -104.0) mode = 1;
-            else if (farg + tabG(tb, 1) > 60.0) mode = 2;
-            else mode = 0;
-        } else {
-#pragma unroll
-            for (int l = 0; l < LM; ++l) wv[l] = 0.f;
+            for (int l = 0; l < LM; ++l) recA[(size_t)u * LM + l] = a[l] * inv;
+            if (k + 1 < k1) forward_step<LM>(tb, pos[k + 1] - pos[k], a, aem[k + 1]);
         }
-    };
-    if (live) open_interval();
+    }
+    __syncwarp();
 
+    // ---- phase 2
+    const uint32_t live_mask = __ballot_sync(0xffffffffu, live);
+    const uint32_t le_mask = 0xffffffffu >> (31 - lane);
+    const uint32_t lj = lane & 7;
     const float keep = 1.0f - A.tie_eps;
-    const uint32_t max_cells = __reduce_max_sync(0xffffffffu, ncells);
-    for (uint32_t cb = 0; cb < max_cells; cb += 32) {
-        for (uint32_t c = 0; c < 32; ++c) {
-            const uint32_t idx = cb + c;
-            if (idx >= ncells) break;
-            const uint32_t m = cstart + idx;
-            if (m == p1) {  // next anchor: forward step with its emission, open its interval
-                forward_step<LM>(tb, n, a, aem[k + 1]);
-                ++k;
-                p0 = p1;
-                open_interval();
+    const bool w_dos = A.dosage != nullptr, w_hap = A.haps != nullptr, w_hp = A.hprob != nullptr;
+    const bool argmax = A.sampling == SI_SAMPLE_ARGMAX;
+    uint32_t r = 0;
+    while (r < 32 && ((live_mask >> r) & 1u)) {
+        const uint32_t sr = __shfl_sync(0xffffffffu, s, r);
+        const uint32_t same = __ballot_sync(0xffffffffu, live && s == sr);
+        const uint32_t r2 = 31 - __clz(same);  // windows of a sample are consecutive
+        const uint32_t c0 = __shfl_sync(0xffffffffu, cstart, r), c1 = __shfl_sync(0xffffffffu, cend, r2);
+        const View v = view_of(A, sr);
+        const Tabs& tb = v.r.tabs;
+        const uint32_t lmask = lmask_of(v.r.L);
+        float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
+#pragma unroll
+        for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
+        const uint8_t* gp = v.geno;
+        const SlotMasks* mp = v.r.masks;
+        float* dos = w_dos ? A.dosage + v.out : nullptr;
+        uint8_t* h0 = w_hap ? A.haps + 2 * v.out : nullptr;
+        uint8_t* h1 = w_hap ? h0 + v.len : nullptr;
+        float2* hp = w_hp ? reinterpret_cast<float2*>(A.hprob) + v.out : nullptr;
+        uint32_t cu = r * C - 1u;  // record of the marker before the step (wraps for r = 0)
+        // codes and slot masks of the step, loaded one step ahead
+        const uint32_t mq = min(c0 + lane, c1 - 1);
+        uint8_t code = gp[mq];
+        SlotMasks mk = mp[mq];
+        for (uint32_t cb = c0; cb < c1; cb += 32) {
+            const uint32_t m_raw = cb + lane;
+            const bool valid = m_raw < c1;
+            const uint32_t m = valid ? m_raw : c1 - 1;  // lanes past the run repeat its last marker, unwritten
+            const uint8_t code_c = code;
+            const SlotMasks mk_c = mk;
+            {
+                const uint32_t mn = min(m_raw + 32, c1 - 1);
+                code = gp[mn];
+                mk = mp[mn];
             }
-            const uint32_t i = m - p0;
-            const float xf = tabQ(tb, i), yf = Sa * tabS(tb, i);
-            float xb = 0.f, yb = 1.f;
-            if (mode != 2) {
-                const uint32_t j1 = n - i;
-                const float Qj = tabQ(tb, j1), Sj = tabS(tb, j1);
-                if (mode == 1) {
-                    xb = Qj;
-                    yb = Sw * Sj;
-                } else {
-                    const double ft = farg + tabG(tb, j1);
+            const bool is_anchor = valid && (m == 0 || code_c < 3);
+            const uint32_t bal = __ballot_sync(0xffffffffu, is_anchor);
+            const uint32_t u = cu + __popc(bal & le_mask);
+            cu += __popc(bal);
+            const uint4 meta = recM[u];
+            const float2 qi = tabQS(tb, m - meta.x), qj = tabQS(tb, meta.y - m);
+            const bool uni = meta.w == kInfHi;                  // beta uniform
+            const bool fin = (meta.w & kInfHi) != kInfHi;       // finite farg': floor term per marker
+            float xb = uni ? 0.f : qj.x, yb = uni ? 1.f : qj.y;
+            if (__any_sync(0xffffffffu, fin)) {
+                if (fin) {
+                    const double ft = __longlong_as_double(((long long)meta.w << 32) | meta.z) + tabG(tb, meta.y - m);
                     if (ft > 0.0) {
                         const float gg = expf(-(float)fmin(ft, 100.0));
-                        xb = gg * Qj;
-                        yb = fmaf(gg * Sw, Sj, 1.0f);
+                        xb = gg * qj.x;
+                        yb = fmaf(gg, qj.y, 1.0f);
                     } else {
-                        xb = Qj;
-                        yb = fmaf(Sw, Sj, ft > -104.0 ? expf((float)ft) : 0.f);
+                        yb = qj.y + (ft > -104.0 ? expf((float)ft) : 0.f);
                     }
                 }
             }
-            const SlotMasks mk = v.r.masks[m];
-            // p_l = (xf a_l + yf)(xb w_l + yb), two slots per packed FP32x2 op
-            float pr[LM];
-            const float2 XF = make_float2(xf, xf), YF = make_float2(yf, yf);
+            const float4* RA = reinterpret_cast<const float4*>(recA + (size_t)u * LM);
+            const float4* RW = reinterpret_cast<const float4*>(recW + (size_t)u * LM);
+            const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
             const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
+            float pr[LM];
             float2 tot2 = make_float2(0.f, 0.f), q02 = tot2, q12 = tot2;
 #pragma unroll
-            for (int l = 0; l < LM; l += 2) {
-                const float2 al = __ffma2_rn(XF, make_float2(a[l], a[l + 1]), YF);
-                const float2 be = __ffma2_rn(XB, make_float2(wv[l], wv[l + 1]), YB);
-                float2 pp = __fmul2_rn(al, be);
-                if (!kFull) pp = __fmul2_rn(pp, make_float2(act[l], act[l + 1]));
-                pr[l] = pp.x;
-                pr[l + 1] = pp.y;
-                tot2 = __fadd2_rn(tot2, pp);
-            }
-#pragma unroll
-            for (int j = 0; j < LM / 4; ++j) {
-                const float4 m0 = nib(lut, mk.a0, j), m1 = nib(lut, mk.a1, j);
-                const float2 p01 = make_float2(pr[4 * j], pr[4 * j + 1]), p23 = make_float2(pr[4 * j + 2], pr[4 * j + 3]);
+            for (int q4 = 0; q4 < LM / 4; ++q4) {
+                const float4 av = RA[q4], wv = RW[q4];
+                float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.x, av.y), YF),
+                                        __ffma2_rn(XB, make_float2(wv.x, wv.y), YB));
+                float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.z, av.w), YF),
+                                        __ffma2_rn(XB, make_float2(wv.z, wv.w), YB));
+                if (!kFull) {
+                    p01 = __fmul2_rn(p01, make_float2(act[4 * q4], act[4 * q4 + 1]));
+                    p23 = __fmul2_rn(p23, make_float2(act[4 * q4 + 2], act[4 * q4 + 3]));
+                }
+                pr[4 * q4] = p01.x; pr[4 * q4 + 1] = p01.y; pr[4 * q4 + 2] = p23.x; pr[4 * q4 + 3] = p23.y;
+                tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
+                const float4 m0 = lut[((mk_c.a0 >> (4 * q4)) & 15u) * 8 + lj];
+                const float4 m1 = lut[((mk_c.a1 >> (4 * q4)) & 15u) * 8 + lj];
                 q02 = __ffma2_rn(p01, make_float2(m0.x, m0.y), q02);
                 q02 = __ffma2_rn(p23, make_float2(m0.z, m0.w), q02);
                 q12 = __ffma2_rn(p01, make_float2(m1.x, m1.y), q12);
@@ -545,7 +644,7 @@ __global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A) {
             }
             const float tot = tot2.x + tot2.y, q0 = q02.x + q02.y, q1 = q12.x + q12.y;
             uint32_t pick;
-            if (A.sampling == SI_SAMPLE_ARGMAX) {
+            if (argmax) {
                 float pmax = pr[0];
 #pragma unroll
                 for (int l = 1; l < LM; ++l) pmax = fmaxf(pmax, pr[l]);
@@ -567,37 +666,23 @@ __global__ void __launch_bounds__(128) anchor_posterior_kernel(TypedArgs A) {
                 }
                 if (pick == LM) pick = last_nz;
             }
-            const float inv = __frcp_rn(tot);
-            sd[lane * kStageD + c] = (q0 + q1) * inv;
-            sh8[(lane * 2 + 0) * kStageH + c] = (uint8_t)((mk.a0 >> pick) & 1u);
-            sh8[(lane * 2 + 1) * kStageH + c] = (uint8_t)((mk.a1 >> pick) & 1u);
-            if (A.hprob) reinterpret_cast<float2*>(A.hprob)[v.out + m] = make_float2(q0 * inv, q1 * inv);
-        }
-        __syncwarp();
-        // flush: row r = the 32 cells thread r just staged
-        const int mine = (int)min(32u, ncells > cb ? ncells - cb : 0u);
-        for (int r = 0; r < 32; ++r) {
-            const int cnt = __shfl_sync(0xffffffffu, mine, r);
-            if (cnt <= 0) continue;
-            const unsigned long long out = __shfl_sync(0xffffffffu, (unsigned long long)v.out, r);
-            const uint32_t len = __shfl_sync(0xffffffffu, v.len, r);
-            const uint32_t m0 = __shfl_sync(0xffffffffu, cstart + cb, r);
-            if ((int)lane < cnt) {
-                if (A.dosage) A.dosage[out + m0 + lane] = sd[r * kStageD + lane];
-                if (A.haps) {
-                    A.haps[2 * out + m0 + lane] = sh8[(r * 2 + 0) * kStageH + lane];
-                    A.haps[2 * out + len + m0 + lane] = sh8[(r * 2 + 1) * kStageH + lane];
+            const float inv = rcp_approx(tot);
+            if (valid) {
+                if (w_dos) dos[m] = (q0 + q1) * inv;
+                if (w_hap) {
+                    h0[m] = (uint8_t)((mk_c.a0 >> pick) & 1u);
+                    h1[m] = (uint8_t)((mk_c.a1 >> pick) & 1u);
                 }
+                if (w_hp) hp[m] = make_float2(q0 * inv, q1 * inv);
             }
         }
-        __syncwarp();
+        r = r2 + 1;
     }
 }
 
 template <int LM>
 size_t post_smem(uint32_t T, uint32_t C) {
-    return 256 + (size_t)C * LM * T * 4 + (size_t)C * T * 8 + (size_t)(T / 32) * 32 * kStageD * 4 +
-           (size_t)(T / 32) * 64 * kStageH;
+    return 2048 + (size_t)T * C * post_record_bytes<LM>();
 }
 
 template <int LM, bool kFull>
@@ -616,7 +701,9 @@ cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
 
 template <int LM>
 cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
-    anchor_chain_kernel<LM><<<(a.B + 63) / 64, 128, 0, s>>>(a);
+    constexpr uint32_t kChainsPerWarp = 32 / LM;
+    const unsigned long long warps = 2ull * ((a.B + kChainsPerWarp - 1) / kChainsPerWarp);  // forward + backward
+    anchor_chain_kernel<LM><<<(uint32_t)((warps + 3) / 4), 128, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (a.ev_chain_done && (e = cudaEventRecord(a.ev_chain_done, s)) != cudaSuccess) return e;
@@ -624,6 +711,12 @@ cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
 }
 
 }  // namespace
+
+// The window (anchors rebuilt from one checkpoint) fixes where rounding
+// restarts, so it must not depend on the batch: one value for every L. The
+// CTA size changes nothing numerically and shrinks as the records grow.
+uint32_t typed_default_window(uint32_t) { return 4u; }
+uint32_t typed_default_threads(uint32_t lmax) { return lmax <= 8 ? 128u : (lmax <= 16 ? 64u : 32u); }
 
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C) {
     switch (fb_lmax(L)) {

@@ -95,7 +95,7 @@ struct si_ctx {
     // typed-marker kernel scratch and tables
     si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_aem, t_wsample, t_ckF, t_ckB, t_ckU;
     struct TableSet {
-        si::DeviceBuffer Q, S, G;
+        si::DeviceBuffer QS, G;
         double consts[4] = {0, 0, 0, 0};  // log2q, lr, lgc, regime
     };
     std::map<uint64_t, TableSet> tables;  // closed-form run tables per (transition, L)

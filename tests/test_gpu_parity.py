@@ -153,14 +153,21 @@ def test_fb_tiles_do_not_change_results(engine):
     panel, pos, codes, _ = workload(300, 400, 100, synth.typed_every(300, 5), 100, 13)
     load(engine, panel, pos, store=False)
     base = engine.impute(codes, N.default_params(), hap_prob=True)
-    for flags in (0, N.IMPUTE_FULL_CHAIN):
-        for C, T in [(8, 32), (17, 96), (32, 128), (1, 32)]:
+    # typed path: C anchors per window; full chain: C markers per checkpoint segment
+    tiles = {0: [(8, 32), (17, 96), (32, 64), (1, 32), (4, 128)],
+             N.IMPUTE_FULL_CHAIN: [(8, 32), (17, 96), (32, 128), (1, 32)]}
+    for flags, pairs in tiles.items():
+        for C, T in pairs:
             alt = engine.impute(codes, N.default_params(checkpoint_interval=C, block_threads=T, flags=flags),
                                 hap_prob=True)
             assert np.array_equal(alt["haps"], base["haps"])
             assert np.abs(alt["dosage"] - base["dosage"]).max() <= 2e-5
     ms = engine.last_kernel_ms()
     assert len(ms) == 4 and ms[3] > 0
+    # a typed tile whose interval records exceed shared memory is refused, not truncated
+    with pytest.raises(N.SIError) as e:
+        engine.impute(codes, N.default_params(checkpoint_interval=32, block_threads=128))
+    assert e.value.status == 4  # SI_ERR_UNSUPPORTED
 
 
 def test_fb_philox_sampling_and_batch_invariance(engine):
