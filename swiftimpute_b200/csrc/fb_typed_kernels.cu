@@ -15,8 +15,9 @@
 // per-cell work runs in parallel. Kernels:
 //   anchor_count / anchor_scan / anchor_fill   per-sample anchor lists (marker 0
 //                                              is always an anchor)
-//   anchor_chain     one group of L lanes per sample and direction: forward and
-//                    backward over anchors, checkpoints every C anchors
+//   anchor_chain     one group of L/4 lanes (four slots each) per sample and
+//                    direction: forward and backward over anchors, checkpoints
+//                    every C anchors
 //   anchor_posterior one thread per (sample, window of C anchors) rebuilds the
 //                    window's anchors from the checkpoints; then one lane per
 //                    marker writes dosage, P(hap=1) and haplotypes.
@@ -285,20 +286,23 @@ __device__ __forceinline__ float group_sum(float v) {
     return v;
 }
 
-// One chain per group of LM lanes, one slot per lane. Even warps run forward
-// chains, odd warps the backward chains of the same samples. The warp steps
-// in lockstep to the longest of its chains (a finished chain holds its state),
-// in blocks of LM anchors: lane k holds the list entry of the block's k-th
-// anchor, loaded one block ahead, and the group reads it by shuffle.
-// Checkpoints: forward vector at anchors k % C == 0; backward vector and the
-// log of its unit at the same anchors.
+constexpr uint32_t kChainBlock = 8;  // anchors per block of list entries (loaded one block ahead)
+
+// One chain per group of G = LM/4 lanes, four slots per lane. Even warps run
+// forward chains, odd warps the backward chains of the same samples. The warp
+// steps in lockstep to the longest of its chains (a finished chain holds its
+// state), in blocks of kChainBlock anchors: step j of a block is held by lane
+// j % G of the group in register j / G, loaded one block ahead and read by
+// shuffle. Checkpoints: forward vector at anchors k % C == 0; backward vector
+// and the log of its unit at the same anchors.
 template <int LM>
 __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
-    constexpr uint32_t G = LM, GPW = 32 / G;
+    constexpr uint32_t G = LM / 4, GPW = 32 / G, R = kChainBlock / G;
+    static_assert(LM % 4 == 0 && kChainBlock % G == 0, "chain layout");
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const bool forward = (wg & 1u) == 0;
-    const uint32_t gl = lane / G, kl = lane % G, g0 = gl * G;
+    const uint32_t gl = lane / G, kl = lane % G, g0 = gl * G, sl = kl * 4;  // sl: first slot of the lane
     const uint32_t s = (wg >> 1) * GPW + gl;
     const bool live = s < A.B;
     View v{};
@@ -317,61 +321,84 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
     const uint32_t* aem = A.aem + base;
     const uint8_t* ash = A.ashift + base;
     const uint32_t C = A.C;
+    auto sum4 = [](const float (&x)[4]) { return (x[0] + x[1]) + (x[2] + x[3]); };
     if (forward) {
-        float a = 0.f, sa = 0.f;
+        float a[4] = {0.f, 0.f, 0.f, 0.f};
         uint32_t prev = 0;
         if (NA > 0) {
-            a = ((aem[0] >> kl) & 1u) ? 1.f : 0.f;
+            const uint32_t e0 = aem[0] >> sl;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] = ((e0 >> i) & 1u) ? 1.f : 0.f;
             prev = pos[0];
         }
-        sa = group_sum<G>(a);
+        float sa = group_sum<G>(sum4(a));
         {
             const float sc = NA > 0 ? pow2_neg(exp2_of(sa)) : 1.f;
-            a *= sc;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) a[i] *= sc;
             sa *= sc;
         }
-        if (NA > 0) A.ckptF[wb * LM + kl] = a;
+        if (NA > 0) *reinterpret_cast<float4*>(A.ckptF + wb * LM + sl) = make_float4(a[0], a[1], a[2], a[3]);
         uint32_t cc = C, ci = 1;  // anchors to the next checkpoint, its window
-        uint32_t pv = 1 + kl < NA ? pos[1 + kl] : 0u, ev = 1 + kl < NA ? aem[1 + kl] : 0u;
-        for (uint32_t k0 = 1; k0 < NAw; k0 += G) {
-            const uint32_t kn = k0 + G + kl;  // next block, in flight during this one
-            const uint32_t pn = kn < NA ? pos[kn] : 0u, en = kn < NA ? aem[kn] : 0u;
+        uint32_t pv[R], ev[R];
 #pragma unroll
-            for (uint32_t j = 0; j < G; ++j) {
-                const uint32_t p = __shfl_sync(0xffffffffu, pv, g0 + j);
-                const uint32_t em = __shfl_sync(0xffffffffu, ev, g0 + j);
+        for (uint32_t i = 0; i < R; ++i) {
+            const uint32_t k = 1 + kl + G * i;
+            pv[i] = k < NA ? pos[k] : 0u;
+            ev[i] = k < NA ? aem[k] : 0u;
+        }
+        for (uint32_t k0 = 1; k0 < NAw; k0 += kChainBlock) {
+            uint32_t pn[R], en[R];
+#pragma unroll
+            for (uint32_t i = 0; i < R; ++i) {  // next block, in flight during this one
+                const uint32_t k = k0 + kChainBlock + kl + G * i;
+                pn[i] = k < NA ? pos[k] : 0u;
+                en[i] = k < NA ? aem[k] : 0u;
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kChainBlock; ++j) {
+                const uint32_t p = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
+                const uint32_t em = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
                 const bool act = k0 + j < NA;
                 const float2 qs = tabQS(tb, act ? p - prev : 0u);
-                float an = ((em >> kl) & 1u) ? fmaf(qs.x, a, sa * qs.y) : 0.f;
-                an = act ? an : a;
-                const float s2 = group_sum<G>(an);
+                const float b = sa * qs.y;
+                float an[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) an[i] = act ? (((em >> i) & 1u) ? fmaf(qs.x, a[i], b) : 0.f) : a[i];
+                const float s2 = group_sum<G>(sum4(an));
                 const float sc = act ? pow2_neg(exp2_of(s2)) : 1.f;
-                a = an * sc;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) a[i] = an[i] * sc;
                 sa = act ? s2 * sc : sa;
                 prev = act ? p : prev;
                 cc = act ? cc - 1 : cc;
                 if (act && cc == 0) {
-                    A.ckptF[(wb + ci) * LM + kl] = a;
+                    *reinterpret_cast<float4*>(A.ckptF + (wb + ci) * LM + sl) = make_float4(a[0], a[1], a[2], a[3]);
                     ++ci;
                     cc = C;
                 }
             }
-            pv = pn;
-            ev = en;
+#pragma unroll
+            for (uint32_t i = 0; i < R; ++i) {
+                pv[i] = pn[i];
+                ev[i] = en[i];
+            }
         }
     } else {
         // step t handles anchor k = NA - 2 - t (t = 0 .. NA - 2)
-        float w = 0.f, sw = 0.f;
+        float w[4] = {0.f, 0.f, 0.f, 0.f};
         uint32_t nextp = 0;
         double logU = 0.0;
         if (NA > 0) {
             nextp = pos[NA - 1];
             logU = chain_end_logU(tb, v.len - 1 - nextp) - 999.0 * (double)ash[NA - 1];
-            w = ((aem[NA - 1] >> kl) & 1u) ? 1.f : 0.f;
+            const uint32_t eL = aem[NA - 1] >> sl;
+#pragma unroll
+            for (int i = 0; i < 4; ++i) w[i] = ((eL >> i) & 1u) ? 1.f : 0.f;
         }
-        sw = group_sum<G>(w);
+        float sw = group_sum<G>(sum4(w));
         if (NA > 0 && (NA - 1) % C == 0) {
-            A.ckptB[(wb + (NA - 1) / C) * LM + kl] = w;
+            *reinterpret_cast<float4*>(A.ckptB + (wb + (NA - 1) / C) * LM + sl) = make_float4(w[0], w[1], w[2], w[3]);
             if (kl == 0) A.ckptU[wb + (NA - 1) / C] = logU;
         }
         uint32_t cc = NA >= 2 ? (NA - 2) % C + 1 : 0u;  // anchors to the next checkpoint (k % C == 0)
@@ -383,54 +410,55 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
             e = ok ? aem[k] : 0u;
             h = ok ? ash[k] : 0u;
         };
-        uint32_t pv, ev, hv;
-        load(kl, pv, ev, hv);
-        for (uint32_t t0 = 0; t0 + 1 < NAw; t0 += G) {
-            uint32_t pn, en, hn;
-            load(t0 + G + kl, pn, en, hn);
+        uint32_t pv[R], ev[R], hv[R];
 #pragma unroll
-            for (uint32_t j = 0; j < G; ++j) {
-                const uint32_t p = __shfl_sync(0xffffffffu, pv, g0 + j);
-                const uint32_t em = __shfl_sync(0xffffffffu, ev, g0 + j);
-                const uint32_t sh = __shfl_sync(0xffffffffu, hv, g0 + j);
+        for (uint32_t i = 0; i < R; ++i) load(kl + G * i, pv[i], ev[i], hv[i]);
+        for (uint32_t t0 = 0; t0 + 1 < NAw; t0 += kChainBlock) {
+            uint32_t pn[R], en[R], hn[R];
+#pragma unroll
+            for (uint32_t i = 0; i < R; ++i) load(t0 + kChainBlock + kl + G * i, pn[i], en[i], hn[i]);
+#pragma unroll
+            for (uint32_t j = 0; j < kChainBlock; ++j) {
+                const uint32_t p = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
+                const uint32_t em = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
+                const uint32_t sh = __shfl_sync(0xffffffffu, hv[j / G], g0 + j % G);
                 const bool act = t0 + j + 2 <= NA;
                 const uint32_t n = act ? nextp - p : 0u;
                 const float2 qs = tabQS(tb, n);
                 const double fterm = act ? -999.0 - logU + tabG(tb, n) : -1000.0;
-                const bool on = (em >> kl) & 1u;
-                float wn;
-                double lu = logU + (double)n * tb.lr;
-                if (fterm > 0.0) {
-                    // the floor dominates: unit becomes U rho^n e^fterm
-                    const float g = expf(-(float)fmin(fterm, 100.0));
-                    const float b = fmaf(g * sw, qs.y, 1.0f);
-                    wn = on ? fmaf(g * qs.x, w, b) : 0.f;
-                    lu += fterm;
-                } else {
-                    const float F = fterm > -104.0 ? expf((float)fterm) : 0.f;
-                    const float b = fmaf(sw, qs.y, F);
-                    wn = on ? fmaf(qs.x, w, b) : 0.f;
-                }
-                lu -= 999.0 * (double)sh;
-                wn = act ? wn : w;
-                const float s2 = group_sum<G>(wn);
+                // fterm > 0: the floor dominates and the unit becomes U rho^n e^fterm
+                const bool big = fterm > 0.0;
+                const float ex = expf(-(float)fmin(fabs(fterm), 104.0));
+                const float xs = big ? ex : 1.f;                          // scale of the carried terms
+                const float F = big ? 1.f : (fterm > -104.0 ? ex : 0.f);  // the floor term
+                const float b = fmaf(xs * sw, qs.y, F), gq = xs * qs.x;
+                float wn[4];
+#pragma unroll
+                for (int i = 0; i < 4; ++i) wn[i] = act ? (((em >> i) & 1u) ? fmaf(gq, w[i], b) : 0.f) : w[i];
+                const float s2 = group_sum<G>(sum4(wn));
                 const int e = act ? exp2_of(s2) : 0;
                 const float sc = pow2_neg(e);
-                w = wn * sc;
+#pragma unroll
+                for (int i = 0; i < 4; ++i) w[i] = wn[i] * sc;
                 sw = act ? s2 * sc : sw;
-                logU = act ? lu + (double)e * 0.69314718055994530942 : logU;
+                const double lu = logU + (double)n * tb.lr + (big ? fterm : 0.0) - 999.0 * (double)sh +
+                                  (double)e * 0.69314718055994530942;
+                logU = act ? lu : logU;
                 nextp = act ? p : nextp;
                 cc = act ? cc - 1 : cc;
                 if (act && cc == 0) {
-                    A.ckptB[(wb + ci) * LM + kl] = w;
+                    *reinterpret_cast<float4*>(A.ckptB + (wb + ci) * LM + sl) = make_float4(w[0], w[1], w[2], w[3]);
                     if (kl == 0) A.ckptU[wb + ci] = logU;
                     --ci;
                     cc = C;
                 }
             }
-            pv = pn;
-            ev = en;
-            hv = hn;
+#pragma unroll
+            for (uint32_t i = 0; i < R; ++i) {
+                pv[i] = pn[i];
+                ev[i] = en[i];
+                hv[i] = hn[i];
+            }
         }
     }
 }
@@ -701,7 +729,7 @@ cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
 
 template <int LM>
 cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
-    constexpr uint32_t kChainsPerWarp = 32 / LM;
+    constexpr uint32_t kChainsPerWarp = 128 / LM;  // LM / 4 lanes per chain
     const unsigned long long warps = 2ull * ((a.B + kChainsPerWarp - 1) / kChainsPerWarp);  // forward + backward
     anchor_chain_kernel<LM><<<(uint32_t)((warps + 3) / 4), 128, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
