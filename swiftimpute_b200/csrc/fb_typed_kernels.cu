@@ -743,7 +743,7 @@ cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
 // The window (anchors rebuilt from one checkpoint) fixes where rounding
 // restarts, so it must not depend on the batch: one value for every L. The
 // CTA size changes nothing numerically and shrinks as the records grow.
-uint32_t typed_default_window(uint32_t) { return 4u; }
+uint32_t typed_default_window(uint32_t) { return 2u; }
 uint32_t typed_default_threads(uint32_t lmax) { return lmax <= 8 ? 128u : (lmax <= 16 ? 64u : 32u); }
 
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C) {
