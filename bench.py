@@ -40,6 +40,11 @@ sys.path.insert(0, str(ROOT))
 CONFIGS = {
     "dense-cohort": dict(M=50_000, N=4432, B=10_000, n_typed=3000, founders=100, L=8, ne=20000, seed=1),
     "plain-small": dict(M=1644, N=4432, B=444, every=5, founders=40, L=8, ne=10000, seed=0),
+    # serving: an 8,000 x 120,000 panel (MAF ~ Beta(0.3, 0.6), switch 0.002); requests of 1-512 samples
+    # (log-uniform) over 1,000-50,000 markers (log-uniform length, uniform start), typed every 20th
+    # marker, L from {4, 8, 16}, Poisson arrivals
+    "serving": dict(M=120_000, N=8000, founders=200, beta=(0.3, 0.6), switch=0.002, every=20, ne=20000, seed=4,
+                    pool=1024, rate=200.0, seconds=10.0),
 }
 ALGO_BYTES_PER_CELL = 7  # 1 B genotype code in, 4 B dosage + 2 B haplotype alleles out
 POST_BYTES_PER_CELL = 6  # the posterior pass writes the outputs: 4 B dosage + 2 B alleles
@@ -58,6 +63,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--rate", type=float, default=0.0, help="serving: request arrivals per second")
+    ap.add_argument("--seconds", type=float, default=0.0, help="serving: length of the arrival window")
     return ap.parse_args()
 
 
@@ -191,6 +198,86 @@ def run_reference(args, cfg):
                                    "so its recurrences run through the FP64 C port"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
+    print(json.dumps(line), flush=True)
+
+
+def run_serving(args, cfg):
+    """Serving workload: Poisson arrivals submitted through the si_serve_* API
+    on one GPU; latency percentiles from the server, throughput over the run."""
+    import threading
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200 import synth
+    from swiftimpute_b200.engine import Engine, Server
+    rank = int(os.environ.get("RANK", "0"))
+    M, Nh = cfg["M"], cfg["N"]
+    panel, pos, _ = synth.make_panel(M, Nh, cfg["founders"], cfg["beta"], cfg["switch"], 0.005, seed=cfg["seed"])
+    pool, _, _ = synth.make_targets(panel, cfg["pool"], synth.typed_every(M, cfg["every"]), seed=cfg["seed"] + 1)
+    rate = args.rate or cfg["rate"]
+    seconds = args.seconds or cfg["seconds"]
+    rng = np.random.default_rng(cfg["seed"] + 2)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5) + 16))
+    arrivals = arrivals[arrivals < seconds]
+    reqs = []
+    for i in range(len(arrivals)):
+        n = int(np.exp(rng.uniform(0, np.log(512))))
+        length = int(np.exp(rng.uniform(np.log(1000), np.log(50_000))))
+        m0 = int(rng.integers(0, M - length))
+        rows = rng.integers(0, pool.shape[0], size=n)
+        reqs.append((m0, m0 + length, int(rng.choice([4, 8, 16])), np.ascontiguousarray(pool[rows, m0:m0 + length])))
+    cells = sum(r[3].size for r in reqs)
+    eng = Engine(int(os.environ.get("LOCAL_RANK", "0")))
+    eng.upload_panel(panel)
+    eng.set_map(pos)
+    eng.pbwt_build()
+    params = N.default_params(ne=cfg["ne"])
+    # warm-up: one request per slot count, so tables and selections exist before timing
+    with Server(eng, params) as srv:
+        for L in (4, 8, 16):
+            srv.wait(srv.submit(0, 2000, pool[:2, :2000], num_states=L, index_origin=N.INDEX_GLOBAL))
+    clocks = clock_sampler_start(int(os.environ.get("LOCAL_RANK", "0")))
+    srv = Server(eng, params)
+    tickets = [None] * len(reqs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for i, (a, b, L, codes) in enumerate(reqs):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(a, b, codes, num_states=L, index_origin=N.INDEX_GLOBAL, sample_id_base=i << 10)
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    for t in tickets:
+        srv.wait(t)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.stop()
+    clock_info = clock_sampler_stop(clocks)
+    eng.close()
+    if rank != 0:
+        return
+    busy_s = st["busy_ms"] / 1e3
+    peak, peak_kind = peaks()
+    line = {
+        "metric": "imputed genotypes/s", "mode": "serving", "value": st["cells"] / wall,
+        "unit": "cells/s over the run (samples x markers, typed included)", "n_gpus": 1,
+        "higher_is_better": True, "dtype": "f32", "data": "synthetic (seeded generator with the config's shape)",
+        "config": {"workload": f"serving: {Nh} haplotypes x {M} markers, Poisson {rate:g} req/s for {seconds:g} s, "
+                               f"1-512 samples x 1,000-50,000 markers per request, typed every {cfg['every']}th, "
+                               "L in {4, 8, 16}, resident index", "requests": len(reqs), "cells": int(cells)},
+        "offered_cells_per_s": cells / seconds,
+        "latency_ms": {"p50": st["latency_p50_ms"], "p99": st["latency_p99_ms"], "max": st["latency_max_ms"]},
+        "busy_fraction": busy_s / wall, "batches": st["batches"],
+        "busy_cells_per_s": st["cells"] / busy_s if busy_s > 0 else None,
+        "busy_roofline": {"bound": "hbm", "achieved": ALGO_BYTES_PER_CELL * st["cells"] / busy_s / 1e9 if busy_s else None,
+                          "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
+                          "note": "7 B per cell over busy intervals (host copies included)"},
+        "completed": st["completed"], "failed": st["failed"],
+    }
+    if clock_info:
+        line["clocks"] = clock_info
     print(json.dumps(line), flush=True)
 
 
@@ -349,7 +436,13 @@ def main():
         cfg["M"] = args.markers
         if "n_typed" in cfg:
             cfg["n_typed"] = max(1, round(cfg["n_typed"] * args.markers / CONFIGS[args.config]["M"]))
-    if args.impl == "reference":
+    if args.config == "serving":
+        if args.impl == "reference":
+            print(json.dumps({"impl": "reference", "mode": "serving", "unavailable":
+                              "the reference has no request queue; its CPU path is timed on the batch configs"}))
+            return
+        run_serving(args, cfg)
+    elif args.impl == "reference":
         run_reference(args, cfg)
     else:
         run_ours(args, cfg)

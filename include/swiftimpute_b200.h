@@ -244,6 +244,67 @@ si_status si_last_timings(si_ctx* ctx, float* ms3);
  * [3] posterior pass (or the whole full-chain kernel). Waits for the call. */
 si_status si_last_kernel_ms(si_ctx* ctx, float* ms4);
 
+/* ---- Serving: requests of any size over a resident panel and index.
+ *
+ * The reference imputes one target set per Imputer::impute call
+ * (imputer.cpp:787-1042, batches of max_batch_size over one panel) and has no
+ * request queue. A server owns a ctx (panel, map and PBWT index already set
+ * up) and one worker thread. Requests are queued from any thread; the worker
+ * forms each launch from the queue in arrival order (continuous batching: a
+ * request that arrives while a launch runs joins the next one), admits
+ * requests while the launch stays within max_batch_cells and within the ctx's
+ * HBM budget, and runs them as one uneven batch (si_impute_jobs_device), so a
+ * request's results never depend on the requests beside it. While a server
+ * runs, no other call may use its ctx. */
+typedef struct si_server si_server;
+
+typedef struct {
+    uint64_t max_batch_cells;  /* samples x markers per launch; 0 = 2^28 */
+    uint32_t max_wait_us;      /* how long the oldest queued request waits for company; 0 = 200 */
+    uint32_t max_queue;        /* queued requests before si_serve_submit refuses; 0 = 65536 */
+} si_serve_config;
+
+typedef struct {
+    uint32_t m_begin, m_end;   /* panel markers [m_begin, m_end) */
+    uint32_t num_states;       /* L, 1..32 */
+    int32_t index_origin;      /* SI_INDEX_* (as si_region) */
+    uint32_t n_samples;
+    uint32_t reserved;
+    uint64_t sample_id_base;   /* Philox id of the first sample; sample i uses base + i */
+    const uint8_t* codes;      /* host [n_samples][m_end - m_begin] genotype codes */
+    float* dosage;             /* host [n_samples][len], or NULL */
+    uint8_t* haps;             /* host [n_samples][2][len], or NULL */
+    float* hap_prob;           /* host [n_samples][len][2], or NULL */
+} si_request;
+
+typedef struct {
+    uint64_t submitted, completed, failed, cancelled, batches, cells;
+    double latency_p50_ms, latency_p99_ms, latency_max_ms;  /* submit -> finished, completed requests */
+    double busy_ms;            /* worker time inside launches (copies included) */
+    double wall_ms;            /* since si_serve_start */
+} si_serve_statistics;
+
+/* Start a server on ctx with fixed imputation parameters (num_states is taken
+ * from each request). params->transition_mode must be SI_TRANS_MATRIX0. */
+si_status si_serve_start(si_ctx* ctx, const si_impute_params* params, const si_serve_config* cfg, si_server** out);
+/* Queue a request. Its host buffers must stay valid until it finishes. A
+ * request larger than max_batch_cells, or than the HBM budget allows alone,
+ * is refused here with SI_ERR_BUDGET. Thread-safe. */
+si_status si_serve_submit(si_server* srv, const si_request* req, uint64_t* ticket);
+/* *finished = 1 once the request has finished; *result is then its status
+ * and the ticket is released. Thread-safe, never blocks on the device. */
+si_status si_serve_poll(si_server* srv, uint64_t ticket, int* finished, si_status* result);
+/* Wait up to timeout_ms (0 = no limit) for the request; SI_ERR_TIMEOUT if it
+ * is still running (the ticket stays valid). Thread-safe. */
+si_status si_serve_wait(si_server* srv, uint64_t ticket, uint32_t timeout_ms, si_status* result);
+/* Cancel a queued request (it finishes as SI_ERR_CANCELLED, outputs untouched);
+ * SI_ERR_STATE if it is already in a launch or finished. Thread-safe. */
+si_status si_serve_cancel(si_server* srv, uint64_t ticket);
+si_status si_serve_stats(si_server* srv, si_serve_statistics* out);
+/* Cancel queued requests, finish the running launch, join the worker, free the
+ * server's buffers. The ctx is usable again afterwards. */
+si_status si_serve_stop(si_server* srv);
+
 #ifdef __cplusplus
 }
 #endif

@@ -72,6 +72,26 @@ class Job(ctypes.Structure):
 
 
 # (name, restype, argtypes) for every symbol the header declares.
+class ServeConfig(ctypes.Structure):
+    """Mirror of ``si_serve_config``."""
+    _fields_ = [("max_batch_cells", c_uint64), ("max_wait_us", c_uint32), ("max_queue", c_uint32)]
+
+
+class Request(ctypes.Structure):
+    """Mirror of ``si_request``."""
+    _fields_ = [("m_begin", c_uint32), ("m_end", c_uint32), ("num_states", c_uint32), ("index_origin", c_int32),
+                ("n_samples", c_uint32), ("reserved", c_uint32), ("sample_id_base", c_uint64),
+                ("codes", c_void_p), ("dosage", c_void_p), ("haps", c_void_p), ("hap_prob", c_void_p)]
+
+
+class ServeStatistics(ctypes.Structure):
+    """Mirror of ``si_serve_statistics``."""
+    _fields_ = [("submitted", c_uint64), ("completed", c_uint64), ("failed", c_uint64), ("cancelled", c_uint64),
+                ("batches", c_uint64), ("cells", c_uint64), ("latency_p50_ms", ctypes.c_double),
+                ("latency_p99_ms", ctypes.c_double), ("latency_max_ms", ctypes.c_double),
+                ("busy_ms", ctypes.c_double), ("wall_ms", ctypes.c_double)]
+
+
 SIGNATURES = [
     ("si_abi_version", c_int, []),
     ("si_status_string", c_char_p, [c_int]),
@@ -99,6 +119,13 @@ SIGNATURES = [
      [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("si_last_timings", c_int, [c_void_p, POINTER(c_float)]),
     ("si_last_kernel_ms", c_int, [c_void_p, POINTER(c_float)]),
+    ("si_serve_start", c_int, [c_void_p, POINTER(ImputeParams), POINTER(ServeConfig), POINTER(c_void_p)]),
+    ("si_serve_submit", c_int, [c_void_p, POINTER(Request), POINTER(c_uint64)]),
+    ("si_serve_poll", c_int, [c_void_p, c_uint64, POINTER(c_int), POINTER(c_int)]),
+    ("si_serve_wait", c_int, [c_void_p, c_uint64, c_uint32, POINTER(c_int)]),
+    ("si_serve_cancel", c_int, [c_void_p, c_uint64]),
+    ("si_serve_stats", c_int, [c_void_p, POINTER(ServeStatistics)]),
+    ("si_serve_stop", c_int, [c_void_p]),
 ]
 
 _lib = None

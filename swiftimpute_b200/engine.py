@@ -181,3 +181,84 @@ class Engine:
         ms = (c_float * 3)()
         self._check(self.lib.si_last_timings(self.h, ms))
         return tuple(ms)
+
+
+class Server:
+    """Request queue with continuous batching over an Engine's resident panel
+    and index (the si_serve_* C ABI). While it runs, the Engine must not be
+    used for anything else; ``stop()`` hands it back.
+
+    ``submit`` copies nothing: it keeps the request's code array and its output
+    arrays alive until ``wait``/``poll`` reports the request finished.
+    """
+
+    def __init__(self, engine: Engine, params: N.ImputeParams | None = None, *, max_batch_cells: int = 0,
+                 max_wait_us: int = 0, max_queue: int = 0):
+        self.engine = engine
+        self.lib = engine.lib
+        self.params = params or N.default_params()
+        cfg = N.ServeConfig(max_batch_cells, max_wait_us, max_queue)
+        h = c_void_p()
+        engine._check(self.lib.si_serve_start(engine.h, byref(self.params), byref(cfg), byref(h)))
+        self.h = h
+        self._held = {}
+
+    def submit(self, m_begin: int, m_end: int, codes: np.ndarray, *, num_states: int = 8,
+               index_origin: int = N.INDEX_REGION, sample_id_base: int = 0, hap_prob: bool = False) -> int:
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        n, length = codes.shape
+        if length != m_end - m_begin:
+            raise ValueError("codes must have m_end - m_begin columns")
+        out = {"dosage": np.empty((n, length), np.float32), "haps": np.empty((n, 2, length), np.uint8)}
+        if hap_prob:
+            out["hap_prob"] = np.empty((n, length, 2), np.float32)
+        req = N.Request(m_begin, m_end, num_states, index_origin, n, 0, sample_id_base, _ptr(codes),
+                        _ptr(out["dosage"]), _ptr(out["haps"]), _ptr(out.get("hap_prob")))
+        t = c_uint64()
+        st = self.lib.si_serve_submit(self.h, byref(req), byref(t))
+        if st != N.SI_OK:
+            raise N.SIError(st, "request refused")
+        self._held[t.value] = (codes, out)
+        return t.value
+
+    def _collect(self, ticket: int, status: int):
+        codes, out = self._held.pop(ticket)
+        if status != N.SI_OK:
+            raise N.SIError(status, f"request {ticket} finished with an error")
+        return out
+
+    def poll(self, ticket: int):
+        """None while the request runs, else its outputs (raises SIError on failure)."""
+        fin, st = ctypes.c_int(), ctypes.c_int()
+        s = self.lib.si_serve_poll(self.h, ticket, byref(fin), byref(st))
+        if s != N.SI_OK:
+            raise N.SIError(s, "unknown ticket")
+        return self._collect(ticket, st.value) if fin.value else None
+
+    def wait(self, ticket: int, timeout_ms: int = 0):
+        st = ctypes.c_int()
+        s = self.lib.si_serve_wait(self.h, ticket, timeout_ms, byref(st))
+        if s != N.SI_OK:
+            raise N.SIError(s, "wait failed" if s != 6 else "timed out")
+        return self._collect(ticket, st.value)
+
+    def cancel(self, ticket: int) -> bool:
+        """True if the request was still queued and is now cancelled."""
+        return self.lib.si_serve_cancel(self.h, ticket) == N.SI_OK
+
+    def stats(self) -> dict:
+        s = N.ServeStatistics()
+        self.engine._check(self.lib.si_serve_stats(self.h, byref(s)))
+        return {name: getattr(s, name) for name, _ in N.ServeStatistics._fields_}
+
+    def stop(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.si_serve_stop(self.h)
+            self.h = None
+            self._held.clear()
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.stop()
