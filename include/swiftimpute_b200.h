@@ -259,7 +259,8 @@ si_status si_last_kernel_ms(si_ctx* ctx, float* ms4);
 typedef struct si_server si_server;
 
 typedef struct {
-    uint64_t max_batch_cells;  /* samples x markers per launch; 0 = 2^28 */
+    uint64_t max_batch_cells;  /* samples x markers per launch; 0 = 2^25. Both staging slots
+                                  (7 B per cell pinned and on the device) are allocated at start */
     uint32_t max_wait_us;      /* how long the oldest queued request waits for company; 0 = 200 */
     uint32_t max_queue;        /* queued requests before si_serve_submit refuses; 0 = 65536 */
 } si_serve_config;

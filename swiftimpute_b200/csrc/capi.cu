@@ -46,6 +46,13 @@ void dev_free(si_ctx* ctx, DeviceBuffer& buf) {
 
 si_status dev_reserve(si_ctx* ctx, DeviceBuffer& buf, size_t bytes) {
     if (buf.ptr && buf.bytes >= bytes) return SI_OK;
+    if (buf.ptr) {
+        // regrowing: take half again the old size when the budget allows, so
+        // slowly rising sizes do not reallocate (and synchronise) every call
+        const size_t roomy = std::max(bytes, buf.bytes + buf.bytes / 2);
+        const uint64_t after = ctx->used - buf.bytes + ((roomy + 255) & ~size_t(255));
+        if (roomy > bytes && after <= ctx->budget) return dev_alloc(ctx, buf, roomy);
+    }
     return dev_alloc(ctx, buf, bytes);
 }
 

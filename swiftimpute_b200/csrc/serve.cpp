@@ -5,8 +5,10 @@
 // region (its marker slice, slot count and index origin; equal regions are
 // shared) and one job per sample, and the whole launch runs through
 // si_impute_jobs_device. Codes are gathered into one pinned buffer, copied to
-// the device once, and the outputs come back with one copy per array before
-// they are scattered into the requests' own buffers.
+// the device once, and the outputs come back with one copy per array. Two
+// staging slots alternate: while the worker runs launch k+1 on the device, a
+// completion thread waits for launch k's copies and scatters its outputs into
+// the requests' own buffers.
 #include "si_internal.hpp"
 
 #include <algorithm>
@@ -88,13 +90,54 @@ struct si_server {
     std::vector<double> latency_ms;
     Clock::time_point t_start;
 
-    // worker-only
-    si::DeviceBuffer d_geno, d_dos, d_haps, d_hp;
-    Pinned h_geno, h_dos, h_haps, h_hp;
+    // staging slots: the worker fills one while the completion thread drains the other
+    struct Slot {
+        si::DeviceBuffer d_geno, d_dos, d_haps, d_hp;
+        Pinned h_geno, h_dos, h_haps, h_hp;
+        cudaEvent_t copied = nullptr;  // the launch's output copies are done
+        std::vector<std::shared_ptr<Pending>> batch;
+        std::vector<uint64_t> first;   // cell offset of each request
+        si_status status = SI_OK;
+        bool busy = false;             // handed to the completion thread
+        Clock::time_point t_launch;
+    } slot[2];
+    std::condition_variable cv_slot;   // slot handed over / released
+    std::thread completer;
+    bool worker_done = false;          // the worker has left its loop (set under mu)
 };
 
 namespace {
 
+// Run body(i) for i in [0, n) on up to 8 threads, split so that each thread
+// gets about the same number of bytes (weight(i)).
+template <class W, class F>
+void par_requests(size_t n, W weight, F body) {
+    uint64_t total = 0;
+    for (size_t i = 0; i < n; ++i) total += weight(i);
+    const unsigned hw = std::max(2u, std::thread::hardware_concurrency());
+    const unsigned T = (unsigned)std::min<uint64_t>(std::min(8u, hw / 2), total / (4u << 20) + 1);
+    if (T <= 1 || n < 2) {
+        for (size_t i = 0; i < n; ++i) body(i);
+        return;
+    }
+    std::vector<size_t> cut{0};
+    uint64_t acc = 0;
+    for (size_t i = 0; i < n; ++i) {
+        acc += weight(i);
+        if (acc * T >= total * cut.size() && cut.size() < T) cut.push_back(i + 1);
+    }
+    cut.push_back(n);
+    std::vector<std::thread> th;
+    for (size_t t = 1; t + 1 < cut.size(); ++t)
+        th.emplace_back([&, a = cut[t], b = cut[t + 1]] {
+            for (size_t i = a; i < b; ++i) body(i);
+        });
+    for (size_t i = cut[0]; i < cut[1]; ++i) body(i);
+    for (auto& x : th) x.join();
+}
+
+// Grow-only pinned staging (sized once for max_batch_cells at start; only
+// P(hap=1) staging is allocated on first use).
 si_status pinned_reserve(Pinned& b, size_t bytes) {
     if (b.ptr && b.bytes >= bytes) return SI_OK;
     if (b.ptr) cudaFreeHost(b.ptr);
@@ -111,19 +154,22 @@ si_status pinned_reserve(Pinned& b, size_t bytes) {
 }
 
 // Bytes of ctx memory the next launch can reuse or regrow (per-call scratch).
-uint64_t reclaimable(const si_server* S) {
+uint64_t reclaimable(const si_server* S, int k) {
     const si_ctx* c = S->ctx;
+    const auto& z = S->slot[k];
     uint64_t b = 0;
     for (const si::DeviceBuffer* x : {&c->t_counts, &c->t_aoff, &c->t_woff, &c->t_apos, &c->t_acode, &c->t_aem,
                                       &c->t_wsample, &c->t_ckF, &c->t_ckB, &c->t_ckU, &c->job_regions,
-                                      &c->job_samples, &S->d_geno, &S->d_dos, &S->d_haps, &S->d_hp})
+                                      &c->job_samples, &z.d_geno, &z.d_dos, &z.d_haps, &z.d_hp})
         b += x->bytes;
     return b;
 }
 
-uint64_t headroom(const si_server* S) {
+// Device bytes a launch into slot k may use: the budget less everything the
+// ctx holds that this launch cannot reuse (the other slot's staging included).
+uint64_t headroom(const si_server* S, int k) {
     const si_ctx* c = S->ctx;
-    const uint64_t fixed = c->used - std::min<uint64_t>(c->used, reclaimable(S));
+    const uint64_t fixed = c->used - std::min<uint64_t>(c->used, reclaimable(S, k));
     return c->budget > fixed ? c->budget - fixed : 0;
 }
 
@@ -151,12 +197,16 @@ void trim_region_cache(si_server* S) {
     c->region_sel.clear();
 }
 
-si_status run_batch(si_server* S, const std::vector<std::shared_ptr<Pending>>& batch) {
+// Device stage of a launch into slot k: gather codes, copy in, impute, queue
+// the output copies and the event that marks them done.
+si_status launch_batch(si_server* S, int k) {
     si_ctx* ctx = S->ctx;
+    auto& z = S->slot[k];
+    const auto& batch = z.batch;
     std::vector<si_region> regions;
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, int32_t>, uint32_t> region_id;
     std::vector<si_job> jobs;
-    std::vector<uint64_t> first(batch.size());
+    z.first.assign(batch.size(), 0);
     uint64_t off = 0;
     bool any_hp = false;
     for (size_t b = 0; b < batch.size(); ++b) {
@@ -172,7 +222,7 @@ si_status run_batch(si_server* S, const std::vector<std::shared_ptr<Pending>>& b
         } else {
             r = it->second;
         }
-        first[b] = off;
+        z.first[b] = off;
         for (uint32_t i = 0; i < q.n_samples; ++i) {
             const uint64_t o = off + (uint64_t)i * len;
             jobs.push_back(si_job{r, 0u, o, o, q.sample_id_base + i});
@@ -181,39 +231,51 @@ si_status run_batch(si_server* S, const std::vector<std::shared_ptr<Pending>>& b
         any_hp |= q.hap_prob != nullptr;
     }
     const uint64_t cells = off;
-    si_status st = pinned_reserve(S->h_geno, cells);
-    if (st == SI_OK) st = pinned_reserve(S->h_dos, cells * 4);
-    if (st == SI_OK) st = pinned_reserve(S->h_haps, cells * 2);
-    if (st == SI_OK && any_hp) st = pinned_reserve(S->h_hp, cells * 8);
+    si_status st = pinned_reserve(z.h_geno, cells);
+    if (st == SI_OK) st = pinned_reserve(z.h_dos, cells * 4);
+    if (st == SI_OK) st = pinned_reserve(z.h_haps, cells * 2);
+    if (st == SI_OK && any_hp) st = pinned_reserve(z.h_hp, cells * 8);
     if (st != SI_OK) return si::fail(ctx, st, "pinned staging for a serving launch");
-    if ((st = si::dev_reserve(ctx, S->d_geno, cells)) != SI_OK) return st;
-    if ((st = si::dev_reserve(ctx, S->d_dos, cells * 4)) != SI_OK) return st;
-    if ((st = si::dev_reserve(ctx, S->d_haps, cells * 2)) != SI_OK) return st;
-    if (any_hp && (st = si::dev_reserve(ctx, S->d_hp, cells * 8)) != SI_OK) return st;
-    for (size_t b = 0; b < batch.size(); ++b)
-        std::memcpy((uint8_t*)S->h_geno.ptr + first[b], batch[b]->req.codes, cells_of(batch[b]->req));
+    if ((st = si::dev_reserve(ctx, z.d_geno, cells)) != SI_OK) return st;
+    if ((st = si::dev_reserve(ctx, z.d_dos, cells * 4)) != SI_OK) return st;
+    if ((st = si::dev_reserve(ctx, z.d_haps, cells * 2)) != SI_OK) return st;
+    if (any_hp && (st = si::dev_reserve(ctx, z.d_hp, cells * 8)) != SI_OK) return st;
+    par_requests(
+        batch.size(), [&](size_t b) { return cells_of(batch[b]->req); },
+        [&](size_t b) { std::memcpy((uint8_t*)z.h_geno.ptr + z.first[b], batch[b]->req.codes, cells_of(batch[b]->req)); });
     cudaStream_t s = ctx->stream;
-    cudaError_t e = cudaMemcpyAsync(S->d_geno.ptr, S->h_geno.ptr, cells, cudaMemcpyHostToDevice, s);
+    cudaError_t e = cudaMemcpyAsync(z.d_geno.ptr, z.h_geno.ptr, cells, cudaMemcpyHostToDevice, s);
     if (e != cudaSuccess) return si::cuda_fail(ctx, e, "serving input copy");
     st = si_impute_jobs_device(ctx, &S->params, regions.data(), (uint32_t)regions.size(), jobs.data(),
-                               (uint32_t)jobs.size(), (const uint8_t*)S->d_geno.ptr, (float*)S->d_dos.ptr,
-                               any_hp ? (float*)S->d_hp.ptr : nullptr, (uint8_t*)S->d_haps.ptr, s);
+                               (uint32_t)jobs.size(), (const uint8_t*)z.d_geno.ptr, (float*)z.d_dos.ptr,
+                               any_hp ? (float*)z.d_hp.ptr : nullptr, (uint8_t*)z.d_haps.ptr, s);
     if (st != SI_OK) return st;
-    e = cudaMemcpyAsync(S->h_dos.ptr, S->d_dos.ptr, cells * 4, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaMemcpyAsync(S->h_haps.ptr, S->d_haps.ptr, cells * 2, cudaMemcpyDeviceToHost, s);
+    e = cudaMemcpyAsync(z.h_dos.ptr, z.d_dos.ptr, cells * 4, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(z.h_haps.ptr, z.d_haps.ptr, cells * 2, cudaMemcpyDeviceToHost, s);
     if (e == cudaSuccess && any_hp)
-        e = cudaMemcpyAsync(S->h_hp.ptr, S->d_hp.ptr, cells * 8, cudaMemcpyDeviceToHost, s);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+        e = cudaMemcpyAsync(z.h_hp.ptr, z.d_hp.ptr, cells * 8, cudaMemcpyDeviceToHost, s);
+    if (e == cudaSuccess) e = cudaEventRecord(z.copied, s);
     if (e != cudaSuccess) return si::cuda_fail(ctx, e, "serving output copy");
-    // a request's jobs are consecutive, so each output is one contiguous block
-    for (size_t b = 0; b < batch.size(); ++b) {
-        const si_request& q = batch[b]->req;
-        const uint64_t n = cells_of(q);
-        if (q.dosage) std::memcpy(q.dosage, (const float*)S->h_dos.ptr + first[b], n * 4);
-        if (q.haps) std::memcpy(q.haps, (const uint8_t*)S->h_haps.ptr + 2 * first[b], n * 2);
-        if (q.hap_prob) std::memcpy(q.hap_prob, (const float*)S->h_hp.ptr + 2 * first[b], n * 8);
-    }
     trim_region_cache(S);
+    return SI_OK;
+}
+
+// Host stage: wait for slot k's copies, scatter into the requests' buffers (a
+// request's jobs are consecutive, so each output is one contiguous block).
+si_status complete_batch(si_server* S, int k) {
+    auto& z = S->slot[k];
+    if (z.status != SI_OK) return z.status;
+    const cudaError_t e = cudaEventSynchronize(z.copied);
+    if (e != cudaSuccess) return SI_ERR_CUDA;
+    par_requests(
+        z.batch.size(), [&](size_t b) { return cells_of(z.batch[b]->req); },
+        [&](size_t b) {
+            const si_request& q = z.batch[b]->req;
+            const uint64_t n = cells_of(q), f = z.first[b];
+            if (q.dosage) std::memcpy(q.dosage, (const float*)z.h_dos.ptr + f, n * 4);
+            if (q.haps) std::memcpy(q.haps, (const uint8_t*)z.h_haps.ptr + 2 * f, n * 2);
+            if (q.hap_prob) std::memcpy(q.hap_prob, (const float*)z.h_hp.ptr + 2 * f, n * 8);
+        });
     return SI_OK;
 }
 
@@ -234,6 +296,7 @@ void finish(si_server* S, Pending& p, si_status status, Clock::time_point t) {
 void worker_main(si_server* S) {
     cudaSetDevice(S->ctx->device);
     std::unique_lock<std::mutex> lk(S->mu);
+    int k = 0;
     for (;;) {
         S->cv_work.wait(lk, [&] { return S->stopping || !S->queue.empty(); });
         if (S->stopping) break;
@@ -242,9 +305,12 @@ void worker_main(si_server* S) {
         while (!S->stopping && !S->queue.empty() && S->queued_cells < S->max_cells && Clock::now() < deadline)
             S->cv_work.wait_until(lk, deadline);
         if (S->stopping) break;
+        // the slot must be drained by the completion thread before it is refilled
+        S->cv_slot.wait(lk, [&] { return !S->slot[k].busy; });
         if (S->queue.empty()) continue;  // everything queued was cancelled meanwhile
-        const uint64_t room = headroom(S);
-        std::vector<std::shared_ptr<Pending>> batch;
+        const uint64_t room = headroom(S, k);
+        auto& z = S->slot[k];
+        z.batch.clear();
         Need need;
         uint64_t cells = 0;
         while (!S->queue.empty()) {
@@ -254,7 +320,7 @@ void worker_main(si_server* S) {
             Need next = need;
             add_need(S, next, p->req);
             if (next.bytes() > room) {
-                if (!batch.empty()) break;
+                if (!z.batch.empty()) break;
                 // alone it does not fit what the budget leaves: refuse it, keep serving
                 S->queue.pop_front();
                 S->queued_cells -= c;
@@ -265,20 +331,42 @@ void worker_main(si_server* S) {
             S->queue.pop_front();
             S->queued_cells -= c;
             p->state = Pending::RUNNING;
-            batch.push_back(p);
+            z.batch.push_back(p);
             need = next;
             cells += c;
         }
-        if (batch.empty()) continue;
+        if (z.batch.empty()) continue;
         lk.unlock();
-        const auto t0 = Clock::now();
-        const si_status rs = run_batch(S, batch);
+        z.t_launch = Clock::now();
+        z.status = launch_batch(S, k);
         const auto t1 = Clock::now();
         lk.lock();
-        S->st.busy_ms += ms_between(t0, t1);
+        S->st.busy_ms += ms_between(z.t_launch, t1);
         S->st.batches++;
-        for (auto& p : batch) finish(S, *p, rs, t1);
+        z.busy = true;
+        S->cv_slot.notify_all();
+        k ^= 1;
+    }
+}
+
+// Drains slots in launch order: their copies, the scatter, the requests' status.
+void completer_main(si_server* S) {
+    cudaSetDevice(S->ctx->device);
+    std::unique_lock<std::mutex> lk(S->mu);
+    int k = 0;
+    for (;;) {
+        S->cv_slot.wait(lk, [&] { return S->slot[k].busy || (S->stopping && S->worker_done); });
+        if (!S->slot[k].busy) break;
+        lk.unlock();
+        const si_status rs = complete_batch(S, k);
+        const auto t = Clock::now();
+        lk.lock();
+        for (auto& p : S->slot[k].batch) finish(S, *p, rs, t);
+        S->slot[k].batch.clear();
+        S->slot[k].busy = false;
         S->cv_done.notify_all();
+        S->cv_slot.notify_all();
+        k ^= 1;
     }
 }
 
@@ -294,11 +382,50 @@ si_status si_serve_start(si_ctx* ctx, const si_impute_params* params, const si_s
     auto* S = new si_server();
     S->ctx = ctx;
     S->params = *params;
-    S->max_cells = cfg && cfg->max_batch_cells ? cfg->max_batch_cells : (1ull << 28);
+    S->max_cells = cfg && cfg->max_batch_cells ? cfg->max_batch_cells : (1ull << 25);
     S->max_wait_us = cfg && cfg->max_wait_us ? cfg->max_wait_us : 200u;
     S->max_queue = cfg && cfg->max_queue ? cfg->max_queue : 65536u;
     S->t_start = Clock::now();
-    S->worker = std::thread(worker_main, S);
+    for (auto& z : S->slot) {
+        if (cudaSetDevice(ctx->device) != cudaSuccess ||
+            cudaEventCreateWithFlags(&z.copied, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            for (auto& y : S->slot)
+                if (y.copied) cudaEventDestroy(y.copied);
+            delete S;
+            return si::fail(ctx, SI_ERR_CUDA, "serving events");
+        }
+    }
+    // staging for a full launch in both slots, allocated once: growing pinned
+    // memory or device buffers between launches stalls the device
+    for (auto& z : S->slot) {
+        const uint64_t c = S->max_cells;
+        si_status st = pinned_reserve(z.h_geno, c);
+        if (st == SI_OK) st = pinned_reserve(z.h_dos, c * 4);
+        if (st == SI_OK) st = pinned_reserve(z.h_haps, c * 2);
+        if (st == SI_OK) st = si::dev_reserve(ctx, z.d_geno, c);
+        if (st == SI_OK) st = si::dev_reserve(ctx, z.d_dos, c * 4);
+        if (st == SI_OK) st = si::dev_reserve(ctx, z.d_haps, c * 2);
+        if (st != SI_OK) {
+            for (auto& y : S->slot) {
+                si::dev_free(ctx, y.d_geno);
+                si::dev_free(ctx, y.d_dos);
+                si::dev_free(ctx, y.d_haps);
+                for (Pinned* b : {&y.h_geno, &y.h_dos, &y.h_haps})
+                    if (b->ptr) cudaFreeHost(b->ptr);
+                if (y.copied) cudaEventDestroy(y.copied);
+            }
+            delete S;
+            return si::fail(ctx, st, "serving staging for max_batch_cells");
+        }
+    }
+    S->worker = std::thread([S] {
+        worker_main(S);
+        std::lock_guard<std::mutex> lk(S->mu);
+        S->worker_done = true;
+        S->cv_slot.notify_all();
+    });
+    S->completer = std::thread(completer_main, S);
     *out = S;
     return SI_OK;
 }
@@ -413,18 +540,22 @@ si_status si_serve_stop(si_server* S) {
         S->cv_done.notify_all();
     }
     if (S->worker.joinable()) S->worker.join();
+    if (S->completer.joinable()) S->completer.join();
     {
         // every request has finished: let callers still inside si_serve_wait return first
         std::unique_lock<std::mutex> lk(S->mu);
         S->cv_done.wait(lk, [&] { return S->waiters == 0; });
     }
     si_ctx* c = S->ctx;
-    si::dev_free(c, S->d_geno);
-    si::dev_free(c, S->d_dos);
-    si::dev_free(c, S->d_haps);
-    si::dev_free(c, S->d_hp);
-    for (Pinned* b : {&S->h_geno, &S->h_dos, &S->h_haps, &S->h_hp})
-        if (b->ptr) cudaFreeHost(b->ptr);
+    for (auto& z : S->slot) {
+        si::dev_free(c, z.d_geno);
+        si::dev_free(c, z.d_dos);
+        si::dev_free(c, z.d_haps);
+        si::dev_free(c, z.d_hp);
+        for (Pinned* b : {&z.h_geno, &z.h_dos, &z.h_haps, &z.h_hp})
+            if (b->ptr) cudaFreeHost(b->ptr);
+        if (z.copied) cudaEventDestroy(z.copied);
+    }
     delete S;
     return SI_OK;
 }

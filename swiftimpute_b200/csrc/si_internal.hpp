@@ -116,7 +116,8 @@ namespace si {
 // Allocation under the ctx's HBM budget.
 si_status dev_alloc(si_ctx* ctx, DeviceBuffer& buf, size_t bytes);
 void dev_free(si_ctx* ctx, DeviceBuffer& buf);
-// Grow-only scratch: keep the buffer if it is already large enough.
+// Grow-only scratch: keep the buffer if it is already large enough; a regrown
+// buffer takes 1.5x its old size when the budget allows.
 si_status dev_reserve(si_ctx* ctx, DeviceBuffer& buf, size_t bytes);
 si_status fail(si_ctx* ctx, si_status s, const std::string& msg);
 si_status cuda_fail(si_ctx* ctx, cudaError_t e, const char* what);

@@ -204,14 +204,23 @@ class Server:
         self._held = {}
 
     def submit(self, m_begin: int, m_end: int, codes: np.ndarray, *, num_states: int = 8,
-               index_origin: int = N.INDEX_REGION, sample_id_base: int = 0, hap_prob: bool = False) -> int:
+               index_origin: int = N.INDEX_REGION, sample_id_base: int = 0, hap_prob: bool = False,
+               out: dict | None = None) -> int:
+        """Queue a request; ``out`` may hold caller-owned output arrays
+        (dosage [n][len] f32, haps [n][2][len] u8, hap_prob [n][len][2] f32)."""
         codes = np.ascontiguousarray(codes, dtype=np.uint8)
         n, length = codes.shape
         if length != m_end - m_begin:
             raise ValueError("codes must have m_end - m_begin columns")
-        out = {"dosage": np.empty((n, length), np.float32), "haps": np.empty((n, 2, length), np.uint8)}
-        if hap_prob:
-            out["hap_prob"] = np.empty((n, length, 2), np.float32)
+        if out is None:
+            out = {"dosage": np.empty((n, length), np.float32), "haps": np.empty((n, 2, length), np.uint8)}
+            if hap_prob:
+                out["hap_prob"] = np.empty((n, length, 2), np.float32)
+        shapes = {"dosage": ((n, length), np.float32), "haps": ((n, 2, length), np.uint8),
+                  "hap_prob": ((n, length, 2), np.float32)}
+        for key, arr in out.items():
+            if arr.shape != shapes[key][0] or arr.dtype != shapes[key][1] or not arr.flags.c_contiguous:
+                raise ValueError(f"out[{key!r}] must be a C-contiguous {shapes[key][1].__name__} {shapes[key][0]}")
         req = N.Request(m_begin, m_end, num_states, index_origin, n, 0, sample_id_base, _ptr(codes),
                         _ptr(out["dosage"]), _ptr(out["haps"]), _ptr(out.get("hap_prob")))
         t = c_uint64()

@@ -115,14 +115,15 @@ def test_hbm_budget_admission():
     panel = _setup(eng, seed=93)
     used, _ = eng.memory()
     eng.close()
-    eng = Engine(0, hbm_budget_bytes=used + (64 << 20))
+    eng = Engine(0, hbm_budget_bytes=used + (256 << 20))
     try:
         panel = _setup(eng, seed=93)
         rng = np.random.default_rng(5)
-        big = (rng.random((20000, 3000)) < 0.2).astype(np.uint8) * 3  # 6e7 cells: needs > 64 MB of launch scratch
-        with Server(eng) as srv:
+        # 3.9e6 cells fit one launch (2^22) but not the budget: L=16 scratch is ~86 B per cell at worst
+        big = (rng.random((1300, 3000)) < 0.2).astype(np.uint8) * 3
+        with Server(eng, max_batch_cells=1 << 22) as srv:
             with pytest.raises(N.SIError) as e:
-                srv.submit(0, 3000, big, num_states=8, index_origin=N.INDEX_GLOBAL)
+                srv.submit(0, 3000, big, num_states=16, index_origin=N.INDEX_GLOBAL)
             assert e.value.status == 7
             q = _requests(panel, 1, seed=600)[0]
             out = srv.wait(srv.submit(q["m0"], q["m1"], q["codes"], num_states=q["L"], index_origin=q["origin"]))
