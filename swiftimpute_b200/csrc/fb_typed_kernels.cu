@@ -615,7 +615,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
         for (uint32_t cb = c0; cb < c1; cb += 32) {
             const uint32_t m_raw = cb + lane;
             const bool valid = m_raw < c1;
-            const uint32_t m = valid ? m_raw : c1 - 1;  // lanes past the run repeat its last marker, unwritten
+            const uint32_t m = valid ? m_raw : c1 - 1;  // lanes past the run repeat its last marker
             const uint8_t code_c = code;
             const SlotMasks mk_c = mk;
             {
@@ -628,20 +628,28 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
             const uint32_t u = cu + __popc(bal & le_mask);
             cu += __popc(bal);
             const uint4 meta = recM[u];
-            const float2 qi = tabQS(tb, m - meta.x), qj = tabQS(tb, meta.y - m);
+            float2 qi, qj;
+            if (__all_sync(0xffffffffu, meta.y - meta.x < tb.NT)) {  // every run of the step is in the table
+                qi = __ldg(tb.QS + (m - meta.x));
+                qj = __ldg(tb.QS + (meta.y - m));
+            } else {
+                qi = tabQS(tb, m - meta.x);
+                qj = tabQS(tb, meta.y - m);
+            }
             const bool uni = meta.w == kInfHi;                  // beta uniform
             const bool fin = (meta.w & kInfHi) != kInfHi;       // finite farg': floor term per marker
             float xb = uni ? 0.f : qj.x, yb = uni ? 1.f : qj.y;
             if (__any_sync(0xffffffffu, fin)) {
                 if (fin) {
-                    const double ft = __longlong_as_double(((long long)meta.w << 32) | meta.z) + tabG(tb, meta.y - m);
-                    if (ft > 0.0) {
-                        const float gg = expf(-(float)fmin(ft, 100.0));
-                        xb = gg * qj.x;
-                        yb = fmaf(gg, qj.y, 1.0f);
-                    } else {
-                        yb = qj.y + (ft > -104.0 ? expf((float)ft) : 0.f);
-                    }
+                    // floor e^ft beside Q w' + S; when it dominates (ft > 0) scale both by e^-ft
+                    const float ft = (float)(__longlong_as_double(((long long)meta.w << 32) | meta.z) +
+                                             tabG(tb, meta.y - m));
+                    const float e = expf(-fminf(fabsf(ft), 104.f));
+                    const bool big = ft > 0.f;
+                    const float xs = big ? e : 1.f;
+                    const float F = big ? 1.f : (ft > -104.f ? e : 0.f);
+                    xb = qj.x * xs;
+                    yb = fmaf(qj.y, xs, F);
                 }
             }
             const float4* RA = reinterpret_cast<const float4*>(recA + (size_t)u * LM);
@@ -695,14 +703,13 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
                 if (pick == LM) pick = last_nz;
             }
             const float inv = rcp_approx(tot);
-            if (valid) {
-                if (w_dos) dos[m] = (q0 + q1) * inv;
-                if (w_hap) {
-                    h0[m] = (uint8_t)((mk_c.a0 >> pick) & 1u);
-                    h1[m] = (uint8_t)((mk_c.a1 >> pick) & 1u);
-                }
-                if (w_hp) hp[m] = make_float2(q0 * inv, q1 * inv);
+            // lanes past the run recomputed its last marker: they store the same bytes there
+            if (w_dos) dos[m] = (q0 + q1) * inv;
+            if (w_hap) {
+                h0[m] = (uint8_t)((mk_c.a0 >> pick) & 1u);
+                h1[m] = (uint8_t)((mk_c.a1 >> pick) & 1u);
             }
+            if (w_hp) hp[m] = make_float2(q0 * inv, q1 * inv);
         }
         r = r2 + 1;
     }
