@@ -495,6 +495,134 @@ __device__ __forceinline__ float rcp_approx(float x) {
 template <int LM>
 __host__ __device__ constexpr uint32_t post_record_bytes() { return 2u * LM * 4u + 16u; }
 
+// Markers [c0, c1) of one sample, covered by consecutive windows whose
+// records start at slot cu + 1 of this warp's record arrays; lane = marker.
+// kFast: dosage and haplotypes are written, argmax picks, no P(hap=1).
+template <int LM, bool kFull, bool kFast>
+__device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v, uint32_t c0, uint32_t c1, uint32_t cu,
+                                              const float* recA, const float* recW, const uint4* recM,
+                                              const float4* lut, uint32_t lane) {
+    const uint32_t le_mask = 0xffffffffu >> (31 - lane);
+    const uint32_t lj = lane & 7;
+    const float keep = 1.0f - A.tie_eps;
+    const bool w_dos = A.dosage != nullptr, w_hap = A.haps != nullptr, w_hp = A.hprob != nullptr;
+    const bool argmax = A.sampling == SI_SAMPLE_ARGMAX;
+    const Tabs& tb = v.r.tabs;
+    const uint32_t lmask = lmask_of(v.r.L);
+    float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
+#pragma unroll
+    for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
+    const uint8_t* gp = v.geno;
+    const SlotMasks* mp = v.r.masks;
+    float* dos = (kFast || w_dos) ? A.dosage + v.out : nullptr;
+    uint8_t* h0 = (kFast || w_hap) ? A.haps + 2 * v.out : nullptr;
+    uint8_t* h1 = (kFast || w_hap) ? h0 + v.len : nullptr;
+    float2* hp = (!kFast && w_hp) ? reinterpret_cast<float2*>(A.hprob) + v.out : nullptr;
+    // codes and slot masks of the step, loaded one step ahead
+    const uint32_t mq = min(c0 + lane, c1 - 1);
+    uint8_t code = gp[mq];
+    SlotMasks mk = mp[mq];
+    for (uint32_t cb = c0; cb < c1; cb += 32) {
+        const uint32_t m_raw = cb + lane;
+        const bool valid = m_raw < c1;
+        const uint32_t m = valid ? m_raw : c1 - 1;  // lanes past the run repeat its last marker
+        const uint8_t code_c = code;
+        const SlotMasks mk_c = mk;
+        {
+            const uint32_t mn = min(m_raw + 32, c1 - 1);
+            code = gp[mn];
+            mk = mp[mn];
+        }
+        const bool is_anchor = valid && (m == 0 || code_c < 3);
+        const uint32_t bal = __ballot_sync(0xffffffffu, is_anchor);
+        const uint32_t u = cu + __popc(bal & le_mask);
+        cu += __popc(bal);
+        const uint4 meta = recM[u];
+        float2 qi, qj;
+        if (__all_sync(0xffffffffu, meta.y - meta.x < tb.NT)) {  // every run of the step is in the table
+            qi = __ldg(tb.QS + (m - meta.x));
+            qj = __ldg(tb.QS + (meta.y - m));
+        } else {
+            qi = tabQS(tb, m - meta.x);
+            qj = tabQS(tb, meta.y - m);
+        }
+        const bool uni = meta.w == kInfHi;                  // beta uniform
+        const bool fin = (meta.w & kInfHi) != kInfHi;       // finite farg': floor term per marker
+        float xb = uni ? 0.f : qj.x, yb = uni ? 1.f : qj.y;
+        if (__any_sync(0xffffffffu, fin)) {
+            if (fin) {
+                // floor e^ft beside Q w' + S; when it dominates (ft > 0) scale both by e^-ft
+                const float ft = (float)(__longlong_as_double(((long long)meta.w << 32) | meta.z) +
+                                         tabG(tb, meta.y - m));
+                const float e = expf(-fminf(fabsf(ft), 104.f));
+                const bool big = ft > 0.f;
+                const float xs = big ? e : 1.f;
+                const float F = big ? 1.f : (ft > -104.f ? e : 0.f);
+                xb = qj.x * xs;
+                yb = fmaf(qj.y, xs, F);
+            }
+        }
+        const float4* RA = reinterpret_cast<const float4*>(recA + (size_t)u * LM);
+        const float4* RW = reinterpret_cast<const float4*>(recW + (size_t)u * LM);
+        const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
+        const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
+        float pr[LM];
+        float2 tot2 = make_float2(0.f, 0.f), q02 = tot2, q12 = tot2;
+#pragma unroll
+        for (int q4 = 0; q4 < LM / 4; ++q4) {
+            const float4 av = RA[q4], wv = RW[q4];
+            float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.x, av.y), YF),
+                                    __ffma2_rn(XB, make_float2(wv.x, wv.y), YB));
+            float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.z, av.w), YF),
+                                    __ffma2_rn(XB, make_float2(wv.z, wv.w), YB));
+            if (!kFull) {
+                p01 = __fmul2_rn(p01, make_float2(act[4 * q4], act[4 * q4 + 1]));
+                p23 = __fmul2_rn(p23, make_float2(act[4 * q4 + 2], act[4 * q4 + 3]));
+            }
+            pr[4 * q4] = p01.x; pr[4 * q4 + 1] = p01.y; pr[4 * q4 + 2] = p23.x; pr[4 * q4 + 3] = p23.y;
+            tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
+            const float4 m0 = lut[((mk_c.a0 >> (4 * q4)) & 15u) * 8 + lj];
+            const float4 m1 = lut[((mk_c.a1 >> (4 * q4)) & 15u) * 8 + lj];
+            q02 = __ffma2_rn(p01, make_float2(m0.x, m0.y), q02);
+            q02 = __ffma2_rn(p23, make_float2(m0.z, m0.w), q02);
+            q12 = __ffma2_rn(p01, make_float2(m1.x, m1.y), q12);
+            q12 = __ffma2_rn(p23, make_float2(m1.z, m1.w), q12);
+        }
+        const float tot = tot2.x + tot2.y, q0 = q02.x + q02.y, q1 = q12.x + q12.y;
+        uint32_t pick;
+        if (kFast || argmax) {
+            float pmax = pr[0];
+#pragma unroll
+            for (int l = 1; l < LM; ++l) pmax = fmaxf(pmax, pr[l]);
+            const float thr = pmax * keep;
+            pick = 0;
+#pragma unroll
+            for (int l = LM - 1; l >= 1; --l) pick = (pr[l] >= thr) ? (uint32_t)l : pick;
+            if (pr[0] >= thr) pick = 0;
+        } else {
+            const float target = cell_uniform(A.seed, v.sid, v.m0 + m) * tot;
+            float cum = 0.f;
+            uint32_t last_nz = 0;
+            pick = LM;
+#pragma unroll
+            for (int l = 0; l < LM; ++l) {
+                cum += pr[l];
+                if (pr[l] > 0.f) last_nz = (uint32_t)l;
+                if (pick == LM && target < cum) pick = (uint32_t)l;
+            }
+            if (pick == LM) pick = last_nz;
+        }
+        const float inv = rcp_approx(tot);
+        // lanes past the run recomputed its last marker: they store the same bytes there
+        if (kFast || w_dos) dos[m] = (q0 + q1) * inv;
+        if (kFast || w_hap) {
+            h0[m] = (uint8_t)((mk_c.a0 >> pick) & 1u);
+            h1[m] = (uint8_t)((mk_c.a1 >> pick) & 1u);
+        }
+        if (!kFast && w_hp) hp[m] = make_float2(q0 * inv, q1 * inv);
+    }
+}
+
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
 template <int LM, bool kFull>
 __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kernel(TypedArgs A) {
@@ -584,11 +712,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
 
     // ---- phase 2
     const uint32_t live_mask = __ballot_sync(0xffffffffu, live);
-    const uint32_t le_mask = 0xffffffffu >> (31 - lane);
-    const uint32_t lj = lane & 7;
-    const float keep = 1.0f - A.tie_eps;
-    const bool w_dos = A.dosage != nullptr, w_hap = A.haps != nullptr, w_hp = A.hprob != nullptr;
-    const bool argmax = A.sampling == SI_SAMPLE_ARGMAX;
+    const bool fast = A.dosage && A.haps && !A.hprob && A.sampling == SI_SAMPLE_ARGMAX;
     uint32_t r = 0;
     while (r < 32 && ((live_mask >> r) & 1u)) {
         const uint32_t sr = __shfl_sync(0xffffffffu, s, r);
@@ -596,121 +720,9 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
         const uint32_t r2 = 31 - __clz(same);  // windows of a sample are consecutive
         const uint32_t c0 = __shfl_sync(0xffffffffu, cstart, r), c1 = __shfl_sync(0xffffffffu, cend, r2);
         const View v = view_of(A, sr);
-        const Tabs& tb = v.r.tabs;
-        const uint32_t lmask = lmask_of(v.r.L);
-        float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
-#pragma unroll
-        for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
-        const uint8_t* gp = v.geno;
-        const SlotMasks* mp = v.r.masks;
-        float* dos = w_dos ? A.dosage + v.out : nullptr;
-        uint8_t* h0 = w_hap ? A.haps + 2 * v.out : nullptr;
-        uint8_t* h1 = w_hap ? h0 + v.len : nullptr;
-        float2* hp = w_hp ? reinterpret_cast<float2*>(A.hprob) + v.out : nullptr;
-        uint32_t cu = r * C - 1u;  // record of the marker before the step (wraps for r = 0)
-        // codes and slot masks of the step, loaded one step ahead
-        const uint32_t mq = min(c0 + lane, c1 - 1);
-        uint8_t code = gp[mq];
-        SlotMasks mk = mp[mq];
-        for (uint32_t cb = c0; cb < c1; cb += 32) {
-            const uint32_t m_raw = cb + lane;
-            const bool valid = m_raw < c1;
-            const uint32_t m = valid ? m_raw : c1 - 1;  // lanes past the run repeat its last marker
-            const uint8_t code_c = code;
-            const SlotMasks mk_c = mk;
-            {
-                const uint32_t mn = min(m_raw + 32, c1 - 1);
-                code = gp[mn];
-                mk = mp[mn];
-            }
-            const bool is_anchor = valid && (m == 0 || code_c < 3);
-            const uint32_t bal = __ballot_sync(0xffffffffu, is_anchor);
-            const uint32_t u = cu + __popc(bal & le_mask);
-            cu += __popc(bal);
-            const uint4 meta = recM[u];
-            float2 qi, qj;
-            if (__all_sync(0xffffffffu, meta.y - meta.x < tb.NT)) {  // every run of the step is in the table
-                qi = __ldg(tb.QS + (m - meta.x));
-                qj = __ldg(tb.QS + (meta.y - m));
-            } else {
-                qi = tabQS(tb, m - meta.x);
-                qj = tabQS(tb, meta.y - m);
-            }
-            const bool uni = meta.w == kInfHi;                  // beta uniform
-            const bool fin = (meta.w & kInfHi) != kInfHi;       // finite farg': floor term per marker
-            float xb = uni ? 0.f : qj.x, yb = uni ? 1.f : qj.y;
-            if (__any_sync(0xffffffffu, fin)) {
-                if (fin) {
-                    // floor e^ft beside Q w' + S; when it dominates (ft > 0) scale both by e^-ft
-                    const float ft = (float)(__longlong_as_double(((long long)meta.w << 32) | meta.z) +
-                                             tabG(tb, meta.y - m));
-                    const float e = expf(-fminf(fabsf(ft), 104.f));
-                    const bool big = ft > 0.f;
-                    const float xs = big ? e : 1.f;
-                    const float F = big ? 1.f : (ft > -104.f ? e : 0.f);
-                    xb = qj.x * xs;
-                    yb = fmaf(qj.y, xs, F);
-                }
-            }
-            const float4* RA = reinterpret_cast<const float4*>(recA + (size_t)u * LM);
-            const float4* RW = reinterpret_cast<const float4*>(recW + (size_t)u * LM);
-            const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
-            const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
-            float pr[LM];
-            float2 tot2 = make_float2(0.f, 0.f), q02 = tot2, q12 = tot2;
-#pragma unroll
-            for (int q4 = 0; q4 < LM / 4; ++q4) {
-                const float4 av = RA[q4], wv = RW[q4];
-                float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.x, av.y), YF),
-                                        __ffma2_rn(XB, make_float2(wv.x, wv.y), YB));
-                float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.z, av.w), YF),
-                                        __ffma2_rn(XB, make_float2(wv.z, wv.w), YB));
-                if (!kFull) {
-                    p01 = __fmul2_rn(p01, make_float2(act[4 * q4], act[4 * q4 + 1]));
-                    p23 = __fmul2_rn(p23, make_float2(act[4 * q4 + 2], act[4 * q4 + 3]));
-                }
-                pr[4 * q4] = p01.x; pr[4 * q4 + 1] = p01.y; pr[4 * q4 + 2] = p23.x; pr[4 * q4 + 3] = p23.y;
-                tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
-                const float4 m0 = lut[((mk_c.a0 >> (4 * q4)) & 15u) * 8 + lj];
-                const float4 m1 = lut[((mk_c.a1 >> (4 * q4)) & 15u) * 8 + lj];
-                q02 = __ffma2_rn(p01, make_float2(m0.x, m0.y), q02);
-                q02 = __ffma2_rn(p23, make_float2(m0.z, m0.w), q02);
-                q12 = __ffma2_rn(p01, make_float2(m1.x, m1.y), q12);
-                q12 = __ffma2_rn(p23, make_float2(m1.z, m1.w), q12);
-            }
-            const float tot = tot2.x + tot2.y, q0 = q02.x + q02.y, q1 = q12.x + q12.y;
-            uint32_t pick;
-            if (argmax) {
-                float pmax = pr[0];
-#pragma unroll
-                for (int l = 1; l < LM; ++l) pmax = fmaxf(pmax, pr[l]);
-                const float thr = pmax * keep;
-                pick = 0;
-#pragma unroll
-                for (int l = LM - 1; l >= 1; --l) pick = (pr[l] >= thr) ? (uint32_t)l : pick;
-                if (pr[0] >= thr) pick = 0;
-            } else {
-                const float target = cell_uniform(A.seed, v.sid, v.m0 + m) * tot;
-                float cum = 0.f;
-                uint32_t last_nz = 0;
-                pick = LM;
-#pragma unroll
-                for (int l = 0; l < LM; ++l) {
-                    cum += pr[l];
-                    if (pr[l] > 0.f) last_nz = (uint32_t)l;
-                    if (pick == LM && target < cum) pick = (uint32_t)l;
-                }
-                if (pick == LM) pick = last_nz;
-            }
-            const float inv = rcp_approx(tot);
-            // lanes past the run recomputed its last marker: they store the same bytes there
-            if (w_dos) dos[m] = (q0 + q1) * inv;
-            if (w_hap) {
-                h0[m] = (uint8_t)((mk_c.a0 >> pick) & 1u);
-                h1[m] = (uint8_t)((mk_c.a1 >> pick) & 1u);
-            }
-            if (w_hp) hp[m] = make_float2(q0 * inv, q1 * inv);
-        }
+        const uint32_t cu = r * C - 1u;  // record of the marker before c0 (wraps for r = 0)
+        if (fast) posterior_run<LM, kFull, true>(A, v, c0, c1, cu, recA, recW, recM, lut, lane);
+        else posterior_run<LM, kFull, false>(A, v, c0, c1, cu, recA, recW, recM, lut, lane);
         r = r2 + 1;
     }
 }
