@@ -1,0 +1,144 @@
+"""The large-panel workload at full size: 100,000 haplotypes x 100,000
+markers (bit-packed, 1.25 GB), 500 founders, switch rate 0.001; 50,000 targets
+typed at every 20th marker (5 %), L = 16, uniform 0.5 cM map.
+
+The panel and targets are generated on the device with torch (a host-side
+byte panel would take 10 GB and minutes to draw); the generator follows the
+same recipe as swiftimpute_b200.synth (founder mosaic with allele flips;
+targets a mosaic of 8 panel haplotypes with switch rate 0.005), without the
+heterozygosity resampling. Checks:
+  * the PBWT sweep equals the oracle's streaming sweep row by row (64-bit
+    hash of every prefix row, all 100,000 rows);
+  * every output of all 50,000 targets is finite and in range;
+  * dosage and argmax haplotypes of a seeded subset of 512 targets equal the
+    FP64 oracle (1e-4; argmax up to threshold flips). The oracle reads the
+    device's slot table through a compact panel of the 32 selected haplotype
+    columns per marker, which gives it the same emissions as the full panel.
+"""
+import numpy as np
+import pytest
+
+import oracle
+from swiftimpute_b200 import _native as N
+
+pytestmark = pytest.mark.gpu
+
+M = NH = 100_000
+B = 50_000
+L = 16
+NE = 10_000
+EVERY = 20
+
+
+def _panel(dev, seed=3, founders=500, switch=0.001, flip=0.005, chunk=2048):
+    import torch
+    rng = np.random.default_rng(seed)
+    p = rng.beta(0.5, 0.5, size=M)
+    fnd = torch.from_numpy((rng.random((founders, M)) < p[None, :]).astype(np.uint8)).to(dev)
+    g = torch.Generator(device=dev).manual_seed(seed)
+    panel = torch.empty((M, NH), dtype=torch.uint8, device=dev)
+    carry = torch.randint(0, founders, (NH,), generator=g, device=dev)
+    for m0 in range(0, M, chunk):
+        c = min(M, m0 + chunk) - m0
+        ar = torch.arange(c, device=dev)[:, None]
+        sw = torch.rand((c, NH), generator=g, device=dev) < switch
+        new = torch.randint(0, founders, (c, NH), generator=g, device=dev)
+        last = torch.cummax(torch.where(sw, ar, torch.full_like(ar, -1)).expand(c, NH), dim=0).values
+        idx = torch.where(last >= 0, torch.gather(new, 0, last.clamp(min=0)), carry[None, :])
+        carry = idx[-1].clone()
+        alle = fnd[idx, (m0 + ar).expand(c, NH)]
+        alle ^= (torch.rand((c, NH), generator=g, device=dev) < flip).to(torch.uint8)
+        panel[m0:m0 + c] = alle
+    return panel
+
+
+def _pack(panel, chunk=1024):
+    import torch
+    W = NH // 32
+    shifts = torch.arange(32, device=panel.device, dtype=torch.int64)
+    out = np.empty((M, W), dtype=np.uint32)
+    for m0 in range(0, M, chunk):
+        rows = panel[m0:m0 + chunk].view(-1, W, 32).to(torch.int64)
+        words = (rows << shifts).sum(-1)  # distinct bits: the sum is the 32-bit word
+        out[m0:m0 + chunk] = words.cpu().numpy().astype(np.uint32)
+    return out
+
+
+def _targets(panel, seed=3, n_mosaic=8, switch=0.005, chunk=1024):
+    """codes [B][M] u8 on the device: h0 + h1 at typed markers, 3 elsewhere."""
+    import torch
+    dev = panel.device
+    g = torch.Generator(device=dev).manual_seed(seed + 1000)
+    H = 2 * B
+    src = torch.randint(0, NH, (H, n_mosaic), generator=g, device=dev)
+    codes = torch.full((B, M), 3, dtype=torch.uint8, device=dev)
+    carry = torch.randint(0, n_mosaic, (H,), generator=g, device=dev)
+    for m0 in range(0, M, chunk):
+        c = min(M, m0 + chunk) - m0
+        ar = torch.arange(c, device=dev)[:, None]
+        sw = torch.rand((c, H), generator=g, device=dev) < switch
+        new = torch.randint(0, n_mosaic, (c, H), generator=g, device=dev)
+        last = torch.cummax(torch.where(sw, ar, torch.full_like(ar, -1)).expand(c, H), dim=0).values
+        k = torch.where(last >= 0, torch.gather(new, 0, last.clamp(min=0)), carry[None, :])
+        carry = k[-1].clone()
+        hap = torch.gather(src.t(), 0, k)                   # [c][H] panel haplotype per marker
+        alle = torch.gather(panel[m0:m0 + c], 1, hap)       # [c][H]
+        geno = alle[:, 0::2] + alle[:, 1::2]                # [c][B]
+        typed = ((m0 + ar) % EVERY == 0).expand(c, B)
+        codes[:, m0:m0 + c] = torch.where(typed, geno, torch.full_like(geno, 3)).t()
+    return codes
+
+
+@pytest.fixture(scope="module")
+def large(engine):
+    import torch
+    dev = torch.device("cuda", 0)
+    panel = _panel(dev)
+    words = _pack(panel)
+    pos = (1 + np.arange(M, dtype=np.uint64) * np.uint64(500_000)).astype(np.uint64)
+    engine.upload_packed(words, NH)
+    engine.set_map(pos)
+    engine.pbwt_build(row_hashes=True)
+    codes = _targets(panel)
+    yield panel, words, pos, codes
+    del panel, codes
+    torch.cuda.empty_cache()
+
+
+def test_pbwt_rows_equal_oracle_streaming_sweep(engine, large):
+    _, words, _, _ = large
+    _, want = oracle.pbwt_build_packed(words, NH, keep_prefix=False)
+    assert np.array_equal(engine.row_hashes(), want)
+
+
+def test_all_targets_and_oracle_subset(engine, large):
+    import torch
+    panel, _, pos, codes = large
+    dev = codes.device
+    params = N.default_params(num_states=L, ne=NE)
+    dos = torch.empty((B, M), dtype=torch.float32, device=dev)
+    haps = torch.empty((B, 2, M), dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+    engine.impute_device(codes.data_ptr(), B, params, dos.data_ptr(), None, haps.data_ptr())
+    torch.cuda.synchronize(dev)
+    assert bool(torch.isfinite(dos).all()) and float(dos.min()) >= -1e-6 and float(dos.max()) <= 2 + 1e-5
+    assert int(haps.max()) <= 1
+    # seeded subset against the oracle, through a compact panel of the selected columns
+    sub = np.sort(np.random.default_rng(3).choice(B, 512, replace=False))
+    pairs = engine.select_states(L)                                        # [M][L][2]
+    cols = torch.from_numpy(pairs.reshape(M, 2 * L).astype(np.int64)).to(dev)
+    compact = torch.gather(panel, 1, cols).cpu().numpy()                   # [M][2L] alleles of the slot pairs
+    cpairs = np.broadcast_to(np.arange(2 * L, dtype=np.uint32).reshape(1, L, 2), (M, L, 2)).copy()
+    idx = torch.from_numpy(sub).to(dev)
+    c_sub = codes.index_select(0, idx).cpu().numpy()
+    got_d = dos.index_select(0, idx).cpu().numpy()
+    got_h = haps.index_select(0, idx).cpu().numpy()
+    want = oracle.fb_batch(c_sub, cpairs, compact, pos, L, float(NE))
+    assert np.abs(got_d - want["dosage"]).max() <= 1e-4
+    diff = (got_h != want["haps_argmax"]).any(axis=1)
+    if diff.any():
+        rows = np.nonzero(diff.any(axis=1))[0]
+        lo = oracle.fb_batch(c_sub[rows], cpairs, compact, pos, L, float(NE), tie_eps=1e-4 - 1e-5)
+        hi = oracle.fb_batch(c_sub[rows], cpairs, compact, pos, L, float(NE), tie_eps=1e-4 + 1e-5)
+        flip = ((lo["haps_argmax"] != want["haps_argmax"][rows]) | (hi["haps_argmax"] != want["haps_argmax"][rows])).any(axis=1)
+        assert not (diff[rows] & ~flip).any()
