@@ -139,9 +139,10 @@ def profile_traffic(kernel: str, config: str):
     return None
 
 
-def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds):
+def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds, gpu_dosage=None, gpu_haps=None):
     """The FP64 port of the reference recurrences on all host threads, on the
-    first S samples of the workload (S sized to ~`seconds` of CPU work)."""
+    first S samples of the workload (S sized to ~`seconds` of CPU work). With
+    the device outputs of the same samples, also the parity of that sample."""
     import oracle
     threads = os.cpu_count() or 1
     M = codes.shape[1]
@@ -151,12 +152,20 @@ def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds):
     dt = time.perf_counter() - t0
     S = int(min(codes.shape[0], max(s, round(s * seconds / max(dt, 1e-3)))))
     t0 = time.perf_counter()
-    oracle.fb_batch(codes[:S], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
+    want = oracle.fb_batch(codes[:S], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
     dt = time.perf_counter() - t0
     imputed = S * (M - len(typed))
-    return {"value": imputed / dt, "unit": "imputed genotypes/s", "cores": threads, "kind": "port",
-            "sample": f"first {S} of {codes.shape[0]} targets x {M} markers, FP64 log-space restatement of the "
-                      f"reference recurrences, {dt:.1f} s"}
+    out = {"value": imputed / dt, "unit": "imputed genotypes/s", "cores": threads, "kind": "port",
+           "sample": f"first {S} of {codes.shape[0]} targets x {M} markers, FP64 log-space restatement of the "
+                     f"reference recurrences, {dt:.1f} s"}
+    parity = None
+    if gpu_dosage is not None:
+        d = np.abs(gpu_dosage[:S] - want["dosage"])
+        parity = {"targets": S, "max_abs_dosage_diff_vs_fp64_oracle": float(d.max()),
+                  "mean_abs_dosage_diff": float(d.mean()),
+                  "argmax_haplotype_cells_differing": int((gpu_haps[:S] != want["haps_argmax"]).sum()),
+                  "cells": int(S * M)}
+    return out, parity
 
 
 def run_reference(args, cfg):
@@ -425,7 +434,8 @@ def run_ours(args, cfg):
     if not args.no_cpu_baseline and world == 1:
         import oracle
         pairs = eng.select_states(cfg["L"])
-        line["cpu_baseline"] = cpu_baseline(panel, pos, codes, pairs, typed, cfg, args.cpu_seconds)
+        line["cpu_baseline"], line["parity"] = cpu_baseline(panel, pos, codes, pairs, typed, cfg, args.cpu_seconds,
+                                                            gpu_dosage=dos, gpu_haps=d_haps.cpu().numpy())
     eng.close()
     print(json.dumps(line), flush=True)
     if dist:

@@ -244,6 +244,37 @@ si_status si_last_timings(si_ctx* ctx, float* ms3);
  * [3] posterior pass (or the whole full-chain kernel). Waits for the call. */
 si_status si_last_kernel_ms(si_ctx* ctx, float* ms4);
 
+/* ---- Plans: a fixed uneven batch launched with no host work in between.
+ *
+ * No counterpart in the reference, which sizes and launches each batch from
+ * the host (imputer.cpp:787-1042). si_impute_jobs_device reads the number of
+ * typed markers back from the device before it sizes its lists; a plan fixes
+ * each job's anchor capacity up front (max_anchors = 0: the job's marker
+ * count; else min(marker count, max_anchors), which must cover marker 0 plus
+ * the typed markers, e.g. the typed sites of a genotyping array + 1), owns its
+ * scratch, and holds the device pointers given here. si_plan_launch queues
+ * four kernels with fixed arguments and no host synchronisation, so it can be
+ * captured into a CUDA graph; si_plan_graph_launch captures it once and
+ * replays the graph. Rewrite the codes in d_geno between launches. A plan
+ * reads the ctx's panel, index and selection tables: it stays valid while they
+ * are unchanged and no server runs on the ctx.
+ * SI_PLAN_AUTOTUNE (with params checkpoint_interval and block_threads 0)
+ * times the launch on this batch for each window size (anchors per
+ * checkpoint) and posterior CTA size and keeps the fastest. */
+typedef struct si_plan si_plan;
+enum { SI_PLAN_AUTOTUNE = 1u };
+si_status si_plan_create(si_ctx* ctx, const si_impute_params* params, const si_region* regions, uint32_t n_regions,
+                         const si_job* jobs, uint32_t n_jobs, uint32_t max_anchors, const uint8_t* d_geno,
+                         float* d_dosage, float* d_hap_prob, uint8_t* d_haps, uint32_t flags, si_plan** out);
+si_status si_plan_launch(si_plan* plan, void* stream);
+si_status si_plan_graph_launch(si_plan* plan, void* stream);
+/* Wait for the device; SI_ERR_BUDGET if a job since the last check had more
+ * anchors than its capacity (it was cut to it; nothing outside the plan's
+ * buffers was touched). */
+si_status si_plan_check(si_plan* plan);
+si_status si_plan_info(const si_plan* plan, uint32_t* window, uint32_t* threads, float* tuned_ms);
+si_status si_plan_destroy(si_plan* plan);
+
 /* ---- Serving: requests of any size over a resident panel and index.
  *
  * The reference imputes one target set per Imputer::impute call

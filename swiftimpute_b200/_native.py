@@ -58,6 +58,7 @@ class ImputeParams(ctypes.Structure):
 
 
 INDEX_GLOBAL, INDEX_REGION = 0, 1
+PLAN_AUTOTUNE = 1
 
 
 class Region(ctypes.Structure):
@@ -119,6 +120,14 @@ SIGNATURES = [
      [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p, c_void_p]),
     ("si_last_timings", c_int, [c_void_p, POINTER(c_float)]),
     ("si_last_kernel_ms", c_int, [c_void_p, POINTER(c_float)]),
+    ("si_plan_create", c_int,
+     [c_void_p, POINTER(ImputeParams), POINTER(Region), c_uint32, POINTER(Job), c_uint32, c_uint32, c_void_p,
+      c_void_p, c_void_p, c_void_p, c_uint32, POINTER(c_void_p)]),
+    ("si_plan_launch", c_int, [c_void_p, c_void_p]),
+    ("si_plan_graph_launch", c_int, [c_void_p, c_void_p]),
+    ("si_plan_check", c_int, [c_void_p]),
+    ("si_plan_info", c_int, [c_void_p, POINTER(c_uint32), POINTER(c_uint32), POINTER(c_float)]),
+    ("si_plan_destroy", c_int, [c_void_p]),
     ("si_serve_start", c_int, [c_void_p, POINTER(ImputeParams), POINTER(ServeConfig), POINTER(c_void_p)]),
     ("si_serve_submit", c_int, [c_void_p, POINTER(Request), POINTER(c_uint64)]),
     ("si_serve_poll", c_int, [c_void_p, c_uint64, POINTER(c_int), POINTER(c_int)]),

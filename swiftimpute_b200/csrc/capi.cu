@@ -363,6 +363,146 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
 
 }  // namespace
 
+namespace si {
+
+// Arguments of an uneven batch (si_impute_jobs_device, si_plan_create).
+si_status check_jobs_args(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
+                          const si_job* jobs, uint32_t n_jobs) {
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!p || !regions || !jobs || n_regions == 0 || n_jobs == 0)
+        return fail(ctx, SI_ERR_INVALID_ARG, "NULL argument or empty batch");
+    if (p->transition_mode != SI_TRANS_MATRIX0)
+        return fail(ctx, SI_ERR_UNSUPPORTED, "uneven batches use the first-gap transition (SI_TRANS_MATRIX0)");
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    if (!ctx->has_map) return fail(ctx, SI_ERR_STATE, "marker positions not set (si_panel_set_map)");
+    if (p->sampling != SI_SAMPLE_ARGMAX && p->sampling != SI_SAMPLE_PHILOX)
+        return fail(ctx, SI_ERR_INVALID_ARG, "bad sampling mode");
+    if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
+    if (p->checkpoint_interval > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "checkpoint_interval must be <= 32");
+    if (p->block_threads && (p->block_threads % 32 || p->block_threads > 128))
+        return fail(ctx, SI_ERR_UNSUPPORTED, "block_threads must be a multiple of 32, <= 128");
+    return SI_OK;
+}
+
+// Region tables of an uneven batch: region-local sweeps and selections not
+// cached yet (one launch for all), global-origin selections, run tables; and
+// the per-job descriptors.
+si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
+                       const si_job* jobs, uint32_t n_jobs, cudaStream_t s, std::vector<TypedRegion>& tr,
+                       std::vector<TypedSample>& ts, uint32_t& lmax, bool& all_full) {
+    const uint32_t N = ctx->N, W = ctx->W;
+    lmax = 4;
+    bool need_global = false;
+    for (uint32_t r = 0; r < n_regions; ++r) {
+        const si_region& g = regions[r];
+        if (g.m_begin >= g.m_end || g.m_end > ctx->M)
+            return fail(ctx, SI_ERR_INVALID_ARG, "region " + std::to_string(r) + " is empty or outside the panel");
+        if (g.num_states == 0 || g.num_states > 32)
+            return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) + ": num_states must be 1..32");
+        if (g.index_origin != SI_INDEX_GLOBAL && g.index_origin != SI_INDEX_REGION)
+            return fail(ctx, SI_ERR_INVALID_ARG, "bad index_origin");
+        lmax = std::max(lmax, fb_lmax(g.num_states));
+        need_global |= g.index_origin == SI_INDEX_GLOBAL;
+    }
+    all_full = true;
+    for (uint32_t r = 0; r < n_regions; ++r) all_full &= regions[r].num_states == lmax;
+    if (need_global) SI_TRY(ensure_trans(ctx, p));  // panel-wide first-gap transition (trans0)
+    tr.assign(n_regions, TypedRegion{});
+    // region-local sweeps that are not cached yet, all in one launch
+    std::vector<SweepJob> sweeps;
+    std::vector<uint32_t> sweep_region;
+    uint64_t head_rows = 0;
+    for (uint32_t r = 0; r < n_regions; ++r) {
+        const si_region& g = regions[r];
+        if (g.index_origin != SI_INDEX_REGION) continue;
+        const uint32_t L = g.num_states;
+        const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+        auto key = std::make_tuple(g.m_begin, g.m_end, L, kind);
+        if (ctx->region_sel.count(key)) continue;
+        bool dup = false;
+        for (uint32_t q : sweep_region)
+            if (regions[q].m_begin == g.m_begin && regions[q].m_end == g.m_end) dup = true;
+        if (dup) continue;
+        sweeps.push_back(SweepJob{g.m_begin, g.m_end - g.m_begin, head_rows * kHead});
+        sweep_region.push_back(r);
+        head_rows += g.m_end - g.m_begin;
+    }
+    if (!sweeps.empty()) {
+        DeviceBuffer head, perm, jb;
+        SI_TRY(dev_alloc(ctx, head, head_rows * kHead * 4));
+        si_status st = dev_alloc(ctx, perm, (size_t)sweeps.size() * 2 * N * 4);
+        if (st == SI_OK) st = dev_alloc(ctx, jb, sweeps.size() * sizeof(SweepJob));
+        cudaError_t e = cudaSuccess;
+        if (st == SI_OK) e = cudaMemsetAsync(head.ptr, 0, head_rows * kHead * 4, s);
+        if (st == SI_OK && e == cudaSuccess)
+            e = cudaMemcpyAsync(jb.ptr, sweeps.data(), sweeps.size() * sizeof(SweepJob), cudaMemcpyHostToDevice, s);
+        if (st == SI_OK && e == cudaSuccess)
+            e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, (const SweepJob*)jb.ptr, (uint32_t)sweeps.size(),
+                                  N, W, (uint32_t*)head.ptr, nullptr, nullptr, (uint32_t*)perm.ptr, s);
+        // selection tables of every region (and slot count) that uses these sweeps
+        for (uint32_t r = 0; st == SI_OK && e == cudaSuccess && r < n_regions; ++r) {
+            const si_region& g = regions[r];
+            if (g.index_origin != SI_INDEX_REGION) continue;
+            const uint32_t L = g.num_states;
+            const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+            auto key = std::make_tuple(g.m_begin, g.m_end, L, kind);
+            if (ctx->region_sel.count(key)) continue;
+            size_t j = 0;
+            while (j < sweeps.size() && !(sweeps[j].m0 == g.m_begin && sweeps[j].len == g.m_end - g.m_begin)) ++j;
+            if (j == sweeps.size()) continue;  // cached already under another slot count? swept above
+            auto& rs = ctx->region_sel[key];
+            st = dev_alloc(ctx, rs.masks, (size_t)(g.m_end - g.m_begin) * sizeof(SlotMasks));
+            if (st != SI_OK) { ctx->region_sel.erase(key); break; }
+            e = launch_select((const uint32_t*)head.ptr + sweeps[j].head_off,
+                              (const uint32_t*)ctx->panel.ptr + (size_t)g.m_begin * W, g.m_end - g.m_begin, N, W, L,
+                              kind, nullptr, (SlotMasks*)rs.masks.ptr, s);
+        }
+        if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);  // scratch reuse below
+        dev_free(ctx, head);
+        dev_free(ctx, perm);
+        dev_free(ctx, jb);
+        if (st != SI_OK) return st;
+        if (e != cudaSuccess) return cuda_fail(ctx, e, "region sweep");
+    }
+    for (uint32_t r = 0; r < n_regions; ++r) {
+        const si_region& g = regions[r];
+        const uint32_t L = g.num_states;
+        tr[r].L = L;
+        if (g.index_origin == SI_INDEX_GLOBAL) {
+            SelectionCache* sel = nullptr;
+            SI_TRY(ensure_selection(ctx, L, p->selection_kind, &sel, false, s));
+            tr[r].masks = (const SlotMasks*)sel->masks.ptr + g.m_begin;
+            SI_TRY(tables_for(ctx, ctx->trans0, L, &tr[r].tabs));
+        } else {
+            const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
+            tr[r].masks = (const SlotMasks*)ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)].masks.ptr;
+            const LinTrans t0 = (g.m_end - g.m_begin >= 2)
+                                    ? lin_trans(ctx->morgans[g.m_begin], ctx->morgans[g.m_begin + 1], (double)p->ne,
+                                                p->rho_rate)
+                                    : LinTrans{1.f, 0.f};
+            if (g.m_end - g.m_begin >= 2 && !(t0.c >= 1e-30f))
+                return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
+                                                         ": zero genetic distance in its first gap");
+            SI_TRY(tables_for(ctx, t0, L, &tr[r].tabs));
+        }
+    }
+    ts.assign(n_jobs, TypedSample{});
+    for (uint32_t j = 0; j < n_jobs; ++j) {
+        if (jobs[j].region >= n_regions) return fail(ctx, SI_ERR_INVALID_ARG, "job region out of range");
+        const si_region& g = regions[jobs[j].region];
+        ts[j].geno_off = jobs[j].geno_offset;
+        ts[j].out_off = jobs[j].out_offset;
+        ts[j].sample_id = jobs[j].sample_id;
+        ts[j].m0 = g.m_begin;
+        ts[j].len = g.m_end - g.m_begin;
+        ts[j].region = jobs[j].region;
+        ts[j].pad = 0;
+    }
+    return SI_OK;
+}
+
+}  // namespace si
+
 extern "C" {
 
 int si_abi_version(void) { return SI_ABI_VERSION; }
@@ -705,129 +845,16 @@ si_status si_impute_jobs_device(si_ctx* ctx, const si_impute_params* p, const si
                                 const si_job* jobs, uint32_t n_jobs, const uint8_t* d_geno, float* d_dosage,
                                 float* d_hap_prob, uint8_t* d_haps, void* stream) {
     if (!ctx) return SI_ERR_INVALID_ARG;
-    if (!p || !regions || !jobs || !d_geno || n_regions == 0 || n_jobs == 0)
-        return fail(ctx, SI_ERR_INVALID_ARG, "NULL argument or empty batch");
-    if (p->transition_mode != SI_TRANS_MATRIX0)
-        return fail(ctx, SI_ERR_UNSUPPORTED, "uneven batches use the first-gap transition (SI_TRANS_MATRIX0)");
-    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
-    if (!ctx->has_map) return fail(ctx, SI_ERR_STATE, "marker positions not set (si_panel_set_map)");
-    if (p->sampling != SI_SAMPLE_ARGMAX && p->sampling != SI_SAMPLE_PHILOX)
-        return fail(ctx, SI_ERR_INVALID_ARG, "bad sampling mode");
-    if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
-    if (p->checkpoint_interval > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "checkpoint_interval must be <= 32");
-    if (p->block_threads && (p->block_threads % 32 || p->block_threads > 128))
-        return fail(ctx, SI_ERR_UNSUPPORTED, "block_threads must be a multiple of 32, <= 128");
+    SI_TRY(check_jobs_args(ctx, p, regions, n_regions, jobs, n_jobs));
+    if (!d_geno) return fail(ctx, SI_ERR_INVALID_ARG, "NULL genotype buffer");
     SI_TRY(set_device(ctx));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     SI_CUDA(ctx, cudaEventRecord(ctx->kev[0], s), "event");
-    const uint32_t N = ctx->N, W = ctx->W;
+    std::vector<TypedRegion> tr;
+    std::vector<TypedSample> ts;
     uint32_t lmax = 4;
-    bool need_global = false;
-    for (uint32_t r = 0; r < n_regions; ++r) {
-        const si_region& g = regions[r];
-        if (g.m_begin >= g.m_end || g.m_end > ctx->M)
-            return fail(ctx, SI_ERR_INVALID_ARG, "region " + std::to_string(r) + " is empty or outside the panel");
-        if (g.num_states == 0 || g.num_states > 32)
-            return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) + ": num_states must be 1..32");
-        if (g.index_origin != SI_INDEX_GLOBAL && g.index_origin != SI_INDEX_REGION)
-            return fail(ctx, SI_ERR_INVALID_ARG, "bad index_origin");
-        lmax = std::max(lmax, fb_lmax(g.num_states));
-        need_global |= g.index_origin == SI_INDEX_GLOBAL;
-    }
     bool all_full = true;
-    for (uint32_t r = 0; r < n_regions; ++r) all_full &= regions[r].num_states == lmax;
-    if (need_global) SI_TRY(ensure_trans(ctx, p));  // panel-wide first-gap transition (trans0)
-    std::vector<TypedRegion> tr(n_regions);
-    // region-local sweeps that are not cached yet, all in one launch
-    std::vector<SweepJob> sweeps;
-    std::vector<uint32_t> sweep_region;
-    uint64_t head_rows = 0;
-    for (uint32_t r = 0; r < n_regions; ++r) {
-        const si_region& g = regions[r];
-        if (g.index_origin != SI_INDEX_REGION) continue;
-        const uint32_t L = g.num_states;
-        const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
-        auto key = std::make_tuple(g.m_begin, g.m_end, L, kind);
-        if (ctx->region_sel.count(key)) continue;
-        bool dup = false;
-        for (uint32_t q : sweep_region)
-            if (regions[q].m_begin == g.m_begin && regions[q].m_end == g.m_end) dup = true;
-        if (dup) continue;
-        sweeps.push_back(SweepJob{g.m_begin, g.m_end - g.m_begin, head_rows * kHead});
-        sweep_region.push_back(r);
-        head_rows += g.m_end - g.m_begin;
-    }
-    if (!sweeps.empty()) {
-        DeviceBuffer head, perm, jb;
-        SI_TRY(dev_alloc(ctx, head, head_rows * kHead * 4));
-        si_status st = dev_alloc(ctx, perm, (size_t)sweeps.size() * 2 * N * 4);
-        if (st == SI_OK) st = dev_alloc(ctx, jb, sweeps.size() * sizeof(SweepJob));
-        cudaError_t e = cudaSuccess;
-        if (st == SI_OK) e = cudaMemsetAsync(head.ptr, 0, head_rows * kHead * 4, s);
-        if (st == SI_OK && e == cudaSuccess)
-            e = cudaMemcpyAsync(jb.ptr, sweeps.data(), sweeps.size() * sizeof(SweepJob), cudaMemcpyHostToDevice, s);
-        if (st == SI_OK && e == cudaSuccess)
-            e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, (const SweepJob*)jb.ptr, (uint32_t)sweeps.size(),
-                                  N, W, (uint32_t*)head.ptr, nullptr, nullptr, (uint32_t*)perm.ptr, s);
-        // selection tables of every region (and slot count) that uses these sweeps
-        for (uint32_t r = 0; st == SI_OK && e == cudaSuccess && r < n_regions; ++r) {
-            const si_region& g = regions[r];
-            if (g.index_origin != SI_INDEX_REGION) continue;
-            const uint32_t L = g.num_states;
-            const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
-            auto key = std::make_tuple(g.m_begin, g.m_end, L, kind);
-            if (ctx->region_sel.count(key)) continue;
-            size_t j = 0;
-            while (j < sweeps.size() && !(sweeps[j].m0 == g.m_begin && sweeps[j].len == g.m_end - g.m_begin)) ++j;
-            if (j == sweeps.size()) continue;  // cached already under another slot count? swept above
-            auto& rs = ctx->region_sel[key];
-            st = dev_alloc(ctx, rs.masks, (size_t)(g.m_end - g.m_begin) * sizeof(SlotMasks));
-            if (st != SI_OK) { ctx->region_sel.erase(key); break; }
-            e = launch_select((const uint32_t*)head.ptr + sweeps[j].head_off,
-                              (const uint32_t*)ctx->panel.ptr + (size_t)g.m_begin * W, g.m_end - g.m_begin, N, W, L,
-                              kind, nullptr, (SlotMasks*)rs.masks.ptr, s);
-        }
-        if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);  // scratch reuse below
-        dev_free(ctx, head);
-        dev_free(ctx, perm);
-        dev_free(ctx, jb);
-        if (st != SI_OK) return st;
-        if (e != cudaSuccess) return cuda_fail(ctx, e, "region sweep");
-    }
-    for (uint32_t r = 0; r < n_regions; ++r) {
-        const si_region& g = regions[r];
-        const uint32_t L = g.num_states;
-        tr[r].L = L;
-        if (g.index_origin == SI_INDEX_GLOBAL) {
-            SelectionCache* sel = nullptr;
-            SI_TRY(ensure_selection(ctx, L, p->selection_kind, &sel, false, s));
-            tr[r].masks = (const SlotMasks*)sel->masks.ptr + g.m_begin;
-            SI_TRY(tables_for(ctx, ctx->trans0, L, &tr[r].tabs));
-        } else {
-            const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
-            tr[r].masks = (const SlotMasks*)ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)].masks.ptr;
-            const LinTrans t0 = (g.m_end - g.m_begin >= 2)
-                                    ? lin_trans(ctx->morgans[g.m_begin], ctx->morgans[g.m_begin + 1], (double)p->ne,
-                                                p->rho_rate)
-                                    : LinTrans{1.f, 0.f};
-            if (g.m_end - g.m_begin >= 2 && !(t0.c >= 1e-30f))
-                return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
-                                                         ": zero genetic distance in its first gap");
-            SI_TRY(tables_for(ctx, t0, L, &tr[r].tabs));
-        }
-    }
-    std::vector<TypedSample> ts(n_jobs);
-    for (uint32_t j = 0; j < n_jobs; ++j) {
-        if (jobs[j].region >= n_regions) return fail(ctx, SI_ERR_INVALID_ARG, "job region out of range");
-        const si_region& g = regions[jobs[j].region];
-        ts[j].geno_off = jobs[j].geno_offset;
-        ts[j].out_off = jobs[j].out_offset;
-        ts[j].sample_id = jobs[j].sample_id;
-        ts[j].m0 = g.m_begin;
-        ts[j].len = g.m_end - g.m_begin;
-        ts[j].region = jobs[j].region;
-        ts[j].pad = 0;
-    }
+    SI_TRY(prepare_jobs(ctx, p, regions, n_regions, jobs, n_jobs, s, tr, ts, lmax, all_full));
     SI_TRY(dev_reserve(ctx, ctx->job_regions, tr.size() * sizeof(TypedRegion)));
     SI_TRY(dev_reserve(ctx, ctx->job_samples, ts.size() * sizeof(TypedSample)));
     SI_CUDA(ctx, cudaMemcpyAsync(ctx->job_regions.ptr, tr.data(), tr.size() * sizeof(TypedRegion),

@@ -48,9 +48,11 @@ struct TypedArgs {
     TypedRegion reg0;                // the region of a plain batch
     const TypedRegion* regions;      // device array, uneven batches (else null)
     const TypedSample* samples;      // device array, uneven batches (else null)
-    unsigned long long* aoff;        // [B+1] anchor offsets
-    unsigned long long* woff;        // [B+1] window offsets
-    uint32_t* counts;                // [B]
+    unsigned long long* aoff;        // [B+1] anchor offsets (exact, or per-job capacities in a plan)
+    unsigned long long* woff;        // [B+1] window offsets (likewise)
+    uint32_t* counts;                // [B] anchors of each job (written by the count kernel)
+    int capacity;                    // offsets are capacities fixed in advance: clamp counts to them
+    uint32_t* err;                   // device flag: bit 0 set when a job had more anchors than its capacity
     uint32_t* apos;                  // anchor positions (within the slice)
     uint32_t* aem;                   // anchor emission masks over the slots
     uint8_t* ashift;                 // 1 where no slot matches the call (every slot scaled by e^-999)
@@ -65,10 +67,19 @@ struct TypedArgs {
     cudaEvent_t ev_chain_done;       // recorded between the chain and the posterior kernel (may be null)
 };
 
-cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s);
+cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s);  // count + offset scan
+cudaError_t launch_anchor_count_only(const TypedArgs& a, cudaStream_t s);   // count (capacity offsets)
 cudaError_t launch_anchor_lists_fill(const TypedArgs& a, cudaStream_t s);
 cudaError_t launch_typed_fb(const TypedArgs& a, uint32_t lmax, bool all_full, cudaStream_t s);
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C);
+// Uneven batches (capi.cu): argument checks, and the region tables and job
+// descriptors of a batch (region sweeps and selections not cached yet run on s).
+si_status check_jobs_args(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
+                          const si_job* jobs, uint32_t n_jobs);
+si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
+                       const si_job* jobs, uint32_t n_jobs, cudaStream_t s, std::vector<TypedRegion>& tr,
+                       std::vector<TypedSample>& ts, uint32_t& lmax, bool& all_full);
+
 uint32_t typed_default_window(uint32_t lmax);   // anchors per window when the caller gives none
 uint32_t typed_default_threads(uint32_t lmax);  // posterior CTA size when the caller gives none
 

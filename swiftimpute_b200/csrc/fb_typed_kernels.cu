@@ -125,7 +125,16 @@ __global__ void anchor_count_kernel(TypedArgs A) {
     }
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) n += __shfl_xor_sync(0xffffffffu, n, o);
-    if (lane == 0) A.counts[s] = n;
+    if (lane == 0) {
+        if (A.capacity) {
+            const uint32_t cap = (uint32_t)(A.aoff[s + 1] - A.aoff[s]);
+            if (n > cap) {
+                atomicOr(A.err, 1u);  // the job is cut to its capacity; the host reports it
+                n = cap;
+            }
+        }
+        A.counts[s] = n;
+    }
 }
 
 // Exclusive scans of anchor counts and window counts (ceil(count / C)) in one
@@ -180,6 +189,7 @@ __global__ void anchor_fill_kernel(TypedArgs A) {
     const uint32_t lmask = lmask_of(v.r.L);
     const bool vec = (reinterpret_cast<uintptr_t>(v.geno) & 15u) == 0;
     unsigned long long o = A.aoff[s];
+    const unsigned long long lim = o + A.counts[s];  // a plan's capacity cut, else every anchor
     for (uint32_t b0 = 0; b0 < v.len; b0 += 512) {
         const uint32_t base = b0 + lane * 16;
         uint32_t bits = base < v.len ? typed_bits16(v.geno, base, v.len, vec) : 0u;
@@ -196,10 +206,12 @@ __global__ void anchor_fill_kernel(TypedArgs A) {
             const uint32_t j = __ffs(bits) - 1;
             bits &= bits - 1;
             const uint32_t m = base + j;
-            uint32_t sh;
-            A.apos[at] = m;
-            A.aem[at] = emission_mask(v.geno[m], v.r.masks[m], lmask, &sh);
-            A.ashift[at] = (uint8_t)sh;
+            if (at < lim) {
+                uint32_t sh;
+                A.apos[at] = m;
+                A.aem[at] = emission_mask(v.geno[m], v.r.masks[m], lmask, &sh);
+                A.ashift[at] = (uint8_t)sh;
+            }
             ++at;
         }
         o += __shfl_sync(0xffffffffu, incl, 31);
@@ -312,7 +324,7 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
         v = view_of(A, s);
         base = A.aoff[s];
         wb = A.woff[s];
-        NA = (uint32_t)(A.aoff[s + 1] - base);
+        NA = A.counts[s];
     }
     const uint32_t NAw = __reduce_max_sync(0xffffffffu, NA);
     if (NAw == 0) return;  // whole warp
@@ -496,11 +508,11 @@ template <int LM>
 __host__ __device__ constexpr uint32_t post_record_bytes() { return 2u * LM * 4u + 16u; }
 
 // Markers [c0, c1) of one sample, covered by consecutive windows whose
-// records start at slot cu + 1 of this warp's record arrays; lane = marker.
+// records are slots cu + 1 .. umax of this warp's record arrays; lane = marker.
 // kFast: dosage and haplotypes are written, argmax picks, no P(hap=1).
 template <int LM, bool kFull, bool kFast>
 __device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v, uint32_t c0, uint32_t c1, uint32_t cu,
-                                              const float* recA, const float* recW, const uint4* recM,
+                                              uint32_t umax, const float* recA, const float* recW, const uint4* recM,
                                               const float4* lut, uint32_t lane) {
     const uint32_t le_mask = 0xffffffffu >> (31 - lane);
     const uint32_t lj = lane & 7;
@@ -535,7 +547,9 @@ __device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v,
         }
         const bool is_anchor = valid && (m == 0 || code_c < 3);
         const uint32_t bal = __ballot_sync(0xffffffffu, is_anchor);
-        const uint32_t u = cu + __popc(bal & le_mask);
+        // the codes' anchors are the list's, except in a job a plan cut to its
+        // capacity: stay on the run's records there
+        const uint32_t u = min(cu + __popc(bal & le_mask), umax);
         cu += __popc(bal);
         const uint4 meta = recM[u];
         float2 qi, qj;
@@ -644,19 +658,27 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
 
     // ---- phase 1
     const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + t;
-    const bool live = g < A.total_windows;
-    uint32_t s = 0xffffffffu, cstart = 0, cend = 0;
+    bool live = g < A.total_windows;
+    uint32_t s = 0xffffffffu, cstart = 0, cend = 0, nrec = 0;
     if (live) {
         s = A.wsample[g];
+        // a plan's capacity windows past the job's anchors hold nothing
+        if ((g - A.woff[s]) * C >= A.counts[s]) {
+            live = false;
+            s = 0xffffffffu;
+        }
+    }
+    if (live) {
         const View v = view_of(A, s);
         const Tabs& tb = v.r.tabs;
         const unsigned long long base = A.aoff[s], wb = A.woff[s], w = g - wb;
-        const unsigned long long NA = A.aoff[s + 1] - base;
+        const unsigned long long NA = A.counts[s];
         const uint32_t* pos = A.apos + base;
         const uint32_t* aem = A.aem + base;
         const uint8_t* ash = A.ashift + base;
         const unsigned long long k0 = w * C, k1 = min(k0 + C, NA);
         const uint32_t u0 = lane * C;  // this window's first record
+        nrec = (uint32_t)(k1 - k0);
         cstart = pos[k0];
         cend = k1 < NA ? pos[k1] : v.len;
         // backward: records k0 .. k1-1 take w' from anchor k+1
@@ -713,17 +735,19 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kerne
     // ---- phase 2
     const uint32_t live_mask = __ballot_sync(0xffffffffu, live);
     const bool fast = A.dosage && A.haps && !A.hprob && A.sampling == SI_SAMPLE_ARGMAX;
-    uint32_t r = 0;
-    while (r < 32 && ((live_mask >> r) & 1u)) {
+    uint32_t rest = live_mask;
+    while (rest) {
+        const uint32_t r = __ffs(rest) - 1;
         const uint32_t sr = __shfl_sync(0xffffffffu, s, r);
         const uint32_t same = __ballot_sync(0xffffffffu, live && s == sr);
         const uint32_t r2 = 31 - __clz(same);  // windows of a sample are consecutive
         const uint32_t c0 = __shfl_sync(0xffffffffu, cstart, r), c1 = __shfl_sync(0xffffffffu, cend, r2);
         const View v = view_of(A, sr);
         const uint32_t cu = r * C - 1u;  // record of the marker before c0 (wraps for r = 0)
-        if (fast) posterior_run<LM, kFull, true>(A, v, c0, c1, cu, recA, recW, recM, lut, lane);
-        else posterior_run<LM, kFull, false>(A, v, c0, c1, cu, recA, recW, recM, lut, lane);
-        r = r2 + 1;
+        const uint32_t umax = r2 * C + __shfl_sync(0xffffffffu, nrec, r2) - 1u;  // the run's last record
+        if (fast) posterior_run<LM, kFull, true>(A, v, c0, c1, cu, umax, recA, recW, recM, lut, lane);
+        else posterior_run<LM, kFull, false>(A, v, c0, c1, cu, umax, recA, recW, recM, lut, lane);
+        rest &= ~((2u << r2) - 1u);  // lanes up to r2 are done (r2 = 31 clears all)
     }
 }
 
@@ -736,9 +760,15 @@ template <int LM, bool kFull>
 cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
     const uint32_t T = a.threads;
     const size_t sm = post_smem<LM>(T, a.C);
-    cudaError_t e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull>,
-                                         cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
+    // set outside stream capture only (a plan launches once before it is captured)
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    cudaError_t e = cudaStreamIsCapturing(s, &cs);
     if (e != cudaSuccess) return e;
+    if (cs == cudaStreamCaptureStatusNone) {
+        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                                 (int)sm);
+        if (e != cudaSuccess) return e;
+    }
     const unsigned long long grid = (a.total_windows + T - 1) / T;
     if (grid == 0) return cudaSuccess;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
@@ -779,6 +809,11 @@ cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s) {
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     anchor_scan_kernel<<<1, 1024, 0, s>>>(a.counts, a.B, a.C, a.aoff, a.woff);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_anchor_count_only(const TypedArgs& a, cudaStream_t s) {
+    anchor_count_kernel<<<(a.B + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, s>>>(a);
     return cudaGetLastError();
 }
 

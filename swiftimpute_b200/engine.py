@@ -171,6 +171,11 @@ class Engine:
             out.append(o)
         return out
 
+    def plan(self, regions, jobs, params: N.ImputeParams | None = None, *, max_anchors: int = 0,
+             autotune: bool = False, hap_prob: bool = False) -> "Plan":
+        """A fixed uneven batch (si_plan_*): same arguments as ``impute_jobs``."""
+        return Plan(self, regions, jobs, params or N.default_params(), max_anchors, autotune, hap_prob)
+
     def last_kernel_ms(self) -> tuple[float, float, float, float]:
         """(selection, typed-marker lists, anchor chain, posterior or full-chain kernel) in ms."""
         ms = (c_float * 4)()
@@ -271,3 +276,70 @@ class Server:
 
     def __exit__(self, *exc):
         self.stop()
+
+
+class Plan:
+    """A fixed uneven batch whose launch needs no host work (CUDA-graph
+    capturable). Owns the device buffers of its codes and outputs (torch,
+    plumbing only); ``set_codes`` rewrites the codes in place between launches."""
+
+    def __init__(self, engine: Engine, regions, jobs, params, max_anchors, autotune, hap_prob):
+        import torch
+        self.engine, self.lib = engine, engine.lib
+        self.regions = list(regions)
+        self.lens = [regions[r][1] - regions[r][0] for r, _, _ in jobs]
+        self.offs = np.concatenate([[0], np.cumsum(self.lens)]).astype(np.int64)
+        total = max(1, int(self.offs[-1]))
+        dev = torch.device("cuda", 0)
+        self.d_geno = torch.zeros(total, dtype=torch.uint8, device=dev)
+        self.d_dos = torch.empty(total, dtype=torch.float32, device=dev)
+        self.d_haps = torch.empty(2 * total, dtype=torch.uint8, device=dev)
+        self.d_hp = torch.empty(2 * total, dtype=torch.float32, device=dev) if hap_prob else None
+        self.set_codes([c for _, c, _ in jobs])
+        R = (N.Region * len(regions))(*[N.Region(a, b, L, o) for a, b, L, o in regions])
+        J = (N.Job * len(jobs))(*[N.Job(r, 0, int(self.offs[i]), int(self.offs[i]), int(sid))
+                                  for i, (r, _, sid) in enumerate(jobs)])
+        h = c_void_p()
+        torch.cuda.synchronize(dev)
+        engine._check(self.lib.si_plan_create(
+            engine.h, byref(params), R, len(regions), J, len(jobs), max_anchors, c_void_p(self.d_geno.data_ptr()),
+            c_void_p(self.d_dos.data_ptr()), c_void_p(self.d_hp.data_ptr()) if hap_prob else None,
+            c_void_p(self.d_haps.data_ptr()), N.PLAN_AUTOTUNE if autotune else 0, byref(h)))
+        self.h = h
+
+    def set_codes(self, codes) -> None:
+        import torch
+        flat = np.concatenate([np.asarray(c, dtype=np.uint8) for c in codes])
+        self.d_geno[: flat.size].copy_(torch.from_numpy(flat))
+        torch.cuda.synchronize(self.d_geno.device)
+
+    def launch(self, graph: bool = False) -> None:
+        fn = self.lib.si_plan_graph_launch if graph else self.lib.si_plan_launch
+        self.engine._check(fn(self.h, None))
+
+    def check(self) -> None:
+        self.engine._check(self.lib.si_plan_check(self.h))
+
+    def info(self) -> dict:
+        c, t, ms = ctypes.c_uint32(), ctypes.c_uint32(), c_float()
+        self.engine._check(self.lib.si_plan_info(self.h, byref(c), byref(t), byref(ms)))
+        return {"window": c.value, "threads": t.value, "tuned_ms": ms.value}
+
+    def outputs(self):
+        """Per job: dosage [len], haps [2][len] (and hap_prob [len][2])."""
+        self.check()
+        dos, haps = self.d_dos.cpu().numpy(), self.d_haps.cpu().numpy()
+        hp = self.d_hp.cpu().numpy() if self.d_hp is not None else None
+        out = []
+        for i, n in enumerate(self.lens):
+            a = int(self.offs[i])
+            o = {"dosage": dos[a:a + n], "haps": haps[2 * a:2 * a + 2 * n].reshape(2, n)}
+            if hp is not None:
+                o["hap_prob"] = hp[2 * a:2 * a + 2 * n].reshape(n, 2)
+            out.append(o)
+        return out
+
+    def destroy(self) -> None:
+        if getattr(self, "h", None):
+            self.lib.si_plan_destroy(self.h)
+            self.h = None
