@@ -29,3 +29,16 @@ def engine():
 @pytest.fixture
 def rng():
     return np.random.default_rng(1234)
+
+
+def report(name: str, **values) -> None:
+    """Record measured parity figures of a test in $SI_REPORT_DIR/parity.json (when set)."""
+    import json
+    import os
+    d = os.environ.get("SI_REPORT_DIR")
+    if not d:
+        return
+    path = Path(d) / "parity.json"
+    data = json.loads(path.read_text()) if path.exists() else {}
+    data[name] = {k: (float(v) if isinstance(v, (np.floating, float)) else v) for k, v in values.items()}
+    path.write_text(json.dumps(data, indent=1, sort_keys=True))

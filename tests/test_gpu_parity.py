@@ -110,7 +110,10 @@ def compare(engine, panel, pos, codes, L, ne, per_gap=False, sampling=N.SAMPLE_A
 def test_fb_plain_small_shape(engine, spacing):
     # the plain-method config (4,432 haplotypes x 1,644 markers, every 5th typed, L=8, Ne=1e4), 96 targets
     panel, pos, codes, _ = workload(1644, 4432, 96, synth.typed_every(1644, 5), spacing, 0, founders=40)
-    compare(engine, panel, pos, codes, 8, 10000)
+    got, want = compare(engine, panel, pos, codes, 8, 10000)
+    from conftest import report
+    report(f"plain-small spacing {spacing}", targets=96, max_abs_dosage_diff=np.abs(got["dosage"] - want["dosage"]).max(),
+           argmax_cells_differing=int((got["haps"] != want["haps_argmax"]).sum()))
 
 
 @pytest.mark.parametrize("L", [1, 2, 3, 4, 5, 8, 13, 16, 24, 32])

@@ -70,6 +70,7 @@ def test_full_shape_jobs_alone_equal_mix(engine, workload):
 def test_full_shape_against_oracle_on_short_regions(workload):
     panel, pos, regions, jobs, out = workload
     short = sorted(range(64), key=lambda r: regions[r][1] - regions[r][0])[:3]
+    worst, checked = 0.0, 0
     for r in short:
         m0, m1, L, _ = regions[r]
         idx = [j for j, (rr, _, _) in enumerate(jobs) if rr == r][:4]
@@ -80,6 +81,8 @@ def test_full_shape_against_oracle_on_short_regions(workload):
         codes = np.stack([jobs[j][1] for j in idx])
         want = oracle.fb_batch(codes, pairs, sl, pos[m0:m1], L, 10000.0)
         for b, j in enumerate(idx):
+            worst = max(worst, float(np.abs(out[j]["dosage"] - want["dosage"][b]).max()))
+            checked += 1
             assert np.abs(out[j]["dosage"] - want["dosage"][b]).max() <= TOL
             diff = out[j]["haps"] != want["haps_argmax"][b]
             if diff.any():
@@ -87,3 +90,5 @@ def test_full_shape_against_oracle_on_short_regions(workload):
                 hi = oracle.fb_batch(codes[b:b + 1], pairs, sl, pos[m0:m1], L, 10000.0, tie_eps=1e-4 + 1e-5)
                 flip = (lo["haps_argmax"][0] != want["haps_argmax"][b]) | (hi["haps_argmax"][0] != want["haps_argmax"][b])
                 assert not (diff & ~flip).any()
+    from conftest import report
+    report("uneven full shape, shortest regions", targets=checked, max_abs_dosage_diff=worst)
