@@ -27,7 +27,6 @@ import argparse
 import json
 import os
 import statistics
-import subprocess
 import sys
 import time
 from pathlib import Path
@@ -77,47 +76,72 @@ def make_workload(cfg):
     return panel, pos, typed, codes, truth
 
 
+class _NvmlSampler:
+    """Reads SM clock, power and clock-event reasons every few ms from a thread
+    (NVML; read-only), so that even a timed region of tens of ms is covered."""
+
+    NAMES = {"hw_slowdown": "nvmlClocksEventReasonHwSlowdown",
+             "hw_thermal_slowdown": "nvmlClocksEventReasonHwThermalSlowdown",
+             "sw_thermal_slowdown": "nvmlClocksEventReasonSwThermalSlowdown",
+             "sw_power_cap": "nvmlClocksEventReasonSwPowerCap"}
+
+    def __init__(self, device: int, period_s: float = 0.002):
+        import threading
+        import pynvml as nv
+        self.nv = nv
+        nv.nvmlInit()
+        import os as _os
+        vis = _os.environ.get("CUDA_VISIBLE_DEVICES")
+        index = int(vis.split(",")[device]) if vis and vis.split(",")[device].isdigit() else device
+        self.h = nv.nvmlDeviceGetHandleByIndex(index)
+        self.max_mhz = float(nv.nvmlDeviceGetMaxClockInfo(self.h, nv.NVML_CLOCK_SM))
+        self.rows = []
+        self.stop_flag = threading.Event()
+        self.period = period_s
+        self.th = threading.Thread(target=self._run, daemon=True)
+        self.th.start()
+
+    def _run(self):
+        nv = self.nv
+        while not self.stop_flag.is_set():
+            try:
+                sm = nv.nvmlDeviceGetClockInfo(self.h, nv.NVML_CLOCK_SM)
+                pw = nv.nvmlDeviceGetPowerUsage(self.h) / 1000.0
+                rs = nv.nvmlDeviceGetCurrentClocksEventReasons(self.h)
+                self.rows.append((sm, pw, rs))
+            except Exception:
+                pass
+            self.stop_flag.wait(self.period)
+
+    def stop(self):
+        self.stop_flag.set()
+        self.th.join(timeout=5)
+        nv = self.nv
+        try:
+            nv.nvmlShutdown()
+        except Exception:
+            pass
+        if not self.rows:
+            return None
+        reasons = set()
+        for _, _, rs in self.rows:
+            for name, attr in self.NAMES.items():
+                if rs & getattr(nv, attr):
+                    reasons.add(name)
+        return {"sm_mhz": statistics.median(r[0] for r in self.rows), "sm_max_mhz": self.max_mhz,
+                "reasons": sorted(reasons), "samples": len(self.rows), "source": "nvml",
+                "power_w_max": max(r[1] for r in self.rows)}
+
+
 def clock_sampler_start(device: int):
-    import tempfile
     try:
-        f = tempfile.NamedTemporaryFile("w", suffix=".clocks.csv", delete=False)
-        p = subprocess.Popen(
-            ["nvidia-smi", f"--id={device}",
-             "--query-gpu=index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
-             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
-             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap",
-             "--format=csv,noheader,nounits", "-lms", "100"], stdout=f, stderr=subprocess.DEVNULL)
-        return p, f
+        return _NvmlSampler(device)
     except Exception:
-        return None, None
+        return None
 
 
 def clock_sampler_stop(handle):
-    p, f = handle
-    if p is None:
-        return None
-    p.terminate()
-    try:
-        p.wait(timeout=5)
-    except Exception:
-        p.kill()
-    f.close()
-    rows = []
-    for line in Path(f.name).read_text().splitlines():
-        parts = [x.strip() for x in line.split(",")]
-        if len(parts) >= 9 and parts[1].replace(".", "").isdigit():
-            rows.append(parts)
-    if not rows:
-        return None
-    sm = [float(r[1]) for r in rows]
-    reasons = set()
-    names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
-    for r in rows:
-        for name, v in zip(names, r[5:9]):
-            if v.lower() in ("active", "1"):
-                reasons.add(name)
-    return {"sm_mhz": statistics.median(sm), "sm_max_mhz": float(rows[0][2]), "reasons": sorted(reasons),
-            "samples": len(rows), "power_w_max": max(float(r[3]) for r in rows if r[3].replace(".", "").isdigit())}
+    return handle.stop() if handle is not None else None
 
 
 def peaks():

@@ -257,8 +257,13 @@ si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32
     a.threads = p->block_threads ? p->block_threads : typed_default_threads(lmax);
     if (typed_post_smem_bytes(lmax, a.threads, a.C) > 227u * 1024u)
         return fail(ctx, SI_ERR_UNSUPPORTED, "posterior tile needs more than 227 KB of shared memory");
-    if (!ctx->pinned_totals)
-        SI_CUDA(ctx, cudaMallocHost(&ctx->pinned_totals, 2 * sizeof(unsigned long long)), "pinned totals");
+    if (!ctx->pinned_totals) {
+        SI_CUDA(ctx, cudaHostAlloc(&ctx->pinned_totals, 2 * sizeof(unsigned long long), cudaHostAllocMapped),
+                "pinned totals");
+        SI_CUDA(ctx, cudaHostGetDevicePointer(&ctx->pinned_totals_dev, ctx->pinned_totals, 0), "pinned totals");
+    }
+    if (!ctx->totals_ev) SI_CUDA(ctx, cudaEventCreateWithFlags(&ctx->totals_ev, cudaEventDisableTiming), "event");
+    a.host_totals = ctx->pinned_totals_dev;
     const uint32_t B = a.B;
     SI_TRY(dev_reserve(ctx, ctx->t_counts, (size_t)B * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_aoff, ((size_t)B + 1) * 8));
@@ -267,10 +272,10 @@ si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32
     a.aoff = (unsigned long long*)ctx->t_aoff.ptr;
     a.woff = (unsigned long long*)ctx->t_woff.ptr;
     SI_CUDA(ctx, launch_anchor_lists_count(a, s), "anchor count");
-    SI_CUDA(ctx, cudaMemcpyAsync(ctx->pinned_totals, a.aoff + B, 8, cudaMemcpyDeviceToHost, s), "read totals");
-    SI_CUDA(ctx, cudaMemcpyAsync(ctx->pinned_totals + 1, a.woff + B, 8, cudaMemcpyDeviceToHost, s), "read totals");
-    SI_CUDA(ctx, cudaStreamSynchronize(s), "anchor count");
-    const unsigned long long NA = ctx->pinned_totals[0], NW = ctx->pinned_totals[1];
+    SI_CUDA(ctx, cudaEventRecord(ctx->totals_ev, s), "event");
+    SI_CUDA(ctx, cudaEventSynchronize(ctx->totals_ev), "anchor count");
+    const volatile unsigned long long* tot = ctx->pinned_totals;
+    const unsigned long long NA = tot[0], NW = tot[1];
     SI_TRY(dev_reserve(ctx, ctx->t_apos, (size_t)NA * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_aem, (size_t)NA * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_acode, (size_t)NA));
@@ -566,9 +571,12 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     }
     for (auto& kv : ctx->region_sel) dev_free(ctx, kv.second.masks);
     if (ctx->pinned_totals) cudaFreeHost(ctx->pinned_totals);
+    if (ctx->totals_ev) cudaEventDestroy(ctx->totals_ev);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
     for (auto& e : ctx->kev) if (e) cudaEventDestroy(e);
     if (ctx->stream) cudaStreamDestroy(ctx->stream);
+    if (ctx->copy_in) cudaStreamDestroy(ctx->copy_in);
+    if (ctx->copy_out) cudaStreamDestroy(ctx->copy_out);
     delete ctx;
     return SI_OK;
 }
@@ -784,27 +792,76 @@ si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno,
     const uint32_t M = ctx->M;
     const size_t cells = (size_t)B * M;
     cudaStream_t s = ctx->stream;
-    cudaEvent_t start;
-    SI_CUDA(ctx, cudaEventCreate(&start), "event");
-    SI_CUDA(ctx, cudaEventRecord(start, s), "event");
+    if (!ctx->copy_in) SI_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking), "copy stream");
+    if (!ctx->copy_out) SI_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking), "copy stream");
     SI_TRY(dev_reserve(ctx, ctx->io_geno, cells));
     if (dosage) SI_TRY(dev_reserve(ctx, ctx->io_dosage, cells * 4));
     if (hap_prob) SI_TRY(dev_reserve(ctx, ctx->io_hprob, cells * 8));
     if (haps) SI_TRY(dev_reserve(ctx, ctx->io_haps, cells * 2));
-    SI_CUDA(ctx, cudaMemcpyAsync(ctx->io_geno.ptr, geno, cells, cudaMemcpyHostToDevice, s), "copy geno");
-    SI_CUDA(ctx, cudaEventRecord(ctx->ev[0], s), "event");
-    SI_TRY(run_device(ctx, p, (const uint8_t*)ctx->io_geno.ptr, B, dosage ? (float*)ctx->io_dosage.ptr : nullptr,
-                      hap_prob ? (float*)ctx->io_hprob.ptr : nullptr, haps ? (uint8_t*)ctx->io_haps.ptr : nullptr, s));
-    if (dosage) SI_CUDA(ctx, cudaMemcpyAsync(dosage, ctx->io_dosage.ptr, cells * 4, cudaMemcpyDeviceToHost, s), "copy dosage");
-    if (hap_prob) SI_CUDA(ctx, cudaMemcpyAsync(hap_prob, ctx->io_hprob.ptr, cells * 8, cudaMemcpyDeviceToHost, s), "copy hprob");
-    if (haps) SI_CUDA(ctx, cudaMemcpyAsync(haps, ctx->io_haps.ptr, cells * 2, cudaMemcpyDeviceToHost, s), "copy haps");
-    SI_CUDA(ctx, cudaEventRecord(ctx->ev[3], s), "event");
-    SI_CUDA(ctx, cudaStreamSynchronize(s), "imputation");
+    // Samples in chunks of about 64 MB of codes: chunk k's codes go in on the
+    // copy-in stream, it is imputed on the ctx stream, and its outputs come
+    // back on the copy-out stream while chunk k+1 is imputed. A chunk keeps the
+    // global sample ids of its rows, so its draws do not depend on the split.
+    const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(B, ((size_t)64 << 20) / std::max<uint32_t>(M, 1)));
+    const uint32_t K = (B + per - 1) / per;
+    std::vector<cudaEvent_t> ev(2 * (size_t)K + 2, nullptr);
+    for (auto& x : ev) SI_CUDA(ctx, cudaEventCreateWithFlags(&x, cudaEventDefault), "event");
+    auto cleanup = [&] {
+        for (auto& x : ev)
+            if (x) cudaEventDestroy(x);
+    };
+    si_status st = SI_OK;
+    cudaError_t e = cudaEventRecord(ev[2 * K], s);  // start
+    if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_in, ev[2 * K], 0);
+    for (uint32_t k = 0; k < K && e == cudaSuccess; ++k) {
+        const size_t r0 = (size_t)k * per, rows = std::min<size_t>(per, B - r0);
+        e = cudaMemcpyAsync((uint8_t*)ctx->io_geno.ptr + r0 * M, geno + r0 * M, rows * M, cudaMemcpyHostToDevice,
+                            ctx->copy_in);
+        if (e == cudaSuccess) e = cudaEventRecord(ev[k], ctx->copy_in);
+    }
+    for (uint32_t k = 0; k < K && e == cudaSuccess && st == SI_OK; ++k) {
+        const size_t r0 = (size_t)k * per, rows = std::min<size_t>(per, B - r0);
+        e = cudaStreamWaitEvent(s, ev[k], 0);
+        if (e != cudaSuccess) break;
+        if (k + 1 == K) e = cudaEventRecord(ctx->ev[0], s);  // stage timings describe the last chunk
+        if (e != cudaSuccess) break;
+        si_impute_params pk = *p;
+        pk.sample_id_base = p->sample_id_base + r0;
+        if (k) pk.flags &= ~(uint32_t)SI_IMPUTE_RESELECT;  // the first chunk rebuilt the selection
+        st = run_device(ctx, &pk, (const uint8_t*)ctx->io_geno.ptr + r0 * M, (uint32_t)rows,
+                        dosage ? (float*)ctx->io_dosage.ptr + r0 * M : nullptr,
+                        hap_prob ? (float*)ctx->io_hprob.ptr + 2 * r0 * M : nullptr,
+                        haps ? (uint8_t*)ctx->io_haps.ptr + 2 * r0 * M : nullptr, s);
+        if (st != SI_OK) break;
+        e = cudaEventRecord(ev[K + k], s);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_out, ev[K + k], 0);
+        if (e == cudaSuccess && dosage)
+            e = cudaMemcpyAsync(dosage + r0 * M, (const float*)ctx->io_dosage.ptr + r0 * M, rows * M * 4,
+                                cudaMemcpyDeviceToHost, ctx->copy_out);
+        if (e == cudaSuccess && hap_prob)
+            e = cudaMemcpyAsync(hap_prob + 2 * r0 * M, (const float*)ctx->io_hprob.ptr + 2 * r0 * M, rows * M * 8,
+                                cudaMemcpyDeviceToHost, ctx->copy_out);
+        if (e == cudaSuccess && haps)
+            e = cudaMemcpyAsync(haps + 2 * r0 * M, (const uint8_t*)ctx->io_haps.ptr + 2 * r0 * M, rows * M * 2,
+                                cudaMemcpyDeviceToHost, ctx->copy_out);
+    }
+    if (e == cudaSuccess) e = cudaEventRecord(ev[2 * K + 1], ctx->copy_out);  // end
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->copy_out);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(s);
+    if (st == SI_OK && e != cudaSuccess) st = cuda_fail(ctx, e, "imputation");
+    if (st != SI_OK) {
+        cudaStreamSynchronize(ctx->copy_in);  // no copy may outlive the call
+        cudaStreamSynchronize(ctx->copy_out);
+        cudaStreamSynchronize(s);
+        cleanup();
+        return st;
+    }
+    // timings of the last chunk's stages; [2] is the whole call, copies included
     cudaEventElapsedTime(&ctx->last_ms[0], ctx->ev[0], ctx->ev[1]);
     cudaEventElapsedTime(&ctx->last_ms[1], ctx->ev[1], ctx->ev[2]);
-    cudaEventElapsedTime(&ctx->last_ms[2], start, ctx->ev[3]);
+    cudaEventElapsedTime(&ctx->last_ms[2], ev[2 * K], ev[2 * K + 1]);
     ctx->timings_pending = false;
-    cudaEventDestroy(start);
+    cleanup();
     return SI_OK;
 }
 

@@ -53,6 +53,7 @@ struct TypedArgs {
     uint32_t* counts;                // [B] anchors of each job (written by the count kernel)
     int capacity;                    // offsets are capacities fixed in advance: clamp counts to them
     uint32_t* err;                   // device flag: bit 0 set when a job had more anchors than its capacity
+    unsigned long long* host_totals; // mapped host memory for the two list totals (may be null)
     uint32_t* apos;                  // anchor positions (within the slice)
     uint32_t* aem;                   // anchor emission masks over the slots
     uint8_t* ashift;                 // 1 where no slot matches the call (every slot scaled by e^-999)

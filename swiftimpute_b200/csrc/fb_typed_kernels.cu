@@ -138,10 +138,13 @@ __global__ void anchor_count_kernel(TypedArgs A) {
 }
 
 // Exclusive scans of anchor counts and window counts (ceil(count / C)) in one
-// CTA; entry B holds the totals.
+// CTA; entry B holds the totals, also written to host_totals (mapped pinned
+// host memory) when given: a copy would queue behind other device-to-host
+// copies on the copy engine.
 __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __restrict__ counts, uint32_t B,
                                                            uint32_t C, unsigned long long* __restrict__ aoff,
-                                                           unsigned long long* __restrict__ woff) {
+                                                           unsigned long long* __restrict__ woff,
+                                                           unsigned long long* __restrict__ host_totals) {
     __shared__ unsigned long long sa[32], sw[32];
     const uint32_t t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5;
     const uint32_t per = (B + T - 1) / T;
@@ -175,7 +178,15 @@ __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __res
         ra += counts[b];
         rw += (counts[b] + C - 1) / C;
     }
-    if (t == T - 1) { aoff[B] = ra; woff[B] = rw; }
+    if (t == T - 1) {
+        aoff[B] = ra;
+        woff[B] = rw;
+        if (host_totals) {  // mapped host memory: the host reads the totals without a copy
+            host_totals[0] = ra;
+            host_totals[1] = rw;
+            __threadfence_system();
+        }
+    }
 }
 
 // Anchor lists: marker position, emission mask over the slots and the
@@ -808,7 +819,7 @@ cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s) {
     anchor_count_kernel<<<(a.B + kWarpsPerBlock - 1) / kWarpsPerBlock, kWarpsPerBlock * 32, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
-    anchor_scan_kernel<<<1, 1024, 0, s>>>(a.counts, a.B, a.C, a.aoff, a.woff);
+    anchor_scan_kernel<<<1, 1024, 0, s>>>(a.counts, a.B, a.C, a.aoff, a.woff, a.host_totals);
     return cudaGetLastError();
 }
 

@@ -65,6 +65,7 @@ struct si_ctx {
     uint64_t used = 0;
     std::string err;
     cudaStream_t stream = nullptr;
+    cudaStream_t copy_in = nullptr, copy_out = nullptr;  // host-buffer calls: copies beside the compute
     cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
     cudaEvent_t kev[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};  // per-kernel timing of the last call
     float kernel_ms[4] = {0.f, 0.f, 0.f, 0.f};
@@ -105,7 +106,9 @@ struct si_ctx {
     };
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, RegionSel> region_sel;
     si::DeviceBuffer job_regions, job_samples;  // uploaded descriptors of the last uneven batch
-    unsigned long long* pinned_totals = nullptr;
+    unsigned long long* pinned_totals = nullptr;  // mapped: written by the scan kernel
+    unsigned long long* pinned_totals_dev = nullptr;
+    cudaEvent_t totals_ev = nullptr;
     si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
     float last_ms[3] = {0.f, 0.f, 0.f};
     bool timings_pending = false;

@@ -267,3 +267,25 @@ def test_long_untyped_gaps_beyond_tables(engine):
     compare(engine, panel, pos, codes, 8, 10000)
     panel, pos, codes, _ = workload(9000, 200, 6, np.array([3, 4500]), 500_000, 22)
     compare(engine, panel, pos, codes, 4, 10000)
+
+
+@pytest.mark.parametrize("sampling", [N.SAMPLE_ARGMAX, N.SAMPLE_PHILOX])
+def test_host_buffer_call_in_chunks_equals_one_launch(engine, sampling):
+    # 50,000 markers: the host-buffer call splits 2,700 targets into chunks of 1,342 (64 MB of codes)
+    import torch
+    panel, pos, codes, _ = workload(50_000, 400, 2700, synth.typed_every(50_000, 9), 100, 14)
+    load(engine, panel, pos, store=False)
+    p = N.default_params(sampling=sampling, seed=21, sample_id_base=5000)
+    got = engine.impute(codes, p, hap_prob=True)
+    B, M = codes.shape
+    dev = torch.device("cuda", 0)
+    d_geno = torch.from_numpy(codes).to(dev)
+    d_dos = torch.empty((B, M), dtype=torch.float32, device=dev)
+    d_hp = torch.empty((B, M, 2), dtype=torch.float32, device=dev)
+    d_haps = torch.empty((B, 2, M), dtype=torch.uint8, device=dev)
+    torch.cuda.synchronize(dev)
+    engine.impute_device(d_geno.data_ptr(), B, p, d_dos.data_ptr(), d_hp.data_ptr(), d_haps.data_ptr())
+    torch.cuda.synchronize(dev)
+    assert np.array_equal(got["dosage"], d_dos.cpu().numpy())
+    assert np.array_equal(got["hap_prob"], d_hp.cpu().numpy())
+    assert np.array_equal(got["haps"], d_haps.cpu().numpy())
