@@ -43,7 +43,7 @@ CONFIGS = {
     # (log-uniform) over 1,000-50,000 markers (log-uniform length, uniform start), typed every 20th
     # marker, L from {4, 8, 16}, Poisson arrivals
     "serving": dict(M=120_000, N=8000, founders=200, beta=(0.3, 0.6), switch=0.002, every=20, ne=20000, seed=4,
-                    pool=1024, rate=200.0, seconds=10.0),
+                    pool=1024, rate=200.0, seconds=10.0, hbm_budget=120 << 30),
 }
 ALGO_BYTES_PER_CELL = 7  # 1 B genotype code in, 4 B dosage + 2 B haplotype alleles out
 POST_BYTES_PER_CELL = 6  # the posterior pass writes the outputs: 4 B dosage + 2 B alleles
@@ -261,7 +261,7 @@ def run_serving(args, cfg):
     # the clients' output buffers, allocated and touched before the run (a client reuses its buffers)
     outs = [{"dosage": np.full(r[3].shape, 0, np.float32), "haps": np.full((r[3].shape[0], 2, r[3].shape[1]), 0, np.uint8)}
             for r in reqs]
-    eng = Engine(int(os.environ.get("LOCAL_RANK", "0")))
+    eng = Engine(int(os.environ.get("LOCAL_RANK", "0")), hbm_budget_bytes=cfg["hbm_budget"])
     eng.upload_panel(panel)
     eng.set_map(pos)
     eng.pbwt_build()
@@ -271,28 +271,35 @@ def run_serving(args, cfg):
     with Server(eng, params) as srv:
         for L in (4, 8, 16):
             srv.wait(srv.submit(0, 50_000, pool[:512, :50_000], num_states=L, index_origin=N.INDEX_GLOBAL))
+    def run(max_batch_requests):
+        """Replay the arrivals through a server; returns (statistics, wall seconds)."""
+        srv = Server(eng, params, max_batch_requests=max_batch_requests)
+        tickets = [None] * len(reqs)
+        t0 = time.perf_counter()
+
+        def submitter():
+            for i, (a, b, L, codes) in enumerate(reqs):
+                d = t0 + arrivals[i] - time.perf_counter()
+                if d > 0:
+                    time.sleep(d)
+                tickets[i] = srv.submit(a, b, codes, num_states=L, index_origin=N.INDEX_GLOBAL,
+                                        sample_id_base=i << 10, out=outs[i])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        th.join()
+        for t in tickets:
+            srv.wait(t)
+        wall = time.perf_counter() - t0
+        st = srv.stats()
+        srv.stop()
+        return st, wall
+
     clocks = clock_sampler_start(int(os.environ.get("LOCAL_RANK", "0")))
-    srv = Server(eng, params)
-    tickets = [None] * len(reqs)
-    t0 = time.perf_counter()
-
-    def submitter():
-        for i, (a, b, L, codes) in enumerate(reqs):
-            d = t0 + arrivals[i] - time.perf_counter()
-            if d > 0:
-                time.sleep(d)
-            tickets[i] = srv.submit(a, b, codes, num_states=L, index_origin=N.INDEX_GLOBAL, sample_id_base=i << 10,
-                                    out=outs[i])
-
-    th = threading.Thread(target=submitter)
-    th.start()
-    th.join()
-    for t in tickets:
-        srv.wait(t)
-    wall = time.perf_counter() - t0
-    st = srv.stats()
-    srv.stop()
+    st, wall = run(0)
     clock_info = clock_sampler_stop(clocks)
+    # the same arrivals served one request per launch (no batching)
+    st1, wall1 = run(1)
     eng.close()
     if rank != 0:
         return
@@ -313,6 +320,11 @@ def run_serving(args, cfg):
                           "peak": peak, "unit": "GB/s", "peak_kind": peak_kind,
                           "note": "7 B per cell over busy intervals (host copies included)"},
         "completed": st["completed"], "failed": st["failed"],
+        "hbm_budget_bytes": cfg["hbm_budget"],
+        "one_request_per_launch": {"cells_per_s": st1["cells"] / wall1,
+                                   "latency_ms": {"p50": st1["latency_p50_ms"], "p99": st1["latency_p99_ms"],
+                                                  "max": st1["latency_max_ms"]},
+                                   "busy_fraction": st1["busy_ms"] / 1e3 / wall1, "launches": st1["batches"]},
     }
     if clock_info:
         line["clocks"] = clock_info

@@ -294,6 +294,8 @@ typedef struct {
                                   (7 B per cell pinned and on the device) are allocated at start */
     uint32_t max_wait_us;      /* how long the oldest queued request waits for company; 0 = 200 */
     uint32_t max_queue;        /* queued requests before si_serve_submit refuses; 0 = 65536 */
+    uint32_t max_batch_requests; /* requests per launch; 0 = no limit (1 = one request per launch) */
+    uint32_t reserved;
 } si_serve_config;
 
 typedef struct {

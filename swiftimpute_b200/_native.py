@@ -75,7 +75,8 @@ class Job(ctypes.Structure):
 # (name, restype, argtypes) for every symbol the header declares.
 class ServeConfig(ctypes.Structure):
     """Mirror of ``si_serve_config``."""
-    _fields_ = [("max_batch_cells", c_uint64), ("max_wait_us", c_uint32), ("max_queue", c_uint32)]
+    _fields_ = [("max_batch_cells", c_uint64), ("max_wait_us", c_uint32), ("max_queue", c_uint32),
+                ("max_batch_requests", c_uint32), ("reserved", c_uint32)]
 
 
 class Request(ctypes.Structure):

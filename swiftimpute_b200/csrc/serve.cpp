@@ -74,6 +74,7 @@ struct si_server {
     uint64_t max_cells = 0;
     uint32_t max_wait_us = 0;
     uint32_t max_queue = 0;
+    uint32_t max_requests = 0;  // per launch; 0 = no limit
 
     std::mutex mu;
     std::condition_variable cv_work;  // the worker waits for requests
@@ -302,7 +303,8 @@ void worker_main(si_server* S) {
         if (S->stopping) break;
         // let the oldest request wait up to max_wait_us for company, unless a launch is full already
         const auto deadline = S->queue.front()->t_submit + std::chrono::microseconds(S->max_wait_us);
-        while (!S->stopping && !S->queue.empty() && S->queued_cells < S->max_cells && Clock::now() < deadline)
+        while (!S->stopping && !S->queue.empty() && S->queued_cells < S->max_cells && S->max_requests != 1 &&
+               Clock::now() < deadline)
             S->cv_work.wait_until(lk, deadline);
         if (S->stopping) break;
         // the slot must be drained by the completion thread before it is refilled
@@ -314,6 +316,7 @@ void worker_main(si_server* S) {
         Need need;
         uint64_t cells = 0;
         while (!S->queue.empty()) {
+            if (S->max_requests && z.batch.size() >= S->max_requests) break;
             std::shared_ptr<Pending> p = S->queue.front();
             const uint64_t c = cells_of(p->req);
             if (cells + c > S->max_cells) break;
@@ -385,6 +388,7 @@ si_status si_serve_start(si_ctx* ctx, const si_impute_params* params, const si_s
     S->max_cells = cfg && cfg->max_batch_cells ? cfg->max_batch_cells : (1ull << 25);
     S->max_wait_us = cfg && cfg->max_wait_us ? cfg->max_wait_us : 200u;
     S->max_queue = cfg && cfg->max_queue ? cfg->max_queue : 65536u;
+    S->max_requests = cfg ? cfg->max_batch_requests : 0u;
     S->t_start = Clock::now();
     for (auto& z : S->slot) {
         if (cudaSetDevice(ctx->device) != cudaSuccess ||

@@ -198,11 +198,11 @@ class Server:
     """
 
     def __init__(self, engine: Engine, params: N.ImputeParams | None = None, *, max_batch_cells: int = 0,
-                 max_wait_us: int = 0, max_queue: int = 0):
+                 max_wait_us: int = 0, max_queue: int = 0, max_batch_requests: int = 0):
         self.engine = engine
         self.lib = engine.lib
         self.params = params or N.default_params()
-        cfg = N.ServeConfig(max_batch_cells, max_wait_us, max_queue)
+        cfg = N.ServeConfig(max_batch_cells, max_wait_us, max_queue, max_batch_requests, 0)
         h = c_void_p()
         engine._check(self.lib.si_serve_start(engine.h, byref(self.params), byref(cfg), byref(h)))
         self.h = h
