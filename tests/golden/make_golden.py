@@ -3,10 +3,11 @@
 
   python tests/golden/make_golden.py cpu   PBWT prefix arrays from the reference's
                                            PBWTBuilder (oracle/_ref/libref_pbwt.so, CPU)
-  python tests/golden/make_golden.py gpu   selection slots, log posteriors and argmax
+  python tests/golden/make_golden.py gpu [DIR]
+                                           selection slots, log posteriors and argmax
                                            haplotypes from the reference's CUDA kernels
                                            (oracle/_ref/libref_gpu.so) on a B200; writes
-                                           gpurun_out/golden_ref_gpu.npz to be copied here
+                                           DIR/ref_gpu_kernels.npz (DIR defaults to tests/golden)
 
 Both libraries are the reference compiled from its unmodified sources by
 oracle/Makefile. Inputs come from the seeded synthetic generator, except the
@@ -91,7 +92,7 @@ def gpu():
         fix[f"{name}_logpost"] = lp
         fix[f"{name}_haps"] = haps
         print(name, "stage ms", ms)
-    out = ROOT / "gpurun_out" / "golden_ref_gpu.npz"
+    out = Path(sys.argv[2] if len(sys.argv) > 2 else ROOT / "tests" / "golden") / "ref_gpu_kernels.npz"
     out.parent.mkdir(exist_ok=True)
     np.savez_compressed(out, **fix)
     print("wrote", out)
