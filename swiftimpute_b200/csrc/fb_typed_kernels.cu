@@ -378,12 +378,24 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
                 pn[i] = k < NA ? pos[k] : 0u;
                 en[i] = k < NA ? aem[k] : 0u;
             }
+            // the block's entries and run tables first, off the dependent chain
+            uint32_t pj[kChainBlock], ej[kChainBlock];
+            float2 qj[kChainBlock];
 #pragma unroll
             for (uint32_t j = 0; j < kChainBlock; ++j) {
-                const uint32_t p = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
-                const uint32_t em = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
+                pj[j] = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
+                ej[j] = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kChainBlock; ++j) {
+                const uint32_t before = j ? pj[j - 1] : prev;
+                qj[j] = tabQS(tb, k0 + j < NA ? pj[j] - before : 0u);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kChainBlock; ++j) {
+                const uint32_t p = pj[j], em = ej[j];
                 const bool act = k0 + j < NA;
-                const float2 qs = tabQS(tb, act ? p - prev : 0u);
+                const float2 qs = qj[j];
                 const float b = sa * qs.y;
                 float an[4];
 #pragma unroll
@@ -440,15 +452,30 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
             uint32_t pn[R], en[R], hn[R];
 #pragma unroll
             for (uint32_t i = 0; i < R; ++i) load(t0 + kChainBlock + kl + G * i, pn[i], en[i], hn[i]);
+            // the block's entries and run tables first, off the dependent chain
+            uint32_t pj[kChainBlock], ej[kChainBlock], hj[kChainBlock], nj[kChainBlock];
+            float2 qj[kChainBlock];
+            double gj[kChainBlock];
 #pragma unroll
             for (uint32_t j = 0; j < kChainBlock; ++j) {
-                const uint32_t p = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
-                const uint32_t em = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
-                const uint32_t sh = __shfl_sync(0xffffffffu, hv[j / G], g0 + j % G);
+                pj[j] = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
+                ej[j] = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
+                hj[j] = __shfl_sync(0xffffffffu, hv[j / G], g0 + j % G);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kChainBlock; ++j) {
+                const uint32_t after = j ? pj[j - 1] : nextp;
+                nj[j] = t0 + j + 2 <= NA ? after - pj[j] : 0u;
+                qj[j] = tabQS(tb, nj[j]);
+                gj[j] = tabG(tb, nj[j]);
+            }
+#pragma unroll
+            for (uint32_t j = 0; j < kChainBlock; ++j) {
+                const uint32_t p = pj[j], em = ej[j], sh = hj[j];
                 const bool act = t0 + j + 2 <= NA;
-                const uint32_t n = act ? nextp - p : 0u;
-                const float2 qs = tabQS(tb, n);
-                const double fterm = act ? -999.0 - logU + tabG(tb, n) : -1000.0;
+                const uint32_t n = nj[j];
+                const float2 qs = qj[j];
+                const double fterm = act ? -999.0 - logU + gj[j] : -1000.0;
                 // fterm > 0: the floor dominates and the unit becomes U rho^n e^fterm
                 const bool big = fterm > 0.0;
                 const float ex = expf(-(float)fmin(fabs(fterm), 104.0));
@@ -591,11 +618,13 @@ __device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v,
         const float4* RW = reinterpret_cast<const float4*>(recW + (size_t)u * LM);
         const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
         const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
+        // beta uniform in every lane: w' is multiplied by 0, so it need not be read
+        const bool all_uni = __all_sync(0xffffffffu, uni);
         float pr[LM];
         float2 tot2 = make_float2(0.f, 0.f), q02 = tot2, q12 = tot2;
 #pragma unroll
         for (int q4 = 0; q4 < LM / 4; ++q4) {
-            const float4 av = RA[q4], wv = RW[q4];
+            const float4 av = RA[q4], wv = all_uni ? make_float4(0.f, 0.f, 0.f, 0.f) : RW[q4];
             float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.x, av.y), YF),
                                     __ffma2_rn(XB, make_float2(wv.x, wv.y), YB));
             float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.z, av.w), YF),
