@@ -335,6 +335,7 @@ def run_ours(args, cfg):
     import torch
     from swiftimpute_b200 import _native as N
     from swiftimpute_b200.engine import Engine
+    from swiftimpute_b200.replicas import max_over_ranks
 
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -389,10 +390,7 @@ def run_ours(args, cfg):
     clock_info = clock_sampler_stop(clocks)
     total_ms = t_start.elapsed_time(t_end)
     kern_ms = [a.elapsed_time(b) for a, b in evs]
-    if dist:
-        t = torch.tensor([total_ms], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms, dist, dev)
     ms_per_step = total_ms / args.steps
     imputed_per_gpu = B * (M - len(typed))
     value = world * imputed_per_gpu / (ms_per_step / 1e3)
@@ -414,10 +412,7 @@ def run_ours(args, cfg):
     for _ in range(args.e2e_steps):
         e2e_step()
     e2e_s = (time.perf_counter() - t0) / args.e2e_steps
-    if dist:
-        t = torch.tensor([e2e_s], device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        e2e_s = float(t.item())
+    e2e_s = max_over_ranks(e2e_s, dist, dev)
     e2e_value = world * imputed_per_gpu / e2e_s
     # quality vs truth on the device outputs (masked markers)
     dos = d_dos.cpu().numpy()
