@@ -679,7 +679,7 @@ __device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v,
 
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
 template <int LM, bool kFull>
-__global__ void __launch_bounds__(128, (LM <= 8 ? 6 : 4)) anchor_posterior_kernel(TypedArgs A) {
+__global__ void __launch_bounds__(128, (LM <= 8 ? 7 : 4)) anchor_posterior_kernel(TypedArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     const uint32_t t = threadIdx.x, C = A.C, lane = t & 31, warp = t >> 5;
     // nibble -> four 0/1 floats, 8 copies so that the 8 lanes of a quarter warp
