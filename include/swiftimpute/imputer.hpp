@@ -13,7 +13,8 @@
 //     (sum of the two phased alleles, imputer.cpp:418-425).
 //   * ReferencePanel::from_haplotypes / TargetData::from_genotypes build inputs
 //     in memory (the reference's constructors are private, imputer.hpp:98-103,
-//     139-143), and load_binary / save_binary work (they throw in the reference).
+//     139-143), and load_binary / save_binary work (they throw in the reference);
+//     TargetData gains the same pair, storing 2 bits per genotype.
 //   * Panel alleles must be 0/1 (the device stores one bit per allele).
 #pragma once
 
@@ -183,6 +184,9 @@ public:
     // genotype codes [B][M]: 0/1/2 ALT count, 3 (or any other value) = missing
     static std::unique_ptr<TargetData> from_genotypes(std::vector<Marker> markers, std::vector<Sample> samples,
                                                       const uint8_t* codes);
+    // 2 bits per cell (the ALT count, 3 = missing) instead of the 12-byte likelihood triple
+    static std::unique_ptr<TargetData> load_binary(const std::string& filename);
+    void save_binary(const std::string& filename) const;
 
     marker_t num_markers() const { return static_cast<marker_t>(markers_.size()); }
     sample_t num_samples() const { return static_cast<sample_t>(samples_.size()); }
@@ -261,6 +265,38 @@ private:
 
     void ensure_panel();
     void check(int status, const char* what) const;
+    // imputes target rows [begin, end) into the same rows of `result`; Philox
+    // draws are keyed by the global row index, so a row does not depend on
+    // which call, pass or device imputes it
+    void impute_rows(const TargetData& targets, sample_t begin, sample_t end, ImputationResult& result,
+                     const std::function<void(uint32_t, uint32_t)>& progress_callback);
+    friend class MultiGPUImputer;
+};
+
+// Sample-sharded replicas on several devices (src/api/imputer.hpp:298-328; the
+// reference's impute() runs everything on the first device). Each device holds
+// its own panel and index; impute() splits the targets into contiguous shards
+// whose sizes differ by at most one and imputes them on one host thread per
+// device, with no traffic between devices. Results are bit-identical to one
+// Imputer over all targets. A device id may repeat: each entry is one replica.
+class MultiGPUImputer {
+public:
+    MultiGPUImputer(const ReferencePanel& reference, const std::vector<int>& device_ids,
+                    const ImputationConfig& config = ImputationConfig());
+    ~MultiGPUImputer();
+
+    void build_indices();
+    std::unique_ptr<ImputationResult> impute(const TargetData& targets);
+    uint32_t num_gpus() const { return static_cast<uint32_t>(imputers_.size()); }
+
+private:
+    const ReferencePanel& reference_;
+    ImputationConfig config_;
+    std::vector<int> device_ids_;
+    std::vector<std::unique_ptr<Imputer>> imputers_;
+
+    void partition_samples(uint32_t num_samples, std::vector<uint32_t>& start_indices,
+                           std::vector<uint32_t>& end_indices) const;
 };
 
 std::unique_ptr<ImputationResult> impute(const std::string& reference_vcf, const std::string& target_vcf,

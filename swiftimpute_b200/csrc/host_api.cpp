@@ -10,11 +10,13 @@
 #include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <exception>
 #include <fstream>
 #include <iomanip>
 #include <iostream>
 #include <mutex>
 #include <sstream>
+#include <thread>
 
 namespace swiftimpute {
 namespace {
@@ -271,24 +273,68 @@ std::unique_ptr<ReferencePanel> ReferencePanel::from_haplotypes(std::vector<Mark
     return p;
 }
 
-// Binary panel: magic "SIPANEL1", M, N (u32), per marker: chrom, id, ref, alt
-// (u32 length + bytes), pos (u64), cM (f64); sample ids; then the alleles
-// bit-packed per marker (ceil(N/8) bytes, haplotype h at bit h%8 of byte h/8).
-void ReferencePanel::save_binary(const std::string& filename) const {
-    std::ofstream o(filename, std::ios::binary);
-    if (!o) throw ImputationError("Cannot write " + filename);
-    auto put_u32 = [&](uint32_t x) { o.write(reinterpret_cast<const char*>(&x), 4); };
-    auto put_str = [&](const std::string& s) { put_u32((uint32_t)s.size()); o.write(s.data(), s.size()); };
-    o.write("SIPANEL1", 8);
-    put_u32(num_markers());
-    put_u32(num_haplotypes_);
-    for (const auto& m : markers_) {
-        put_str(m.chrom); put_str(m.id); put_str(m.ref); put_str(m.alt);
+namespace {
+
+void put_u32(std::ostream& o, uint32_t x) { o.write(reinterpret_cast<const char*>(&x), 4); }
+void put_str(std::ostream& o, const std::string& s) {
+    put_u32(o, (uint32_t)s.size());
+    o.write(s.data(), s.size());
+}
+uint32_t get_u32(std::istream& in) {
+    uint32_t x = 0;
+    in.read(reinterpret_cast<char*>(&x), 4);
+    return x;
+}
+std::string get_str(std::istream& in) {
+    const uint32_t n = get_u32(in);
+    if (!in || n > (1u << 20)) throw ImputationError("corrupt string field in binary file");
+    std::string s(n, '\0');
+    in.read(&s[0], n);
+    return s;
+}
+
+// per marker: chrom, id, ref, alt (u32 length + bytes), pos (u64), cM (f64);
+// then the sample count and ids. The same in panel and target files.
+void put_meta(std::ostream& o, const std::vector<Marker>& markers, const std::vector<Sample>& samples) {
+    for (const auto& m : markers) {
+        put_str(o, m.chrom); put_str(o, m.id); put_str(o, m.ref); put_str(o, m.alt);
         o.write(reinterpret_cast<const char*>(&m.pos), 8);
         o.write(reinterpret_cast<const char*>(&m.cM), 8);
     }
-    put_u32((uint32_t)samples_.size());
-    for (const auto& s : samples_) put_str(s.id);
+    put_u32(o, (uint32_t)samples.size());
+    for (const auto& s : samples) put_str(o, s.id);
+}
+void get_meta(std::istream& in, uint32_t M, std::vector<Marker>& markers, std::vector<std::string>& names) {
+    if (!in) throw ImputationError("truncated binary file header");
+    markers.resize(M);
+    for (auto& m : markers) {
+        m.chrom = get_str(in); m.id = get_str(in); m.ref = get_str(in); m.alt = get_str(in);
+        in.read(reinterpret_cast<char*>(&m.pos), 8);
+        in.read(reinterpret_cast<char*>(&m.cM), 8);
+    }
+    names.resize(get_u32(in));
+    for (auto& s : names) s = get_str(in);
+    if (!in) throw ImputationError("truncated binary file header");
+}
+
+void check_magic(std::istream& in, const char* magic, const char* what, const std::string& filename) {
+    char got[8];
+    in.read(got, 8);
+    if (!in || std::memcmp(got, magic, 8) != 0) throw ImputationError(std::string("not a ") + what + ": " + filename);
+}
+
+}  // namespace
+
+// Binary panel: magic "SIPANEL1", M and N (u32), the markers and sample ids,
+// then the alleles bit-packed per marker: ceil(N/8) bytes, haplotype h at bit
+// h%8 of byte h/8
+void ReferencePanel::save_binary(const std::string& filename) const {
+    std::ofstream o(filename, std::ios::binary);
+    if (!o) throw ImputationError("Cannot write " + filename);
+    o.write("SIPANEL1", 8);
+    put_u32(o, num_markers());
+    put_u32(o, num_haplotypes_);
+    put_meta(o, markers_, samples_);
     const size_t rb = (num_haplotypes_ + 7) / 8;
     std::vector<char> row(rb);
     for (marker_t m = 0; m < num_markers(); ++m) {
@@ -306,20 +352,11 @@ void ReferencePanel::save_binary(const std::string& filename) const {
 std::unique_ptr<ReferencePanel> ReferencePanel::load_binary(const std::string& filename) {
     std::ifstream in(filename, std::ios::binary);
     if (!in) throw ImputationError("Cannot open " + filename);
-    char magic[8];
-    in.read(magic, 8);
-    if (!in || std::memcmp(magic, "SIPANEL1", 8) != 0) throw ImputationError("not a binary panel: " + filename);
-    auto get_u32 = [&]() { uint32_t x = 0; in.read(reinterpret_cast<char*>(&x), 4); return x; };
-    auto get_str = [&]() { std::string s(get_u32(), '\0'); in.read(&s[0], s.size()); return s; };
-    const uint32_t M = get_u32(), N = get_u32();
-    std::vector<Marker> ms(M);
-    for (auto& m : ms) {
-        m.chrom = get_str(); m.id = get_str(); m.ref = get_str(); m.alt = get_str();
-        in.read(reinterpret_cast<char*>(&m.pos), 8);
-        in.read(reinterpret_cast<char*>(&m.cM), 8);
-    }
-    std::vector<std::string> names(get_u32());
-    for (auto& s : names) s = get_str();
+    check_magic(in, "SIPANEL1", "binary panel", filename);
+    const uint32_t M = get_u32(in), N = get_u32(in);
+    std::vector<Marker> ms;
+    std::vector<std::string> names;
+    get_meta(in, M, ms, names);
     const size_t rb = (N + 7) / 8;
     auto h = std::make_unique<allele_t[]>((size_t)M * N);
     std::vector<unsigned char> row(rb);
@@ -375,6 +412,60 @@ std::unique_ptr<TargetData> TargetData::from_genotypes(std::vector<Marker> marke
                                         : GenotypeLikelihoods();
     }
     return t;
+}
+
+namespace {
+
+// the four likelihood triples a target cell can hold (imputer.cpp:263-287)
+// and their genotype codes: 0/1/2 ALT alleles, 3 = missing
+uint8_t gl_code(const GenotypeLikelihoods& g) {
+    const auto is = [&](prob_t a, prob_t b, prob_t c) { return g.ll_00 == a && g.ll_01 == b && g.ll_11 == c; };
+    if (is(0.f, kLog10Zero, kLog10Zero)) return 0;
+    if (is(kLog10Zero, 0.f, kLog10Zero)) return 1;
+    if (is(kLog10Zero, kLog10Zero, 0.f)) return 2;
+    if (g.ll_00 == g.ll_01 && g.ll_01 == g.ll_11) return 3;
+    throw ImputationError("binary target format stores hard calls and missing cells only");
+}
+
+}  // namespace
+
+// Binary targets: magic "SITARGT1", M (u32), the markers and sample ids, then
+// one row of ceil(M/4) bytes per sample, the code of marker m at bits
+// 2(m%4)..2(m%4)+1 of byte m/4: 2 bits per cell instead of the 12-byte
+// likelihood triple
+void TargetData::save_binary(const std::string& filename) const {
+    std::ofstream o(filename, std::ios::binary);
+    if (!o) throw ImputationError("Cannot write " + filename);
+    o.write("SITARGT1", 8);
+    put_u32(o, (uint32_t)markers_.size());
+    put_meta(o, markers_, samples_);
+    const size_t M = markers_.size(), rb = (M + 3) / 4;
+    std::vector<unsigned char> row(rb);
+    for (size_t s = 0; s < samples_.size(); ++s) {
+        std::fill(row.begin(), row.end(), 0);
+        for (size_t m = 0; m < M; ++m) row[m / 4] |= (unsigned char)(gl_code(genotype_liks_[s * M + m]) << (2 * (m % 4)));
+        o.write(reinterpret_cast<const char*>(row.data()), rb);
+    }
+    if (!o) throw ImputationError("write failed: " + filename);
+}
+
+std::unique_ptr<TargetData> TargetData::load_binary(const std::string& filename) {
+    std::ifstream in(filename, std::ios::binary);
+    if (!in) throw ImputationError("Cannot open " + filename);
+    check_magic(in, "SITARGT1", "binary target file", filename);
+    const uint32_t n_markers = get_u32(in);
+    std::vector<Marker> ms;
+    std::vector<std::string> names;
+    get_meta(in, n_markers, ms, names);
+    const size_t M = ms.size(), B = names.size(), rb = (M + 3) / 4;
+    std::vector<uint8_t> codes(B * M);
+    std::vector<unsigned char> row(rb);
+    for (size_t s = 0; s < B; ++s) {
+        in.read(reinterpret_cast<char*>(row.data()), rb);
+        for (size_t m = 0; m < M; ++m) codes[s * M + m] = (row[m / 4] >> (2 * (m % 4))) & 3u;
+    }
+    if (!in) throw ImputationError("truncated binary target file: " + filename);
+    return from_genotypes(std::move(ms), to_samples(names), codes.data());
 }
 
 GenotypeLikelihoods TargetData::get_likelihood(sample_t s, marker_t m) const {
@@ -560,13 +651,20 @@ std::unique_ptr<ImputationResult> Imputer::impute(const TargetData& targets) {
 
 std::unique_ptr<ImputationResult> Imputer::impute_with_progress(
     const TargetData& targets, std::function<void(uint32_t, uint32_t)> progress_callback) {
+    auto result = std::make_unique<ImputationResult>(targets.num_samples(), targets.num_markers());
+    impute_rows(targets, 0, targets.num_samples(), *result, progress_callback);
+    result->compute_info_scores();
+    return result;
+}
+
+void Imputer::impute_rows(const TargetData& targets, sample_t begin, sample_t end, ImputationResult& result,
+                          const std::function<void(uint32_t, uint32_t)>& progress_callback) {
     if (targets.num_markers() != reference_.num_markers())  // imputer.cpp:730-741
         throw ImputationError("Target and reference marker counts don't match: " +
                               std::to_string(targets.num_markers()) + " vs " +
                               std::to_string(reference_.num_markers()));
     ensure_panel();
-    const uint32_t B = targets.num_samples(), M = targets.num_markers();
-    auto result = std::make_unique<ImputationResult>(B, M);
+    const uint32_t B = end - begin, M = targets.num_markers();
     si_impute_params p;
     si_impute_params_default(&p);
     p.num_states = config_.hmm_params.num_states;
@@ -589,17 +687,15 @@ std::unique_ptr<ImputationResult> Imputer::impute_with_progress(
     uint32_t chunk = (uint32_t)std::max<uint64_t>(1, std::min<uint64_t>(B, room / per_sample));
     chunk = std::max<uint32_t>(std::min<uint32_t>(chunk, B), std::min<uint32_t>(B, config_.batch_size));
     if (config_.max_samples_per_call) chunk = std::min<uint32_t>(chunk, config_.max_samples_per_call);
-    for (uint32_t s0 = 0; s0 < B; s0 += chunk) {
-        const uint32_t n = std::min(chunk, B - s0);
+    for (uint32_t s0 = begin; s0 < end; s0 += chunk) {
+        const uint32_t n = std::min(chunk, end - s0);
         p.sample_id_base = s0;
         check(si_impute_gl(ctx_, &p, reinterpret_cast<const float*>(targets.genotype_likelihoods() + (size_t)s0 * M), n,
-                           result->dosage_data() + (size_t)s0 * M, result->posterior_data() + (size_t)s0 * M * 2,
-                           result->haplotype_data() + (size_t)s0 * 2 * M),
+                           result.dosage_data() + (size_t)s0 * M, result.posterior_data() + (size_t)s0 * M * 2,
+                           result.haplotype_data() + (size_t)s0 * 2 * M),
               "imputation");
-        if (progress_callback) progress_callback(s0 + n, B);
+        if (progress_callback) progress_callback(s0 + n - begin, B);
     }
-    result->compute_info_scores();
-    return result;
 }
 
 size_t Imputer::device_memory_usage() const {
@@ -618,6 +714,80 @@ size_t Imputer::estimate_memory_requirement(const ReferencePanel& reference, uin
     total += (size_t)num_target_samples * M * (1 + 4 + 8 + 2);               // codes in, dosage/P/haps out
     total += (size_t)num_target_samples * (M / 16 + 1) * lmax * 4;           // forward checkpoints
     return total;
+}
+
+// ---------------------------------------------------------------- MultiGPUImputer
+
+MultiGPUImputer::MultiGPUImputer(const ReferencePanel& reference, const std::vector<int>& device_ids,
+                                 const ImputationConfig& config)
+    : reference_(reference), config_(config), device_ids_(device_ids) {
+    if (device_ids_.empty()) throw ImputationError("MultiGPUImputer needs at least one device id");
+    for (int d : device_ids_) {
+        if (d < 0) throw ImputationError("device id " + std::to_string(d) + " is negative");
+        ImputationConfig c = config_;
+        c.device_id = d;
+        imputers_.push_back(std::make_unique<Imputer>(reference_, c));
+    }
+}
+
+MultiGPUImputer::~MultiGPUImputer() = default;
+
+namespace {
+
+// runs fn(i) for every replica on its own host thread; the first exception
+// (in replica order) is rethrown after all threads have joined
+template <class Fn>
+void on_every_replica(size_t n, Fn fn) {
+    std::vector<std::exception_ptr> errors(n);
+    std::vector<std::thread> threads;
+    threads.reserve(n);
+    for (size_t i = 0; i < n; ++i)
+        threads.emplace_back([&, i] {
+            try {
+                fn(i);
+            } catch (...) {
+                errors[i] = std::current_exception();
+            }
+        });
+    for (auto& t : threads) t.join();
+    for (auto& e : errors)
+        if (e) std::rethrow_exception(e);
+}
+
+}  // namespace
+
+void MultiGPUImputer::build_indices() {
+    on_every_replica(imputers_.size(), [&](size_t i) { imputers_[i]->build_index(); });
+}
+
+void MultiGPUImputer::partition_samples(uint32_t num_samples, std::vector<uint32_t>& start_indices,
+                                        std::vector<uint32_t>& end_indices) const {
+    const uint32_t g = (uint32_t)imputers_.size(), base = num_samples / g, extra = num_samples % g;
+    start_indices.clear();
+    end_indices.clear();
+    uint32_t s = 0;
+    for (uint32_t i = 0; i < g; ++i) {
+        const uint32_t n = base + (i < extra ? 1 : 0);
+        if (n == 0) continue;
+        start_indices.push_back(s);
+        end_indices.push_back(s + n);
+        s += n;
+    }
+}
+
+std::unique_ptr<ImputationResult> MultiGPUImputer::impute(const TargetData& targets) {
+    if (targets.num_markers() != reference_.num_markers())
+        throw ImputationError("Target and reference marker counts don't match: " +
+                              std::to_string(targets.num_markers()) + " vs " +
+                              std::to_string(reference_.num_markers()));
+    auto result = std::make_unique<ImputationResult>(targets.num_samples(), targets.num_markers());
+    std::vector<uint32_t> starts, ends;
+    partition_samples(targets.num_samples(), starts, ends);
+    on_every_replica(starts.size(), [&](size_t i) {
+        imputers_[i]->impute_rows(targets, starts[i], ends[i], *result, nullptr);
+    });
+    result->compute_info_scores();
+    return result;
 }
 
 // ---------------------------------------------------------------- convenience

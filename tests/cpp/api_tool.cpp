@@ -2,14 +2,18 @@
 // the way a caller of the reference would: load VCFs, build the index, impute,
 // write the VCF. Used by tests/test_cpp_api.py.
 //
-//   api_tool parse  <ref.vcf> <tgt.vcf> <prefix>     (no GPU) dump panel / GL, binary round trip
+//   api_tool parse  <ref.vcf> <tgt.vcf> <prefix>     (no GPU) dump panel / GL, binary round trips
 //   api_tool impute <ref.vcf> <tgt.vcf> <out.vcf> <prefix> <deterministic> <L> <ne> [posteriors]
+//   api_tool multi  <ref.vcf> <tgt.vcf> <devices> <prefix> <deterministic> <L> <ne>
+//                   MultiGPUImputer over a comma-separated device list (repeats allowed),
+//                   compared with one Imputer over all targets
 #include "swiftimpute/imputer.hpp"
 
 #include <cstdio>
 #include <cstring>
 #include <fstream>
 #include <iostream>
+#include <vector>
 
 using namespace swiftimpute;
 
@@ -37,6 +41,26 @@ int main(int argc, char** argv) {
                                           (size_t)ref->num_markers() * ref->num_haplotypes()) == 0 &&
                               back->markers()[1].pos == ref->markers()[1].pos &&
                               back->markers()[1].id == ref->markers()[1].id;
+            tgt->save_binary(pre + ".sitarget");
+            auto tback = TargetData::load_binary(pre + ".sitarget");
+            const bool tsame = tback->num_markers() == tgt->num_markers() &&
+                               tback->num_samples() == tgt->num_samples() &&
+                               std::memcmp(tback->genotype_likelihoods(), tgt->genotype_likelihoods(),
+                                           (size_t)tgt->num_samples() * tgt->num_markers() *
+                                               sizeof(GenotypeLikelihoods)) == 0 &&
+                               tback->samples().back().id == tgt->samples().back().id &&
+                               tback->markers().back().pos == tgt->markers().back().pos;
+            bool refused = false;  // each loader refuses the other's file
+            try {
+                ReferencePanel::load_binary(pre + ".sitarget");
+            } catch (const ImputationError&) {
+                refused = true;
+            }
+            try {
+                TargetData::load_binary(pre + ".sipanel");
+                refused = false;
+            } catch (const ImputationError&) {
+            }
             // a result written without a device: phased alleles from the panel's first two haplotypes
             ImputationResult r(tgt->num_samples(), tgt->num_markers());
             std::vector<allele_t> h(tgt->num_markers());
@@ -48,8 +72,48 @@ int main(int argc, char** argv) {
             r.compute_info_scores();
             ImputationConfig cfg;
             r.write_vcf(pre + ".out.vcf", *tgt, *ref, cfg);
-            std::printf("M=%u N=%u B=%u roundtrip=%d info0=%.4f\n", ref->num_markers(), ref->num_haplotypes(),
-                        tgt->num_samples(), same ? 1 : 0, r.get_info_score(0));
+            std::printf("M=%u N=%u B=%u roundtrip=%d target_roundtrip=%d refused=%d info0=%.4f\n",
+                        ref->num_markers(), ref->num_haplotypes(), tgt->num_samples(), same ? 1 : 0, tsame ? 1 : 0,
+                        refused ? 1 : 0, r.get_info_score(0));
+            return same && tsame && refused ? 0 : 3;
+        }
+        if (cmd == "multi") {
+            std::vector<int> devices;
+            for (const char* c = argv[4]; *c;) {
+                devices.push_back(std::atoi(c));
+                while (*c && *c != ',') ++c;
+                if (*c == ',') ++c;
+            }
+            ImputationConfig cfg;
+            cfg.deterministic = std::atoi(argv[6]) != 0;
+            cfg.hmm_params.num_states = (uint32_t)std::atoi(argv[7]);
+            cfg.hmm_params.ne = (uint32_t)std::atoi(argv[8]);
+            MultiGPUImputer multi(*ref, devices, cfg);
+            multi.build_indices();
+            auto res = multi.impute(*tgt);
+            Imputer one(*ref, cfg);
+            one.build_index();
+            auto want = one.impute(*tgt);
+            const size_t n = (size_t)res->num_samples() * res->num_markers();
+            bool same = std::memcmp(res->haplotype0(0), want->haplotype0(0), 2 * n) == 0;
+            for (sample_t s = 0; s < res->num_samples(); ++s)
+                for (marker_t m = 0; m < res->num_markers(); ++m) {
+                    prob_t a[3], b[3];
+                    res->get_probabilities(s, m, a);
+                    want->get_probabilities(s, m, b);
+                    same = same && std::memcmp(a, b, sizeof a) == 0 &&
+                           res->get_posterior_dosage(s, m) == want->get_posterior_dosage(s, m);
+                }
+            for (marker_t m = 0; m < res->num_markers(); ++m)
+                same = same && res->get_info_score(m) == want->get_info_score(m);
+            const std::string pre = argv[5];
+            std::vector<float> ds(n);
+            for (sample_t s = 0; s < res->num_samples(); ++s)
+                for (marker_t m = 0; m < res->num_markers(); ++m)
+                    ds[(size_t)s * res->num_markers() + m] = res->get_posterior_dosage(s, m);
+            dump(pre + ".dosage", ds.data(), n * 4);
+            dump(pre + ".haps", res->haplotype0(0), 2 * n);
+            std::printf("multi ok: replicas=%u identical=%d\n", multi.num_gpus(), same ? 1 : 0);
             return same ? 0 : 3;
         }
         if (cmd == "impute") {

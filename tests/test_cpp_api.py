@@ -14,6 +14,15 @@ from vcfutil import write_panel_vcf, write_target_vcf
 ROOT = Path(__file__).resolve().parent.parent
 
 
+def _has_device():
+    import ctypes
+    n = ctypes.c_int(0)
+    try:
+        return ctypes.CDLL("libcudart.so").cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0
+    except OSError:
+        return False
+
+
 @pytest.fixture(scope="module")
 def api_tool(tmp_path_factory):
     exe = tmp_path_factory.mktemp("bin") / "api_tool"
@@ -39,7 +48,10 @@ def test_vcf_parse_binary_roundtrip_and_writer(api_tool, vcfs):
     r = subprocess.run([str(api_tool), "parse", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "p")],
                        capture_output=True, text=True)
     assert r.returncode == 0, r.stdout + r.stderr
-    assert "roundtrip=1" in r.stdout
+    assert "roundtrip=1 target_roundtrip=1 refused=1" in r.stdout
+    # 2 bits per target cell: a header plus ceil(M/4) bytes per sample, against 12 B per cell in memory
+    B, M = codes.shape
+    assert (d / "p.sitarget").stat().st_size - B * ((M + 3) // 4) < 64 * M + 64 * B
     got_panel = np.fromfile(d / "p.panel", np.uint8).reshape(panel.shape)
     assert np.array_equal(got_panel, panel)
     gl = np.fromfile(d / "p.gl", np.float32).reshape(codes.shape + (3,))
@@ -54,14 +66,7 @@ def test_vcf_parse_binary_roundtrip_and_writer(api_tool, vcfs):
 
 
 def test_imputer_without_device_raises_cuda_error(api_tool, vcfs):
-    import ctypes
-    from swiftimpute_b200 import _native as N
-    n = ctypes.c_int(0)
-    try:
-        has_gpu = ctypes.CDLL("libcudart.so").cudaGetDeviceCount(ctypes.byref(n)) == 0 and n.value > 0
-    except OSError:
-        has_gpu = False
-    if has_gpu:
+    if _has_device():
         pytest.skip("a device is visible")
     d, *_ = vcfs
     r = subprocess.run([str(api_tool), "impute", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "o.vcf"),
@@ -97,6 +102,40 @@ def test_imputer_end_to_end(api_tool, vcfs, deterministic, posteriors):
     fmt = lines[9].split("\t")[8]
     assert fmt == ("GT:DS:GP" if posteriors else "GT")
     assert len(lines) == 9 + M
+
+
+def test_multi_gpu_imputer_refusals_without_device(api_tool, vcfs):
+    d, *_ = vcfs
+    args = [str(api_tool), "multi", str(d / "ref.vcf"), str(d / "tgt.vcf")]
+    r = subprocess.run(args + ["", str(d / "m"), "1", "8", "10000"], capture_output=True, text=True)
+    assert r.returncode == 11 and "at least one device" in r.stdout  # checked before any device call
+    r = subprocess.run(args + ["0,-1", str(d / "m"), "1", "8", "10000"], capture_output=True, text=True)
+    if _has_device():
+        assert r.returncode == 11 and "negative" in r.stdout
+    else:
+        assert r.returncode == 10 and "CUDAError" in r.stdout
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("devices,deterministic", [("0", 1), ("0,0,0", 1), ("0,0", 0)])
+def test_multi_gpu_imputer_replicas_match_one_imputer(api_tool, vcfs, devices, deterministic):
+    """MultiGPUImputer (src/api/imputer.hpp:298-328) as sample-sharded replicas:
+    repeated device ids give several replicas on the one device here; 17
+    targets split 6/6/5 (or 9/8) and the gathered result is bit-identical to one
+    Imputer, argmax and Philox sampling alike."""
+    d, panel, pos, codes = vcfs
+    r = subprocess.run([str(api_tool), "multi", str(d / "ref.vcf"), str(d / "tgt.vcf"), devices, str(d / "m"),
+                        str(deterministic), "8", "10000"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert f"replicas={len(devices.split(','))} identical=1" in r.stdout
+    B, M = codes.shape
+    pairs = oracle.select_pairs(oracle.pbwt_build(panel), 8)
+    want = oracle.fb_batch(codes, pairs, panel, pos, 8, 10000.0, sampled=not deterministic)
+    ds = np.fromfile(d / "m.dosage", np.float32).reshape(B, M)
+    assert np.abs(ds - want["dosage"]).max() <= 1e-4
+    if deterministic:
+        haps = np.fromfile(d / "m.haps", np.uint8).reshape(B, 2, M)
+        assert np.array_equal(haps, want["haps_argmax"])
 
 
 REF_MAIN = Path("/root/reference/src/main.cpp")
