@@ -31,6 +31,16 @@ def rng():
     return np.random.default_rng(1234)
 
 
+def r2_masked(got, want, codes) -> float:
+    """Squared Pearson correlation of two dosage arrays over the masked (untyped)
+    cells, where imputation happens; typed cells reproduce the call in both."""
+    m = np.asarray(codes) == 3
+    x, y = np.asarray(got, np.float64)[m], np.asarray(want, np.float64)[m]
+    if x.size < 2 or x.std() == 0 or y.std() == 0:
+        return 1.0 if np.array_equal(x, y) else 0.0
+    return float(np.corrcoef(x, y)[0, 1] ** 2)
+
+
 def report(name: str, **values) -> None:
     """Record measured parity figures of a test in $SI_REPORT_DIR/parity.json (when set)."""
     import json

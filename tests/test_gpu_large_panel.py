@@ -134,10 +134,12 @@ def test_all_targets_and_oracle_subset(engine, large):
     got_d = dos.index_select(0, idx).cpu().numpy()
     got_h = haps.index_select(0, idx).cpu().numpy()
     want = oracle.fb_batch(c_sub, cpairs, compact, pos, L, float(NE))
-    from conftest import report
+    from conftest import r2_masked, report
+    r2 = r2_masked(got_d, want["dosage"], c_sub)
     report("large panel 100,000 x 100,000, 512 targets", targets=512,
-           max_abs_dosage_diff=np.abs(got_d - want["dosage"]).max(),
+           max_abs_dosage_diff=np.abs(got_d - want["dosage"]).max(), dosage_r2_vs_oracle=r2,
            argmax_cells_differing=int((got_h != want["haps_argmax"]).sum()), cells=int(512 * M))
+    assert r2 >= 1 - 1e-6
     assert np.abs(got_d - want["dosage"]).max() <= 1e-4
     diff = (got_h != want["haps_argmax"]).any(axis=1)
     if diff.any():

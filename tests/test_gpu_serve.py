@@ -50,6 +50,34 @@ def _same(got, want):
         assert np.array_equal(got[key], want[key]), key
 
 
+def _against_oracle(panel, reqs, got):
+    """Served results (equal to the requests alone) against the FP64 oracle on
+    each request's slice; the panel's map is uniform, so both index origins
+    take the slice's own positions."""
+    import oracle
+    from conftest import r2_masked, report
+    pos = 1 + np.arange(panel.shape[0], dtype=np.uint64) * np.uint64(100)
+    full = {}
+    dd = dp = 0.0
+    gd, wd, cs = [], [], []
+    for q, g in zip(reqs, got):
+        sl = panel[q["m0"]:q["m1"]]
+        if q["origin"] == N.INDEX_REGION:
+            pairs = oracle.select_pairs(oracle.pbwt_build(sl), q["L"])
+        else:
+            if q["L"] not in full:
+                full[q["L"]] = oracle.select_pairs(oracle.pbwt_build(panel), q["L"])
+            pairs = full[q["L"]][q["m0"]:q["m1"]]
+        want = oracle.fb_batch(q["codes"], pairs, sl, pos[q["m0"]:q["m1"]], q["L"], 10000.0)
+        dd = max(dd, float(np.abs(g["dosage"] - want["dosage"]).max()))
+        dp = max(dp, float(np.abs(g["hap_prob"] - want["hap_prob"]).max()))
+        gd.append(g["dosage"].ravel()); wd.append(want["dosage"].ravel()); cs.append(q["codes"].ravel())
+    r2 = r2_masked(np.concatenate(gd), np.concatenate(wd), np.concatenate(cs))
+    report("serving requests, 24 mixed regions and L", targets=sum(q["codes"].shape[0] for q in reqs),
+           max_abs_dosage_diff=dd, max_abs_hap_prob_diff=dp, dosage_r2_vs_oracle=r2)
+    assert dd <= 1e-4 and dp <= 1e-4 and r2 >= 1 - 1e-6
+
+
 @pytest.mark.parametrize("sampling", [N.SAMPLE_ARGMAX, N.SAMPLE_PHILOX])
 def test_served_requests_equal_requests_alone(engine, sampling):
     panel = _setup(engine)
@@ -75,6 +103,8 @@ def test_served_requests_equal_requests_alone(engine, sampling):
         st = srv.stats()
     assert st["completed"] == len(reqs) and st["failed"] == 0
     assert st["cells"] == sum(q["codes"].size for q in reqs)
+    if sampling == N.SAMPLE_ARGMAX:
+        _against_oracle(panel, reqs, want)
     assert 1 <= st["batches"] < len(reqs)  # requests shared launches
     assert 0 < st["latency_p50_ms"] <= st["latency_p99_ms"] <= st["latency_max_ms"]
 

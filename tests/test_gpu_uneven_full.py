@@ -71,6 +71,7 @@ def test_full_shape_against_oracle_on_short_regions(workload):
     panel, pos, regions, jobs, out = workload
     short = sorted(range(64), key=lambda r: regions[r][1] - regions[r][0])[:3]
     worst, checked = 0.0, 0
+    gots, wants, masks = [], [], []
     for r in short:
         m0, m1, L, _ = regions[r]
         idx = [j for j, (rr, _, _) in enumerate(jobs) if rr == r][:4]
@@ -83,6 +84,9 @@ def test_full_shape_against_oracle_on_short_regions(workload):
         for b, j in enumerate(idx):
             worst = max(worst, float(np.abs(out[j]["dosage"] - want["dosage"][b]).max()))
             checked += 1
+            gots.append(out[j]["dosage"])
+            wants.append(want["dosage"][b])
+            masks.append(codes[b])
             assert np.abs(out[j]["dosage"] - want["dosage"][b]).max() <= TOL
             diff = out[j]["haps"] != want["haps_argmax"][b]
             if diff.any():
@@ -90,5 +94,7 @@ def test_full_shape_against_oracle_on_short_regions(workload):
                 hi = oracle.fb_batch(codes[b:b + 1], pairs, sl, pos[m0:m1], L, 10000.0, tie_eps=1e-4 + 1e-5)
                 flip = (lo["haps_argmax"][0] != want["haps_argmax"][b]) | (hi["haps_argmax"][0] != want["haps_argmax"][b])
                 assert not (diff & ~flip).any()
-    from conftest import report
-    report("uneven full shape, shortest regions", targets=checked, max_abs_dosage_diff=worst)
+    from conftest import r2_masked, report
+    r2 = r2_masked(np.concatenate(gots), np.concatenate(wants), np.concatenate(masks))
+    report("uneven full shape, shortest regions", targets=checked, max_abs_dosage_diff=worst, dosage_r2_vs_oracle=r2)
+    assert r2 >= 1 - 1e-6
