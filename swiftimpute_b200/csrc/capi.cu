@@ -371,6 +371,12 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
 namespace si {
 
 // Arguments of an uneven batch (si_impute_jobs_device, si_plan_create).
+bool region_first_gap_ok(const si_ctx* ctx, const si_impute_params* p, uint32_t m_begin, uint32_t m_end) {
+    if (m_end - m_begin < 2) return true;
+    const LinTrans t0 = lin_trans(ctx->morgans[m_begin], ctx->morgans[m_begin + 1], (double)p->ne, p->rho_rate);
+    return t0.c >= 1e-30f;
+}
+
 si_status check_jobs_args(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
                           const si_job* jobs, uint32_t n_jobs) {
     if (!ctx) return SI_ERR_INVALID_ARG;
@@ -481,13 +487,13 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
         } else {
             const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
             tr[r].masks = (const SlotMasks*)ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)].masks.ptr;
+            if (!region_first_gap_ok(ctx, p, g.m_begin, g.m_end))
+                return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
+                                                         ": zero genetic distance in its first gap");
             const LinTrans t0 = (g.m_end - g.m_begin >= 2)
                                     ? lin_trans(ctx->morgans[g.m_begin], ctx->morgans[g.m_begin + 1], (double)p->ne,
                                                 p->rho_rate)
                                     : LinTrans{1.f, 0.f};
-            if (g.m_end - g.m_begin >= 2 && !(t0.c >= 1e-30f))
-                return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
-                                                         ": zero genetic distance in its first gap");
             SI_TRY(tables_for(ctx, t0, L, &tr[r].tabs));
         }
     }

@@ -442,6 +442,18 @@ si_status si_serve_submit(si_server* S, const si_request* q, uint64_t* ticket) {
         (q->index_origin != SI_INDEX_GLOBAL && q->index_origin != SI_INDEX_REGION) ||
         (!q->dosage && !q->haps && !q->hap_prob))
         return SI_ERR_INVALID_ARG;
+    // what the launch would refuse for this request alone is refused here, so
+    // that it cannot fail the requests it would share a launch with
+    if (q->index_origin == SI_INDEX_GLOBAL) {
+        if (S->params.selection_kind == SI_SEL_FIRST_PAIRS) {
+            if ((uint64_t)2 * q->num_states > c->N) return SI_ERR_UNSUPPORTED;
+        } else if (!c->has_index) {
+            return SI_ERR_STATE;  // the global index is not built
+        }
+        if (!si::region_first_gap_ok(c, &S->params, 0, c->M)) return SI_ERR_UNSUPPORTED;
+    } else if (!si::region_first_gap_ok(c, &S->params, q->m_begin, q->m_end)) {
+        return SI_ERR_UNSUPPORTED;
+    }
     auto p = std::make_shared<Pending>();
     p->req = *q;
     const uint64_t cells = cells_of(*q);

@@ -124,6 +124,11 @@ void dev_free(si_ctx* ctx, DeviceBuffer& buf);
 si_status dev_reserve(si_ctx* ctx, DeviceBuffer& buf, size_t bytes);
 si_status fail(si_ctx* ctx, si_status s, const std::string& msg);
 si_status cuda_fail(si_ctx* ctx, cudaError_t e, const char* what);
+// Whether the first-gap transition of markers [m_begin, m_end) has a switch
+// weight the FP32 closed form can carry (false when the first two markers
+// share a genetic position). Reads only the ctx's map and writes nothing, so
+// threads other than the ctx's user may call it.
+bool region_first_gap_ok(const si_ctx* ctx, const si_impute_params* p, uint32_t m_begin, uint32_t m_end);
 
 // Kernel launchers (pbwt_kernels.cu, select_kernels.cu, fb_kernels.cu).
 cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,

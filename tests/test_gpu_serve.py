@@ -124,6 +124,30 @@ def test_request_alone_and_in_a_crowd(engine):
     _same(outs[5], alone)
 
 
+def test_submit_refuses_what_would_fail_a_shared_launch(engine):
+    """A region whose first two markers share a genetic position has no FP32
+    first-gap transition. Its request is refused at submission, since in a
+    launch it would fail the requests beside it; requests around it are served."""
+    panel, pos, _ = synth.make_panel(600, 200, 8, seed=93, spacing=100)
+    pos = pos.copy()
+    pos[301:] -= np.uint64(100)  # markers 300 and 301 share a position
+    engine.upload_panel(panel)
+    engine.set_map(pos)
+    engine.pbwt_build()
+    codes, _, _ = synth.make_targets(panel[300:400], 2, synth.typed_every(100, 5), seed=94)
+    with Server(engine, max_wait_us=2000) as srv:
+        with pytest.raises(N.SIError) as e:
+            srv.submit(300, 400, codes, num_states=8, index_origin=N.INDEX_REGION)
+        assert e.value.status == 4  # SI_ERR_UNSUPPORTED
+        ok = [srv.submit(299, 399, codes, num_states=8, index_origin=N.INDEX_REGION),
+              srv.submit(300, 400, codes, num_states=8, index_origin=N.INDEX_GLOBAL)]
+        for t in ok:
+            out = srv.wait(t)
+            assert np.isfinite(out["dosage"]).all()
+        st = srv.stats()
+    assert st["completed"] == 2 and st["failed"] == 0
+
+
 def test_admission_refuses_oversized_requests(engine):
     panel = _setup(engine, seed=92)
     q = _requests(panel, 1, seed=500)[0]
