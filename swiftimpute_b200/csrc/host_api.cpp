@@ -14,6 +14,7 @@
 #include <fstream>
 #include <iomanip>
 #include <iostream>
+#include <map>
 #include <mutex>
 #include <sstream>
 #include <thread>
@@ -722,10 +723,20 @@ MultiGPUImputer::MultiGPUImputer(const ReferencePanel& reference, const std::vec
                                  const ImputationConfig& config)
     : reference_(reference), config_(config), device_ids_(device_ids) {
     if (device_ids_.empty()) throw ImputationError("MultiGPUImputer needs at least one device id");
+    std::map<int, uint32_t> replicas_on;
+    for (int d : device_ids_) ++replicas_on[d];
     for (int d : device_ids_) {
         if (d < 0) throw ImputationError("device id " + std::to_string(d) + " is negative");
         ImputationConfig c = config_;
         c.device_id = d;
+        // replicas that share a device split its free memory, unless the config sets a budget
+        if (c.hbm_budget_bytes == 0 && replicas_on[d] > 1) {
+            size_t free_b = 0, total_b = 0;
+            if (cudaSetDevice(d) == cudaSuccess && cudaMemGetInfo(&free_b, &total_b) == cudaSuccess)
+                c.hbm_budget_bytes = free_b / replicas_on[d];
+            else
+                cudaGetLastError();
+        }
         imputers_.push_back(std::make_unique<Imputer>(reference_, c));
     }
 }
