@@ -196,6 +196,24 @@ def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds, gpu_dosage=None,
     return out, parity
 
 
+def pbwt_reference_time(panel):
+    """The reference's own PBWTBuilder::build (compiled from its sources into
+    oracle/_ref), single-threaded as the reference runs it, on the bench panel:
+    the CPU path the device sweep replaces. Never fails the bench line."""
+    import oracle
+    if not oracle.ref_pbwt_available():
+        return {"unavailable": "oracle/_ref/libref_pbwt.so is not built"}
+    try:
+        t0 = time.perf_counter()
+        oracle.ref_pbwt_build(panel)
+        dt = time.perf_counter() - t0
+    except Exception as e:  # noqa: BLE001 - reported in the line instead
+        return {"unavailable": f"{type(e).__name__}: {e}"}
+    M, N = panel.shape
+    return {"ms": dt * 1e3, "kind": "reference", "cores": 1,
+            "sample": f"PBWTBuilder::build over the whole {N} x {M} panel, prefix and divergence arrays copied out"}
+
+
 def run_reference(args, cfg):
     """Reference arm: the reference's recurrences on the host cores (rank 0)."""
     rank = int(os.environ.get("RANK", "0"))
@@ -474,6 +492,7 @@ def run_ours(args, cfg):
         pairs = eng.select_states(cfg["L"])
         line["cpu_baseline"], line["parity"] = cpu_baseline(panel, pos, codes, pairs, typed, cfg, args.cpu_seconds,
                                                             gpu_dosage=dos, gpu_haps=d_haps.cpu().numpy())
+        line["pbwt_cpu_reference"] = pbwt_reference_time(panel)
     eng.close()
     print(json.dumps(line), flush=True)
     if dist:
