@@ -55,3 +55,36 @@ def test_no_fallback_when_library_missing(monkeypatch, tmp_path):
     monkeypatch.setattr(N, "_lib", None)
     with pytest.raises(N.NativeLibraryError):
         N.load()
+
+
+MIRRORS = {"si_impute_params": "ImputeParams", "si_region": "Region", "si_job": "Job",
+           "si_serve_config": "ServeConfig", "si_request": "Request", "si_serve_statistics": "ServeStatistics"}
+
+
+def test_header_is_c99_and_ctypes_layouts_match(tmp_path):
+    """A cgo / JNI / ctypes binder parses the header as C: it must compile as
+    C99, and every struct's size and field offsets seen by the C compiler must
+    equal the Python mirrors' (a mismatch would corrupt arguments silently)."""
+    import ctypes
+    import subprocess
+    lines = ["#include <stddef.h>", "#include <stdio.h>", '#include "swiftimpute_b200.h"', "int main(void) {"]
+    for c_name, py_name in MIRRORS.items():
+        cls = getattr(N, py_name)
+        lines.append(f'printf("{c_name} size %zu\\n", sizeof({c_name}));')
+        for field, _ in cls._fields_:
+            lines.append(f'printf("{c_name} {field} %zu\\n", offsetof({c_name}, {field}));')
+    lines += ["return 0;", "}"]
+    src = tmp_path / "layout.c"
+    src.write_text("\n".join(lines) + "\n")
+    exe = tmp_path / "layout"
+    subprocess.run(["gcc", "-std=c99", "-Wall", "-Werror", "-pedantic", "-I", str(ROOT / "include"), str(src),
+                    "-o", str(exe)], check=True)
+    seen = {}
+    for line in subprocess.run([str(exe)], check=True, capture_output=True, text=True).stdout.splitlines():
+        struct, key, value = line.split()
+        seen[(struct, key)] = int(value)
+    for c_name, py_name in MIRRORS.items():
+        cls = getattr(N, py_name)
+        assert seen[(c_name, "size")] == ctypes.sizeof(cls), c_name
+        for field, _ in cls._fields_:
+            assert seen[(c_name, field)] == getattr(cls, field).offset, f"{c_name}.{field}"
