@@ -18,6 +18,20 @@ def _ptr(a: np.ndarray | None):
     return None if a is None else a.ctypes.data_as(c_void_p)
 
 
+def _job_layout(regions, jobs):
+    """Per-job code counts and offsets of an uneven batch. Every job's codes
+    must cover its region exactly: the device reads the region's length from
+    the job's offset, so a shorter array would be read past its end. Jobs of
+    an unknown region get length 0 (the C ABI refuses them)."""
+    lens = []
+    for i, (r, c, _) in enumerate(jobs):
+        n = max(0, regions[r][1] - regions[r][0]) if 0 <= r < len(regions) else 0
+        if np.asarray(c).size != n:
+            raise ValueError(f"job {i}: {np.asarray(c).size} codes for a region of {n} markers")
+        lens.append(n)
+    return lens, np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+
+
 class Engine:
     def __init__(self, device: int = 0, hbm_budget_bytes: int = 0):
         self.lib = N.load()
@@ -26,6 +40,7 @@ class Engine:
         if st != N.SI_OK:
             raise N.SIError(st, "si_ctx_create failed (is a CUDA device visible?)")
         self.h = h
+        self.device = device
         self.M = self.N = 0
 
     # -- plumbing -------------------------------------------------------------
@@ -109,6 +124,9 @@ class Engine:
         """
         params = params or N.default_params()
         geno = np.ascontiguousarray(geno, dtype=np.float32 if gl else np.uint8)
+        want = (self.M, 3) if gl else (self.M,)
+        if geno.ndim != 1 + len(want) or geno.shape[1:] != want:
+            raise ValueError(f"geno must have shape [B]{list(want)}, got {list(geno.shape)}")
         B = geno.shape[0]
         out = {}
         d = np.empty((B, self.M), np.float32) if dosage else None
@@ -142,13 +160,12 @@ class Engine:
         import torch
         params = params or N.default_params()
         R = (N.Region * len(regions))(*[N.Region(a, b, L, o) for a, b, L, o in regions])
-        lens = [max(0, regions[r][1] - regions[r][0]) if 0 <= r < len(regions) else 0 for r, _, _ in jobs]
-        offs = np.concatenate([[0], np.cumsum(lens)]).astype(np.int64)
+        lens, offs = _job_layout(regions, jobs)
         J = (N.Job * len(jobs))(*[N.Job(r, 0, int(offs[i]), int(offs[i]), int(sid))
                                   for i, (r, _, sid) in enumerate(jobs)])
         total = max(1, int(offs[-1]))
-        geno = np.concatenate([np.asarray(c, dtype=np.uint8) for _, c, _ in jobs] + [np.zeros(1, np.uint8)])
-        dev = torch.device("cuda", 0)
+        geno = np.concatenate([np.asarray(c, dtype=np.uint8).ravel() for _, c, _ in jobs] + [np.zeros(1, np.uint8)])
+        dev = torch.device("cuda", self.device)
         d_geno = torch.from_numpy(geno).to(dev)
         d_dos = torch.empty(total, dtype=torch.float32, device=dev)
         d_haps = torch.empty(2 * total, dtype=torch.uint8, device=dev)
@@ -287,10 +304,9 @@ class Plan:
         import torch
         self.engine, self.lib = engine, engine.lib
         self.regions = list(regions)
-        self.lens = [regions[r][1] - regions[r][0] for r, _, _ in jobs]
-        self.offs = np.concatenate([[0], np.cumsum(self.lens)]).astype(np.int64)
+        self.lens, self.offs = _job_layout(regions, jobs)
         total = max(1, int(self.offs[-1]))
-        dev = torch.device("cuda", 0)
+        dev = torch.device("cuda", engine.device)
         self.d_geno = torch.zeros(total, dtype=torch.uint8, device=dev)
         self.d_dos = torch.empty(total, dtype=torch.float32, device=dev)
         self.d_haps = torch.empty(2 * total, dtype=torch.uint8, device=dev)
@@ -309,7 +325,10 @@ class Plan:
 
     def set_codes(self, codes) -> None:
         import torch
-        flat = np.concatenate([np.asarray(c, dtype=np.uint8) for c in codes])
+        codes = [np.asarray(c, dtype=np.uint8).ravel() for c in codes]
+        if [c.size for c in codes] != list(self.lens):
+            raise ValueError("set_codes needs one code array per job, each as long as its region")
+        flat = np.concatenate(codes) if codes else np.zeros(0, np.uint8)
         self.d_geno[: flat.size].copy_(torch.from_numpy(flat))
         torch.cuda.synchronize(self.d_geno.device)
 
