@@ -163,6 +163,18 @@ def profile_traffic(kernel: str, config: str):
     return None
 
 
+def cpu_model() -> str:
+    """The host CPU's model name (Linux /proc/cpuinfo), for the baseline records."""
+    try:
+        with open("/proc/cpuinfo") as f:
+            for line in f:
+                if line.startswith("model name"):
+                    return line.split(":", 1)[1].strip()
+    except OSError:
+        pass
+    return "unknown"
+
+
 def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds, gpu_dosage=None, gpu_haps=None):
     """The FP64 port of the reference recurrences on all host threads, on the
     first S samples of the workload (S sized to ~`seconds` of CPU work). With
@@ -179,7 +191,8 @@ def cpu_baseline(panel, pos, codes, pairs, typed, cfg, seconds, gpu_dosage=None,
     want = oracle.fb_batch(codes[:S], pairs, panel, pos, cfg["L"], cfg["ne"], threads=threads)
     dt = time.perf_counter() - t0
     imputed = S * (M - len(typed))
-    out = {"value": imputed / dt, "unit": "imputed genotypes/s", "cores": threads, "kind": "port",
+    out = {"value": imputed / dt, "unit": "imputed genotypes/s", "cores": threads, "cpu_model": cpu_model(),
+           "kind": "port",
            "sample": f"first {S} of {codes.shape[0]} targets x {M} markers, FP64 log-space restatement of the "
                      f"reference recurrences, {dt:.1f} s"}
     parity = None
@@ -210,8 +223,14 @@ def pbwt_reference_time(panel):
     except Exception as e:  # noqa: BLE001 - reported in the line instead
         return {"unavailable": f"{type(e).__name__}: {e}"}
     M, N = panel.shape
-    return {"ms": dt * 1e3, "kind": "reference", "cores": 1,
+    return {"ms": dt * 1e3, "kind": "reference", "cores": 1, "cpu_model": cpu_model(),
             "sample": f"PBWTBuilder::build over the whole {N} x {M} panel, prefix and divergence arrays copied out"}
+
+
+def workload_name(config: str, cfg: dict, M: int, B: int, n_typed: int) -> str:
+    """The workload string both arms put in config.workload."""
+    return (f"{config}: {cfg['N']} haplotypes x {M} markers, {B} targets typed at {n_typed} markers, "
+            f"L={cfg['L']}, Ne={cfg['ne']}")
 
 
 def run_reference(args, cfg):
@@ -246,9 +265,10 @@ def run_reference(args, cfg):
         "impl": "reference", "metric": "imputed genotypes/s", "value": value, "unit": unit, "n_gpus": args.gpus,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f64", "data": "synthetic (seeded generator, config shape)",
-        "config": {"workload": args.config, "markers": M, "haplotypes": cfg["N"], "targets_per_step": S,
+        "config": {"workload": workload_name(args.config, cfg, M, codes.shape[0], len(typed)), "markers": M,
+                   "haplotypes": cfg["N"], "targets": codes.shape[0], "targets_per_step": S,
                    "typed_markers": int(len(typed)), "L": cfg["L"], "ne": cfg["ne"]},
-        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "kind": "port",
+        "cpu_baseline": {"value": value, "unit": unit, "cores": threads, "cpu_model": cpu_model(), "kind": "port",
                          "sample": f"{S} targets x {M} markers per step; the reference has no CPU forward-backward, "
                                    "so its recurrences run through the FP64 C port"},
         "e2e": {"value": value, "unit": unit, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
@@ -461,8 +481,7 @@ def run_ours(args, cfg):
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32",
         "data": "synthetic (seeded generator with the config's shape; the reference's dataset is unavailable)",
-        "config": {"workload": f"{args.config}: {cfg['N']} haplotypes x {M} markers, {B} targets typed at "
-                               f"{len(typed)} markers, L={cfg['L']}, Ne={cfg['ne']}",
+        "config": {"workload": workload_name(args.config, cfg, M, B, len(typed)),
                    "markers": M, "haplotypes": cfg["N"], "targets": B, "typed_markers": int(len(typed)),
                    "L": cfg["L"], "ne": cfg["ne"], "l2": "inputs (B*M bytes) larger than L2, no flush",
                    "parallelism": f"replicas x{world} (independent chains)"},
