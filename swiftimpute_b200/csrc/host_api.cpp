@@ -288,7 +288,8 @@ uint32_t get_u32(std::istream& in) {
 }
 std::string get_str(std::istream& in) {
     const uint32_t n = get_u32(in);
-    if (!in || n > (1u << 20)) throw ImputationError("corrupt string field in binary file");
+    if (!in) throw ImputationError("truncated binary file header");
+    if (n > (1u << 20)) throw ImputationError("corrupt string field in binary file");
     std::string s(n, '\0');
     in.read(&s[0], n);
     return s;
@@ -307,15 +308,31 @@ void put_meta(std::ostream& o, const std::vector<Marker>& markers, const std::ve
 }
 void get_meta(std::istream& in, uint32_t M, std::vector<Marker>& markers, std::vector<std::string>& names) {
     if (!in) throw ImputationError("truncated binary file header");
-    markers.resize(M);
-    for (auto& m : markers) {
+    // grown entry by entry: a damaged count fails at the end of the file, not in one huge allocation
+    markers.clear();
+    markers.reserve(std::min<uint32_t>(M, 1u << 16));
+    for (uint32_t i = 0; i < M; ++i) {
+        Marker m;
         m.chrom = get_str(in); m.id = get_str(in); m.ref = get_str(in); m.alt = get_str(in);
         in.read(reinterpret_cast<char*>(&m.pos), 8);
         in.read(reinterpret_cast<char*>(&m.cM), 8);
+        markers.push_back(std::move(m));
     }
-    names.resize(get_u32(in));
-    for (auto& s : names) s = get_str(in);
+    const uint32_t n_names = get_u32(in);
+    names.clear();
+    names.reserve(std::min<uint32_t>(n_names, 1u << 16));
+    for (uint32_t i = 0; i < n_names && in; ++i) names.push_back(get_str(in));
     if (!in) throw ImputationError("truncated binary file header");
+}
+
+// the body that follows the header must be there before it is allocated
+void check_body(std::istream& in, uint64_t rows, uint64_t row_bytes, const char* what, const std::string& filename) {
+    const std::streampos here = in.tellg();
+    in.seekg(0, std::ios::end);
+    const std::streampos end = in.tellg();
+    in.seekg(here);
+    if (here < 0 || end < here || (uint64_t)(end - here) < rows * row_bytes)
+        throw ImputationError(std::string("truncated ") + what + ": " + filename);
 }
 
 void check_magic(std::istream& in, const char* magic, const char* what, const std::string& filename) {
@@ -359,6 +376,7 @@ std::unique_ptr<ReferencePanel> ReferencePanel::load_binary(const std::string& f
     std::vector<std::string> names;
     get_meta(in, M, ms, names);
     const size_t rb = (N + 7) / 8;
+    check_body(in, M, rb, "binary panel", filename);
     auto h = std::make_unique<allele_t[]>((size_t)M * N);
     std::vector<unsigned char> row(rb);
     for (uint32_t m = 0; m < M; ++m) {
@@ -459,6 +477,7 @@ std::unique_ptr<TargetData> TargetData::load_binary(const std::string& filename)
     std::vector<std::string> names;
     get_meta(in, n_markers, ms, names);
     const size_t M = ms.size(), B = names.size(), rb = (M + 3) / 4;
+    check_body(in, B, rb, "binary target file", filename);
     std::vector<uint8_t> codes(B * M);
     std::vector<unsigned char> row(rb);
     for (size_t s = 0; s < B; ++s) {

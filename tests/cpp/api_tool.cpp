@@ -4,6 +4,7 @@
 //
 //   api_tool parse  <ref.vcf> <tgt.vcf> <prefix>     (no GPU) dump panel / GL, binary round trips
 //   api_tool impute <ref.vcf> <tgt.vcf> <out.vcf> <prefix> <deterministic> <L> <ne> [posteriors]
+//   api_tool loadbin <panel|target> <file>           (no GPU) load a binary file, print its shape
 //   api_tool multi  <ref.vcf> <tgt.vcf> <devices> <prefix> <deterministic> <L> <ne>
 //                   MultiGPUImputer over a comma-separated device list (repeats allowed),
 //                   compared with one Imputer over all targets
@@ -23,6 +24,24 @@ static void dump(const std::string& path, const void* p, size_t n) {
 }
 
 int main(int argc, char** argv) {
+    if (argc == 4 && std::string(argv[1]) == "loadbin") {
+        try {
+            if (std::string(argv[2]) == "panel") {
+                auto p = ReferencePanel::load_binary(argv[3]);
+                std::printf("panel M=%u N=%u\n", p->num_markers(), p->num_haplotypes());
+            } else {
+                auto t = TargetData::load_binary(argv[3]);
+                std::printf("target M=%u B=%u\n", t->num_markers(), t->num_samples());
+            }
+            return 0;
+        } catch (const ImputationError& e) {
+            std::printf("ImputationError: %s\n", e.what());
+            return 11;
+        } catch (const std::exception& e) {
+            std::printf("error: %s\n", e.what());
+            return 12;
+        }
+    }
     if (argc < 5) return 2;
     const std::string cmd = argv[1];
     try {

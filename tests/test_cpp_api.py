@@ -65,6 +65,30 @@ def test_vcf_parse_binary_roundtrip_and_writer(api_tool, vcfs):
     assert len(lines) == 9 + panel.shape[0]
 
 
+def test_binary_loaders_refuse_damaged_files(api_tool, vcfs):
+    d, panel, pos, codes = vcfs
+    r = subprocess.run([str(api_tool), "parse", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "b")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    for kind, name, shape in (("panel", "b.sipanel", f"M={panel.shape[0]} N={panel.shape[1]}"),
+                              ("target", "b.sitarget", f"M={codes.shape[1]} B={codes.shape[0]}")):
+        whole = (d / name).read_bytes()
+        ok = subprocess.run([str(api_tool), "loadbin", kind, str(d / name)], capture_output=True, text=True)
+        assert ok.returncode == 0 and shape in ok.stdout
+        for cut, words in ((len(whole) - 1, "truncated"), (len(whole) // 3, "truncated"), (6, "not a")):
+            (d / "damaged").write_bytes(whole[:cut])
+            r = subprocess.run([str(api_tool), "loadbin", kind, str(d / "damaged")], capture_output=True, text=True)
+            assert r.returncode == 11 and words in r.stdout, (kind, cut, r.stdout)
+        # a damaged count in the header (haplotypes of a panel, markers of a target file): refused
+        # before anything of that size is allocated
+        bad = bytearray(whole)
+        at = 12 if kind == "panel" else 8
+        bad[at:at + 4] = b"\xff\xff\xff\x7f"
+        (d / "damaged").write_bytes(bytes(bad))
+        r = subprocess.run([str(api_tool), "loadbin", kind, str(d / "damaged")], capture_output=True, text=True)
+        assert r.returncode == 11 and ("truncated" in r.stdout or "corrupt" in r.stdout), (kind, r.stdout)
+
+
 def test_imputer_without_device_raises_cuda_error(api_tool, vcfs):
     if _has_device():
         pytest.skip("a device is visible")
