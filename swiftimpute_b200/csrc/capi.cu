@@ -687,6 +687,7 @@ si_status si_panel_set_map(si_ctx* ctx, const uint64_t* pos, const double* cM) {
 }
 
 si_status si_pbwt_build(si_ctx* ctx, uint32_t flags) {
+    Range range("si_pbwt_build");
     if (!ctx) return SI_ERR_INVALID_ARG;
     if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
     SI_TRY(set_device(ctx));
@@ -750,6 +751,7 @@ si_status si_pbwt_last_ms(const si_ctx* ctx, float* ms) {
 }
 
 si_status si_select_states(si_ctx* ctx, uint32_t L, int32_t kind, uint32_t m0, uint32_t m1, uint32_t* out_pairs) {
+    Range range("si_select_states");
     if (!ctx) return SI_ERR_INVALID_ARG;
     if (!out_pairs || m0 > m1 || m1 > ctx->M) return fail(ctx, SI_ERR_INVALID_ARG, "bad marker range");
     SI_TRY(set_device(ctx));
@@ -780,6 +782,7 @@ si_status si_impute_params_default(si_impute_params* p) {
 
 si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
                            float* d_dosage, float* d_hprob, uint8_t* d_haps, void* stream) {
+    Range range("si_impute_device");
     if (!ctx) return SI_ERR_INVALID_ARG;
     SI_TRY(check_params(ctx, p));
     if (!d_geno || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "geno is NULL or B == 0");
@@ -791,6 +794,7 @@ si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t
 
 si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno, uint32_t B, float* dosage,
                     float* hap_prob, uint8_t* haps) {
+    Range range("si_impute");
     if (!ctx) return SI_ERR_INVALID_ARG;
     SI_TRY(check_params(ctx, p));
     if (!geno || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "geno is NULL or B == 0");
@@ -907,6 +911,7 @@ si_status si_last_timings(si_ctx* ctx, float* ms3) {
 si_status si_impute_jobs_device(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
                                 const si_job* jobs, uint32_t n_jobs, const uint8_t* d_geno, float* d_dosage,
                                 float* d_hap_prob, uint8_t* d_haps, void* stream) {
+    Range range("si_impute_jobs_device");
     if (!ctx) return SI_ERR_INVALID_ARG;
     SI_TRY(check_jobs_args(ctx, p, regions, n_regions, jobs, n_jobs));
     if (!d_geno) return fail(ctx, SI_ERR_INVALID_ARG, "NULL genotype buffer");

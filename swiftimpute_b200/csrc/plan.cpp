@@ -93,6 +93,7 @@ extern "C" {
 si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,
                          const si_job* jobs, uint32_t n_jobs, uint32_t max_anchors, const uint8_t* d_geno,
                          float* d_dosage, float* d_hap_prob, uint8_t* d_haps, uint32_t flags, si_plan** out) {
+    si::Range range("si_plan_create");
     if (!ctx || !out) return SI_ERR_INVALID_ARG;
     si_status st = si::check_jobs_args(ctx, p, regions, n_regions, jobs, n_jobs);
     if (st != SI_OK) return st;
@@ -237,6 +238,7 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
 }
 
 si_status si_plan_launch(si_plan* P, void* stream) {
+    si::Range range("si_plan_launch");
     if (!P) return SI_ERR_INVALID_ARG;
     cudaError_t e = cudaSetDevice(P->ctx->device);
     if (e == cudaSuccess) e = enqueue(P, stream ? (cudaStream_t)stream : P->ctx->stream);
@@ -244,6 +246,7 @@ si_status si_plan_launch(si_plan* P, void* stream) {
 }
 
 si_status si_plan_graph_launch(si_plan* P, void* stream) {
+    si::Range range("si_plan_graph_launch");
     if (!P) return SI_ERR_INVALID_ARG;
     cudaError_t e = cudaSetDevice(P->ctx->device);
     if (e != cudaSuccess) return si::cuda_fail(P->ctx, e, "cudaSetDevice");

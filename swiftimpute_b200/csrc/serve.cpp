@@ -201,6 +201,7 @@ void trim_region_cache(si_server* S) {
 // Device stage of a launch into slot k: gather codes, copy in, impute, queue
 // the output copies and the event that marks them done.
 si_status launch_batch(si_server* S, int k) {
+    si::Range range("serve launch");
     si_ctx* ctx = S->ctx;
     auto& z = S->slot[k];
     const auto& batch = z.batch;
@@ -264,6 +265,7 @@ si_status launch_batch(si_server* S, int k) {
 // Host stage: wait for slot k's copies, scatter into the requests' buffers (a
 // request's jobs are consecutive, so each output is one contiguous block).
 si_status complete_batch(si_server* S, int k) {
+    si::Range range("serve complete");
     auto& z = S->slot[k];
     if (z.status != SI_OK) return z.status;
     const cudaError_t e = cudaEventSynchronize(z.copied);

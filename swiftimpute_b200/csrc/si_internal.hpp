@@ -4,6 +4,7 @@
 #include "../../include/swiftimpute_b200.h"
 
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <cstdint>
 #include <map>
@@ -13,6 +14,15 @@
 #include <vector>
 
 namespace si {
+
+// A named host range for profiler timelines (NVTX, header-only); without an
+// attached tool each push and pop is a few nanoseconds.
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
 
 // Bit-packed panel row: ceil(N / 32) words, padded to a multiple of 4 so every
 // row starts on a 16-byte boundary (128-bit loads, bulk copies).
