@@ -176,22 +176,30 @@ si_status si_impute_gl(si_ctx* ctx, const si_impute_params* p, const float* gl, 
 si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
                            float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
 
-/* Allocation-free variant of si_impute_device for callers that cannot call
- * cudaMalloc while they impute: code inside CUDA stream capture, where an
- * allocation synchronises the device and breaks the capture, and programs
- * whose device memory belongs to another allocator (a framework's pool). It
- * has no counterpart in the reference. The caller passes device inputs and
- * outputs; the forward checkpoints live in a fixed 16 MiB array inside the
- * library (held by every GPU that loads it, until exit). Needs B * ceil(M/C - 1)
- * * Lmax * 4 bytes of checkpoints (C = 32 markers, 16 for L > 16; Lmax = L
- * rounded up to 4/8/16/32) within that limit, else SI_ERR_UNSUPPORTED. The
- * ctx must hold the slot and transition tables for these parameters: make one
+/* Allocation-free variant of si_impute_device. It has no counterpart in the
+ * reference. It is for callers that cannot call cudaMalloc while they impute:
+ * programs whose device memory belongs to another allocator (a framework's
+ * pool that reserves the free memory and forbids raw allocations beside it),
+ * and latency-bound programs that share the device with other streams, where
+ * cudaMalloc/cudaFree may synchronise the device. The caller passes device
+ * inputs and outputs; the forward checkpoints live in a fixed 16 MiB array
+ * inside the library (held by every GPU that loads it, until exit).
+ * It always runs the marker-by-marker (full-chain) recursion, whatever the
+ * transition mode; flags other than SI_IMPUTE_FULL_CHAIN are refused. Results
+ * agree with si_impute_device within the parity tolerance (1e-4 in dosage),
+ * not bit for bit, where that call takes the typed-marker path.
+ * Checkpoint bytes: max(ceil(M / C) - 1, 1) * Lmax * B * 4, with C =
+ * checkpoint_interval or 32 markers (16 for L > 16) and Lmax = L rounded up to
+ * 4/8/16/32; more than 16 MiB is refused with SI_ERR_UNSUPPORTED. The ctx must
+ * hold the slot and transition tables for these parameters: make one
  * allocating call (si_impute or si_impute_device) with them first, and let it
- * complete. Its first call on a device is its set-up: it looks up the
- * array's device address (with lazy module loading, that is also when the
- * driver commits the array's memory); make that call before any stream
- * capture. Calls share the array, so calls
- * whose kernels overlap on the GPU race; serialise them on one stream. */
+ * complete. The first call on a ctx is its set-up: it looks up the array's
+ * device address (with lazy module loading, that is also when the driver
+ * commits the array's memory); make that call before any stream capture.
+ * After a device reset, create a new ctx. Calls share the array, so calls
+ * whose kernels overlap on the GPU race; serialise them on one stream.
+ * si_last_timings / si_last_kernel_ms do not cover this entry point: after it
+ * they still report the last allocating call. */
 si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B,
                                    float* d_dosage, float* d_hap_prob, uint8_t* d_haps, void* stream);
 

@@ -22,6 +22,11 @@ ORACLE_SO = HERE / "_build" / "libsi_oracle.so"
 REF_PBWT_SO = HERE / "_ref" / "libref_pbwt.so"
 REF_GPU_SO = HERE / "_ref" / "libref_gpu.so"
 
+# Where the reference's source tree lies when it is present (the oracle/_ref
+# builds, the golden-vector generator and the drop-in compile test read it);
+# SI_REFERENCE_TREE overrides. Absent on machines that only run the prebuilt files.
+REFERENCE_TREE = Path(os.environ.get("SI_REFERENCE_TREE", "/root/reference"))
+
 SEL_AUTO, SEL_WARP, SEL_INSERTION, SEL_FIRST_PAIRS = 0, 1, 2, 3
 TRANS_MATRIX0, TRANS_PER_GAP = 0, 1
 
@@ -32,7 +37,7 @@ class FbArgs(ctypes.Structure):
 
 
 def build(target: str = "oracle") -> None:
-    subprocess.run(["make", "-s", "-C", str(HERE), target], check=True)
+    subprocess.run(["make", "-s", "-C", str(HERE), target, f"REF={REFERENCE_TREE}"], check=True)
 
 
 _lib = None

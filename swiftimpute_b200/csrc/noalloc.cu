@@ -1,49 +1,46 @@
 // noalloc.cu — imputation entry point that performs no device allocation.
 //
-// For callers that cannot call cudaMalloc at the point where they impute:
-// code running inside CUDA stream capture (a cudaMalloc there synchronises
-// the device and invalidates the capture), or a host program whose device
-// memory is owned by another allocator (a framework's memory pool) that
-// forbids raw allocations on its hot path. The caller allocates inputs and
-// outputs; the forward checkpoints, the only scratch this path needs, live in
-// a fixed array compiled into the library.
+// For callers that cannot call cudaMalloc at the point where they impute: a
+// host program whose device memory is owned by another allocator (a
+// framework's memory pool that reserves the free memory up front and forbids
+// raw allocations beside it), and latency-bound callers that share the device
+// with other streams (cudaMalloc and cudaFree may synchronise the device, which
+// stalls the other streams' work). The caller allocates inputs and outputs;
+// the forward checkpoints, the only scratch this path needs, live in a fixed
+// array compiled into the library.
 //
 // The array below is a file-scope __device__ variable: every GPU that loads
 // this library holds kNoAllocScratchBytes of it until the process exits. In
 // host code its name is only a host-side stand-in, so its device address is
-// looked up once per device with cudaGetSymbolAddress (with that device
-// current) and cached. All calls share the array: a call leaves its
+// looked up with cudaGetSymbolAddress (with the ctx's device current) by the
+// first call on a ctx, and kept in the ctx. A ctx lives in one CUDA context:
+// after a device reset the caller creates a new ctx, whose first call looks
+// the address up again. All calls share the array: a call leaves its
 // checkpoints there, and calls whose kernels overlap on the GPU (different
 // streams, or different host threads) race on it. Checkpoints are written
 // before they are read within a call, so nothing needs clearing.
 #include "si_internal.hpp"
 
 #include <cstring>
-#include <mutex>
 #include <string>
 
 namespace si {
 namespace {
 
 constexpr size_t kNoAllocScratchBytes = 16u << 20;  // 16 MiB of forward checkpoints
-constexpr int kMaxDevices = 64;
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
-std::mutex g_addr_mu;
-void* g_addr[kMaxDevices] = {};
-
-// Device address of the scratch array on the current device, resolved once.
-cudaError_t scratch_address(int device, void** out) {
-    std::lock_guard<std::mutex> lock(g_addr_mu);
-    if (device < 0 || device >= kMaxDevices) return cudaErrorInvalidDevice;
-    if (!g_addr[device]) {
+// Device address of the scratch array, looked up by the ctx's first call (its
+// device is current) and kept in the ctx.
+cudaError_t scratch_address(si_ctx* ctx, void** out) {
+    if (!ctx->noalloc_scratch) {
         void* p = nullptr;
         const cudaError_t e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
         if (e != cudaSuccess) return e;
-        g_addr[device] = p;
+        ctx->noalloc_scratch = p;
     }
-    *out = g_addr[device];
+    *out = ctx->noalloc_scratch;
     return cudaSuccess;
 }
 
@@ -73,6 +70,8 @@ extern "C" si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_param
     if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
     if (p->flags & SI_IMPUTE_RESELECT)
         return fail(ctx, SI_ERR_INVALID_ARG, "SI_IMPUTE_RESELECT is not available without allocation");
+    // this entry point always runs the full-chain recursion; SI_IMPUTE_FULL_CHAIN is accepted
+    if (p->flags & ~(uint32_t)SI_IMPUTE_FULL_CHAIN) return fail(ctx, SI_ERR_INVALID_ARG, "unknown flag bits");
     // set-up state must already exist: an earlier allocating call with the same
     // parameters built the slot table and the transition table
     const uint32_t L = p->num_states;
@@ -97,7 +96,7 @@ extern "C" si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_param
     cudaError_t e = cudaSetDevice(ctx->device);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaSetDevice");
     void* scratch = nullptr;
-    e = scratch_address(ctx->device, &scratch);
+    e = scratch_address(ctx, &scratch);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "cudaGetSymbolAddress");
     FbLaunch l;
     l.geno = d_geno;

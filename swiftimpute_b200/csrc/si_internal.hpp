@@ -122,6 +122,7 @@ struct si_ctx {
     si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
     float last_ms[3] = {0.f, 0.f, 0.f};
     bool timings_pending = false;
+    void* noalloc_scratch = nullptr;  // device address of the allocation-free path's fixed array
 };
 
 namespace si {

@@ -28,7 +28,7 @@ sys.path.insert(0, str(ROOT))
 import oracle  # noqa: E402
 from swiftimpute_b200 import synth  # noqa: E402
 
-REF_TREE = Path("/root/reference")
+REF_TREE = oracle.REFERENCE_TREE
 
 
 def parse_vcf_panel(path: Path) -> np.ndarray:

@@ -162,7 +162,7 @@ def test_multi_gpu_imputer_replicas_match_one_imputer(api_tool, vcfs, devices, d
         assert np.array_equal(haps, want["haps_argmax"])
 
 
-REF_MAIN = Path("/root/reference/src/main.cpp")
+REF_MAIN = oracle.REFERENCE_TREE / "src" / "main.cpp"
 
 
 @pytest.mark.skipif(not REF_MAIN.exists(), reason="reference source tree not present")
