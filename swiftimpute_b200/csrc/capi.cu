@@ -85,9 +85,13 @@ void reset_index(si_ctx* ctx) {
     for (auto& kv : ctx->sel) {
         dev_free(ctx, kv.second.pairs);
         dev_free(ctx, kv.second.masks);
+        dev_free(ctx, kv.second.g);
     }
     ctx->sel.clear();
-    for (auto& kv : ctx->region_sel) dev_free(ctx, kv.second.masks);
+    for (auto& kv : ctx->region_sel) {
+        dev_free(ctx, kv.second.masks);
+        dev_free(ctx, kv.second.g);
+    }
     ctx->region_sel.clear();
     ctx->has_index = false;
     ctx->pbwt_flags = 0;
@@ -162,10 +166,12 @@ si_status ensure_selection(si_ctx* ctx, uint32_t L, int kind, SelectionCache** o
         if (!c.pairs.ptr) {
             SI_TRY(dev_alloc(ctx, c.pairs, (size_t)ctx->M * L * 2 * sizeof(uint32_t)));
             SI_TRY(dev_alloc(ctx, c.masks, (size_t)ctx->M * sizeof(SlotMasks)));
+            SI_TRY(dev_alloc(ctx, c.g, (size_t)ctx->M * fb_lmax(L) * sizeof(float)));
         }
         SI_CUDA(ctx,
                 launch_select((const uint32_t*)ctx->head.ptr, (const uint32_t*)ctx->panel.ptr, ctx->M, ctx->N, ctx->W,
-                              L, kind, (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, s ? s : ctx->stream),
+                              L, kind, (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, (float*)c.g.ptr, fb_lmax(L),
+                              s ? s : ctx->stream),
                 "select kernel");
     }
     *out = &c;
@@ -250,7 +256,7 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
 
 // The typed-marker pipeline once the per-sample views are set in `a`
 // (geno, B, M, regions/samples or reg0, sampling, outputs): anchor lists,
-// chain, posterior. Waits once on `s` for the 16-byte list totals.
+// chain, posterior. Waits once on `s` for the list totals.
 si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32_t lmax, bool all_full,
                     cudaStream_t s) {
     a.C = p->checkpoint_interval ? p->checkpoint_interval : typed_default_window(lmax);
@@ -258,12 +264,13 @@ si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32
     if (typed_post_smem_bytes(lmax, a.threads, a.C) > 227u * 1024u)
         return fail(ctx, SI_ERR_UNSUPPORTED, "posterior tile needs more than 227 KB of shared memory");
     if (!ctx->pinned_totals) {
-        SI_CUDA(ctx, cudaHostAlloc(&ctx->pinned_totals, 2 * sizeof(unsigned long long), cudaHostAllocMapped),
+        SI_CUDA(ctx, cudaHostAlloc(&ctx->pinned_totals, 4 * sizeof(unsigned long long), cudaHostAllocMapped),
                 "pinned totals");
         SI_CUDA(ctx, cudaHostGetDevicePointer(&ctx->pinned_totals_dev, ctx->pinned_totals, 0), "pinned totals");
     }
     if (!ctx->totals_ev) SI_CUDA(ctx, cudaEventCreateWithFlags(&ctx->totals_ev, cudaEventDisableTiming), "event");
     a.host_totals = ctx->pinned_totals_dev;
+    a.K = kPostGroup;
     const uint32_t B = a.B;
     SI_TRY(dev_reserve(ctx, ctx->t_counts, (size_t)B * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_aoff, ((size_t)B + 1) * 8));
@@ -276,17 +283,16 @@ si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32
     SI_CUDA(ctx, cudaEventSynchronize(ctx->totals_ev), "anchor count");
     const volatile unsigned long long* tot = ctx->pinned_totals;
     const unsigned long long NA = tot[0], NW = tot[1];
+    a.max_windows = (uint32_t)tot[2];
     SI_TRY(dev_reserve(ctx, ctx->t_apos, (size_t)NA * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_aem, (size_t)NA * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_acode, (size_t)NA));
-    SI_TRY(dev_reserve(ctx, ctx->t_wsample, (size_t)NW * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_ckF, (size_t)NW * lmax * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_ckB, (size_t)NW * lmax * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_ckU, (size_t)NW * 8));
     a.apos = (uint32_t*)ctx->t_apos.ptr;
     a.aem = (uint32_t*)ctx->t_aem.ptr;
     a.ashift = (uint8_t*)ctx->t_acode.ptr;
-    a.wsample = (uint32_t*)ctx->t_wsample.ptr;
     a.total_windows = NW;
     a.ckptF = (float*)ctx->t_ckF.ptr;
     a.ckptB = (float*)ctx->t_ckB.ptr;
@@ -311,6 +317,8 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
     a.seed = p->seed;
     a.sid_base = p->sample_id_base;
     a.reg0.masks = (const SlotMasks*)sel->masks.ptr;
+    a.reg0.g = (const float*)sel->g.ptr;
+    a.reg0.gs = fb_lmax(p->num_states);
     a.reg0.L = p->num_states;
     SI_TRY(tables_for(ctx, ctx->trans0, p->num_states, &a.reg0.tabs));
     a.dosage = d_dosage;
@@ -463,10 +471,15 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             if (j == sweeps.size()) continue;  // cached already under another slot count? swept above
             auto& rs = ctx->region_sel[key];
             st = dev_alloc(ctx, rs.masks, (size_t)(g.m_end - g.m_begin) * sizeof(SlotMasks));
-            if (st != SI_OK) { ctx->region_sel.erase(key); break; }
+            if (st == SI_OK) st = dev_alloc(ctx, rs.g, (size_t)(g.m_end - g.m_begin) * fb_lmax(L) * sizeof(float));
+            if (st != SI_OK) {
+                dev_free(ctx, rs.masks);
+                ctx->region_sel.erase(key);
+                break;
+            }
             e = launch_select((const uint32_t*)head.ptr + sweeps[j].head_off,
                               (const uint32_t*)ctx->panel.ptr + (size_t)g.m_begin * W, g.m_end - g.m_begin, N, W, L,
-                              kind, nullptr, (SlotMasks*)rs.masks.ptr, s);
+                              kind, nullptr, (SlotMasks*)rs.masks.ptr, (float*)rs.g.ptr, fb_lmax(L), s);
         }
         if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);  // scratch reuse below
         dev_free(ctx, head);
@@ -483,10 +496,15 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             SelectionCache* sel = nullptr;
             SI_TRY(ensure_selection(ctx, L, p->selection_kind, &sel, false, s));
             tr[r].masks = (const SlotMasks*)sel->masks.ptr + g.m_begin;
+            tr[r].g = (const float*)sel->g.ptr + (size_t)g.m_begin * fb_lmax(L);
+            tr[r].gs = fb_lmax(L);
             SI_TRY(tables_for(ctx, ctx->trans0, L, &tr[r].tabs));
         } else {
             const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
-            tr[r].masks = (const SlotMasks*)ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)].masks.ptr;
+            const auto& rs = ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)];
+            tr[r].masks = (const SlotMasks*)rs.masks.ptr;
+            tr[r].g = (const float*)rs.g.ptr;
+            tr[r].gs = fb_lmax(L);
             if (!region_first_gap_ok(ctx, p, g.m_begin, g.m_end))
                 return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
                                                          ": zero genetic distance in its first gap");
@@ -568,14 +586,17 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     dev_free(ctx, ctx->io_hprob);
     dev_free(ctx, ctx->io_haps);
     for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_acode, &ctx->t_aem,
-                                &ctx->t_wsample, &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->job_regions,
+                                &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->job_regions,
                                 &ctx->job_samples})
         dev_free(ctx, *b);
     for (auto& kv : ctx->tables) {
         dev_free(ctx, kv.second.QS);
         dev_free(ctx, kv.second.G);
     }
-    for (auto& kv : ctx->region_sel) dev_free(ctx, kv.second.masks);
+    for (auto& kv : ctx->region_sel) {
+        dev_free(ctx, kv.second.masks);
+        dev_free(ctx, kv.second.g);
+    }
     if (ctx->pinned_totals) cudaFreeHost(ctx->pinned_totals);
     if (ctx->totals_ev) cudaEventDestroy(ctx->totals_ev);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);

@@ -18,10 +18,13 @@ struct TypedTables {
     int regime;  // 0: rho < 1, 1: rho > 1, 2: rho == 1
 };
 
-// A panel slice imputed with L slots: its slot masks (index 0 = the slice's
-// first marker) and the closed-form tables of its transition.
+// A panel slice imputed with L slots: its slot masks and per-slot ALT counts
+// g [marker][gs] (index 0 = the slice's first marker), and the closed-form
+// tables of its transition.
 struct TypedRegion {
     const SlotMasks* masks;
+    const float* g;
+    uint32_t gs;
     uint32_t L;
     TypedTables tabs;
 };
@@ -41,7 +44,9 @@ struct TypedArgs {
     const uint8_t* geno;
     uint32_t B;                      // samples
     uint32_t M;                      // markers per sample of a plain batch
-    uint32_t C, threads;
+    uint32_t C, threads;             // anchors per window (backward checkpoints), posterior CTA size
+    uint32_t K;                      // windows per posterior group (forward checkpoints every K windows)
+    uint32_t max_windows;            // most windows of any sample (posterior grid)
     int sampling;
     float tie_eps;
     uint64_t seed, sid_base;
@@ -53,13 +58,12 @@ struct TypedArgs {
     uint32_t* counts;                // [B] anchors of each job (written by the count kernel)
     int capacity;                    // offsets are capacities fixed in advance: clamp counts to them
     uint32_t* err;                   // device flag: bit 0 set when a job had more anchors than its capacity
-    unsigned long long* host_totals; // mapped host memory for the two list totals (may be null)
+    unsigned long long* host_totals; // mapped host memory: anchors, windows, most windows of a sample (may be null)
     uint32_t* apos;                  // anchor positions (within the slice)
     uint32_t* aem;                   // anchor emission masks over the slots
     uint8_t* ashift;                 // 1 where no slot matches the call (every slot scaled by e^-999)
-    uint32_t* wsample;               // window -> sample
     unsigned long long total_windows;
-    float* ckptF;                    // [windows][Lmax] forward anchor at each window's first anchor
+    float* ckptF;                    // [windows][Lmax] forward anchor at the first anchor of every K-th window
     float* ckptB;                    // [windows][Lmax] backward anchor (E . beta, scaled)
     double* ckptU;                   // [windows] log of the backward anchor's unit
     float* dosage;
@@ -82,6 +86,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
                        std::vector<TypedSample>& ts, uint32_t& lmax, bool& all_full);
 
 uint32_t typed_default_window(uint32_t lmax);   // anchors per window when the caller gives none
+constexpr uint32_t kPostGroup = 16;             // windows per posterior group (fixed: rounding restarts there)
 uint32_t typed_default_threads(uint32_t lmax);  // posterior CTA size when the caller gives none
 
 }  // namespace si

@@ -16,11 +16,14 @@
 //   anchor_count / anchor_scan / anchor_fill   per-sample anchor lists (marker 0
 //                                              is always an anchor)
 //   anchor_chain     one group of L/4 lanes (four slots each) per sample and
-//                    direction: forward and backward over anchors, checkpoints
-//                    every C anchors
-//   anchor_posterior one thread per (sample, window of C anchors) rebuilds the
-//                    window's anchors from the checkpoints; then one lane per
-//                    marker writes dosage, P(hap=1) and haplotypes.
+//                    direction: forward and backward over anchors; backward
+//                    checkpoints every C anchors (a window), forward ones
+//                    every K windows
+//   anchor_posterior one lane per sample walks the markers of K windows:
+//                    the window's backward records are rebuilt from its
+//                    checkpoint, alpha is carried from anchor to anchor, and
+//                    every marker's dosage, P(hap=1) and haplotypes are
+//                    written through a shared-memory tile.
 #include "fb_typed.hpp"
 #include "philox.cuh"
 
@@ -138,19 +141,27 @@ __global__ void anchor_count_kernel(TypedArgs A) {
 }
 
 // Exclusive scans of anchor counts and window counts (ceil(count / C)) in one
-// CTA; entry B holds the totals, also written to host_totals (mapped pinned
-// host memory) when given: a copy would queue behind other device-to-host
-// copies on the copy engine.
+// CTA; entry B holds the totals, also written with the most windows of any
+// sample to host_totals[0..2] (mapped pinned host memory) when given: a copy
+// would queue behind other device-to-host copies on the copy engine.
 __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __restrict__ counts, uint32_t B,
                                                            uint32_t C, unsigned long long* __restrict__ aoff,
                                                            unsigned long long* __restrict__ woff,
                                                            unsigned long long* __restrict__ host_totals) {
     __shared__ unsigned long long sa[32], sw[32];
+    __shared__ uint32_t smax[32];
     const uint32_t t = threadIdx.x, T = blockDim.x, lane = t & 31, warp = t >> 5;
     const uint32_t per = (B + T - 1) / T;
     const uint32_t b0 = min(B, t * per), b1 = min(B, b0 + per);
     unsigned long long la = 0, lw = 0;
-    for (uint32_t b = b0; b < b1; ++b) { la += counts[b]; lw += (counts[b] + C - 1) / C; }
+    uint32_t mx = 0;
+    for (uint32_t b = b0; b < b1; ++b) {
+        la += counts[b];
+        lw += (counts[b] + C - 1) / C;
+        mx = max(mx, counts[b]);
+    }
+    mx = __reduce_max_sync(0xffffffffu, mx);
+    if (lane == 0) smax[warp] = mx;
     unsigned long long ia = la, iw = lw;
 #pragma unroll
     for (int o = 1; o < 32; o <<= 1) {
@@ -169,6 +180,7 @@ __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __res
         }
         sa[lane] = pa - xa;
         sw[lane] = pw - xw;
+        smax[lane] = __reduce_max_sync(0xffffffffu, lane < (T >> 5) ? smax[lane] : 0u);
     }
     __syncthreads();
     unsigned long long ra = sa[warp] + ia - la, rw = sw[warp] + iw - lw;
@@ -184,6 +196,7 @@ __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __res
         if (host_totals) {  // mapped host memory: the host reads the totals without a copy
             host_totals[0] = ra;
             host_totals[1] = rw;
+            host_totals[2] = (smax[0] + C - 1) / C;
             __threadfence_system();
         }
     }
@@ -227,7 +240,6 @@ __global__ void anchor_fill_kernel(TypedArgs A) {
         }
         o += __shfl_sync(0xffffffffu, incl, 31);
     }
-    for (unsigned long long w = A.woff[s] + lane; w < A.woff[s + 1]; w += 32) A.wsample[w] = s;
 }
 
 // ---------------------------------------------------------------- chain
@@ -316,8 +328,8 @@ constexpr uint32_t kChainBlock = 8;  // anchors per block of list entries (loade
 // steps in lockstep to the longest of its chains (a finished chain holds its
 // state), in blocks of kChainBlock anchors: step j of a block is held by lane
 // j % G of the group in register j / G, loaded one block ahead and read by
-// shuffle. Checkpoints: forward vector at anchors k % C == 0; backward vector
-// and the log of its unit at the same anchors.
+// shuffle. Checkpoints: backward vector and the log of its unit at anchors
+// k % C == 0 (window starts); forward vector at anchors k % (K C) == 0.
 template <int LM>
 __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
     constexpr uint32_t G = LM / 4, GPW = 32 / G, R = kChainBlock / G;
@@ -408,7 +420,8 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
                 prev = act ? p : prev;
                 cc = act ? cc - 1 : cc;
                 if (act && cc == 0) {
-                    *reinterpret_cast<float4*>(A.ckptF + (wb + ci) * LM + sl) = make_float4(a[0], a[1], a[2], a[3]);
+                    if (ci % A.K == 0)
+                        *reinterpret_cast<float4*>(A.ckptF + (wb + ci) * LM + sl) = make_float4(a[0], a[1], a[2], a[3]);
                     ++ci;
                     cc = C;
                 }
@@ -515,26 +528,35 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
 
 // ---------------------------------------------------------------- posterior
 //
-// Phase 1, one thread per window (C consecutive anchors of one sample): from
-// the window's checkpoints, rebuild for every anchor k of the window the
-// interval record of the run [pos[k], pos[k+1]):
-//   a'  forward vector after the emission at k, divided by its sum
-//   w'  backward vector of anchor k+1 (E . beta), divided by its sum
-//   {p0, p1, farg'} with farg' = -999 - logU - ln(sum w) the log of beta's
-//       e^-999 floor in units of w'; -inf when the floor is negligible over
-//       the whole run, +inf when beta is uniform (the chain's last run, or a
-//       floor that dominates everywhere).
-// With a' and w' of unit sum, a cell i markers after p0 and j = p1 - m before
-// p1 has
-//   alpha_l ~ Q[i] a'_l + S[i]      beta_l ~ Q[j] w'_l + S[j] (+ floor)
-//   p_l = alpha_l beta_l.
-// Phase 2, one warp per run of windows of the same sample: lane = marker, so
-// each warp step covers 32 consecutive markers and writes them coalesced. A
-// lane finds its record by counting anchors (typed markers and marker 0) up
-// to its marker with a ballot over the codes.
+// One warp per (32 samples, group of K consecutive windows of C anchors); lane
+// = sample. A lane walks its sample's markers of the group one per step:
+//   group start: alpha from the forward checkpoint at the group's first anchor
+//     (the chain writes one every K windows), and the first window's
+//     backward records (rebuild_window);
+//   at an anchor (a typed marker, or marker 0): alpha steps over the run from
+//     the previous anchor and takes the anchor's emission; the run starting
+//     there takes its backward record, and at a window's first anchor the
+//     window's records are rebuilt from the window's end checkpoint;
+//   every marker: p_l = (Q[i] a'_l + S[i]) (X w'_l + Y), dosage, pick and
+//     P(hap=1).
+// The backward record of the run [pos[k], pos[k+1]) holds
+//   w'     the backward vector of anchor k+1 (E . beta), divided by its sum;
+//   farg'  -999 - logU - ln(sum w), the log of beta's e^-999 floor in units of
+//          w': -inf when the floor is negligible over the whole run, and the
+//          run is "uniform" (w' = 0, beta constant) for the chain's last run
+//          or where the floor dominates everywhere.
+// With a' and w' of unit sum, a cell i markers after pos[k] and j = pos[k+1]
+// - m before the next anchor has alpha_l ~ Q[i] a'_l + S[i] and beta_l ~
+// Q[j] w'_l + S[j] (+ floor). Lanes whose samples share typed positions (an
+// array's sites, every batch of the benchmark workloads) step through the
+// same markers, so the per-marker slot data are warp-uniform loads; other
+// lanes still work, with divergent anchor steps. Outputs are staged in a
+// per-warp tile [32 samples][32 steps] in shared memory and leave as row
+// segments of 32 consecutive markers.
 
-// mode of a record from the high word of farg'
+// high word of farg' for a uniform run and for a negligible floor
 constexpr uint32_t kInfHi = 0x7ff00000u;
+constexpr uint32_t kNegInfHi = 0xfff00000u;
 
 __device__ __forceinline__ float rcp_approx(float x) {
     float r;
@@ -542,70 +564,236 @@ __device__ __forceinline__ float rcp_approx(float x) {
     return r;
 }
 
-template <int LM>
-__host__ __device__ constexpr uint32_t post_record_bytes() { return 2u * LM * 4u + 16u; }
+// three-input maximum (sm_100)
+__device__ __forceinline__ float max3(float a, float b, float c) {
+    float r;
+    asm("max.f32 %0, %1, %2, %3;" : "=f"(r) : "f"(a), "f"(b), "f"(c));
+    return r;
+}
 
-// Markers [c0, c1) of one sample, covered by consecutive windows whose
-// records are slots cu + 1 .. umax of this warp's record arrays; lane = marker.
+template <int LM>
+__device__ __forceinline__ float vmax(const float (&p)[LM]) {
+    float m = p[0];
+#pragma unroll
+    for (int l = 1; l + 1 < LM; l += 2) m = max3(m, p[l], p[l + 1]);
+    if (LM % 2 == 0) m = fmaxf(m, p[LM - 1]);
+    return m;
+}
+
+// Shared memory of one warp: backward records [C][LM/4][32] float4 and
+// [C][32] farg'; the flush descriptors [2][32] uint4; the dosage tile
+// [32][33] f32, the allele tile [32][34] u16 and, for P(hap=1), [32][33] f32x2.
+__host__ __device__ constexpr size_t post_warp_bytes(uint32_t LM, uint32_t C, bool hprob) {
+    return (size_t)C * LM * 128 + (size_t)C * 256 + 1024 + 32 * 33 * 4 + 32 * 34 * 2 + (hprob ? 32 * 33 * 8 : 0);
+}
+
+// Backward records of window w (anchors [wC, min(wC + C, NA))) of one sample,
+// rebuilt from the window's end checkpoint, into the lane's column of recW/recF.
+template <int LM>
+__device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& tb, const uint32_t* pos,
+                                               const uint32_t* aem, const uint8_t* ash, unsigned long long wb,
+                                               uint32_t NA, uint32_t len, uint32_t w, float4* recW, uint2* recF,
+                                               uint32_t lane) {
+    constexpr uint32_t Q4 = LM / 4;
+    const uint32_t C = A.C;
+    const uint32_t k0 = w * C, k1 = min(k0 + C, NA);
+    float bv[LM];
+    double logU;
+    uint32_t kstart;
+    if (k1 < NA) {
+        const float4* src = reinterpret_cast<const float4*>(A.ckptB + (wb + w + 1) * LM);
+#pragma unroll
+        for (uint32_t q = 0; q < Q4; ++q) {
+            const float4 x = src[q];
+            bv[4 * q] = x.x; bv[4 * q + 1] = x.y; bv[4 * q + 2] = x.z; bv[4 * q + 3] = x.w;
+        }
+        logU = A.ckptU[wb + w + 1];
+        kstart = k1;
+    } else {
+        // the chain's last run: beta is uniform there
+        logU = chain_end_logU(tb, len - 1 - pos[NA - 1]) - 999.0 * (double)ash[NA - 1];
+        init_forward<LM>(bv, aem[NA - 1]);
+        kstart = NA - 1;
+        const uint32_t r = NA - 1 - k0;
+#pragma unroll
+        for (uint32_t q = 0; q < Q4; ++q) recW[(r * Q4 + q) * 32 + lane] = make_float4(0.f, 0.f, 0.f, 0.f);
+        recF[r * 32 + lane] = make_uint2(0u, kInfHi);
+    }
+    for (uint32_t k = kstart; k > k0; --k) {
+        const uint32_t n = pos[k] - pos[k - 1];
+        const float sw = vsum<LM>(bv);
+        const double farg = -999.0 - logU;
+        uint32_t lo = 0u, hi;
+        if (farg + tabG(tb, n) < -104.0) hi = kNegInfHi;  // floor negligible over the run
+        else if (farg + tabG(tb, 1) > 60.0) hi = kInfHi;  // floor dominates: beta uniform
+        else {
+            const double f = farg - log((double)sw);
+            lo = (uint32_t)__double_as_longlong(f);
+            hi = (uint32_t)((unsigned long long)__double_as_longlong(f) >> 32);
+        }
+        const uint32_t r = k - 1 - k0;
+        const float inv = hi == kInfHi ? 0.f : rcp_approx(sw);
+#pragma unroll
+        for (uint32_t q = 0; q < Q4; ++q)
+            recW[(r * Q4 + q) * 32 + lane] =
+                make_float4(bv[4 * q] * inv, bv[4 * q + 1] * inv, bv[4 * q + 2] * inv, bv[4 * q + 3] * inv);
+        recF[r * 32 + lane] = make_uint2(lo, hi);
+        if (k - 1 > k0) backward_step<LM>(tb, n, bv, logU, aem[k - 1], ash[k - 1], 0u);
+    }
+}
+
+// kFull: every sample of the launch uses all LM slots (no active-slot masking).
 // kFast: dosage and haplotypes are written, argmax picks, no P(hap=1).
 template <int LM, bool kFull, bool kFast>
-__device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v, uint32_t c0, uint32_t c1, uint32_t cu,
-                                              uint32_t umax, const float* recA, const float* recW, const uint4* recM,
-                                              const float4* lut, uint32_t lane) {
-    const uint32_t le_mask = 0xffffffffu >> (31 - lane);
-    const uint32_t lj = lane & 7;
-    const float keep = 1.0f - A.tie_eps;
-    const bool w_dos = A.dosage != nullptr, w_hap = A.haps != nullptr, w_hp = A.hprob != nullptr;
-    const bool argmax = A.sampling == SI_SAMPLE_ARGMAX;
+__global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kernel(TypedArgs A) {
+    extern __shared__ __align__(16) unsigned char smem[];
+    constexpr uint32_t Q4 = LM / 4;
+    constexpr uint32_t kAll = 0xffffffffu;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t C = A.C, K = A.K;
+    unsigned char* wbase = smem + (size_t)warp * post_warp_bytes(LM, C, !kFast);
+    float4* recW = reinterpret_cast<float4*>(wbase);                     // [C][Q4][32]
+    uint2* recF = reinterpret_cast<uint2*>(recW + (size_t)C * Q4 * 32);  // [C][32]
+    uint4* meta = reinterpret_cast<uint4*>(recF + (size_t)C * 32);       // [2][32]
+    float* tD = reinterpret_cast<float*>(meta + 64);                     // [32][33]
+    uint16_t* tH = reinterpret_cast<uint16_t*>(tD + 32 * 33);            // [32][34]
+    float2* tP = reinterpret_cast<float2*>(tH + 32 * 34);                // [32][33]
+
+    const uint32_t SG = (A.B + 31) / 32;
+    const unsigned long long gw = (unsigned long long)blockIdx.x * nw + warp;
+    const uint32_t s = (uint32_t)(gw % SG) * 32 + lane;
+    const unsigned long long grp = gw / SG;
+    bool live = s < A.B && grp * K < A.max_windows;
+    View v{};
+    uint32_t NA = 0;
+    unsigned long long ab = 0, wb = 0;
+    if (live) {
+        v = view_of(A, s);
+        NA = A.counts[s];
+        ab = A.aoff[s];
+        wb = A.woff[s];
+    }
+    const uint32_t NW = (NA + C - 1) / C;
+    const uint32_t w0 = live ? (uint32_t)grp * K : 0u;
+    const uint32_t wend = min(w0 + K, NW);
+    live = live && w0 < wend;
+    if (!__any_sync(kAll, live)) return;  // whole warp
+
     const Tabs& tb = v.r.tabs;
-    const uint32_t lmask = lmask_of(v.r.L);
+    const uint32_t* pos = A.apos + ab;
+    const uint32_t* aem = A.aem + ab;
+    const uint8_t* ash = A.ashift + ab;
+    const bool w_dos = kFast || A.dosage != nullptr, w_hap = kFast || A.haps != nullptr;
+    const bool w_hp = !kFast && A.hprob != nullptr;
+    const bool argmax = kFast || A.sampling == SI_SAMPLE_ARGMAX;
+    const float keep = 1.0f - A.tie_eps;
     float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
+    {
+        const uint32_t lmask = lmask_of(v.r.L);
 #pragma unroll
-    for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
-    const uint8_t* gp = v.geno;
-    const SlotMasks* mp = v.r.masks;
-    float* dos = (kFast || w_dos) ? A.dosage + v.out : nullptr;
-    uint8_t* h0 = (kFast || w_hap) ? A.haps + 2 * v.out : nullptr;
-    uint8_t* h1 = (kFast || w_hap) ? h0 + v.len : nullptr;
-    float2* hp = (!kFast && w_hp) ? reinterpret_cast<float2*>(A.hprob) + v.out : nullptr;
-    // codes and slot masks of the step, loaded one step ahead
-    const uint32_t mq = min(c0 + lane, c1 - 1);
-    uint8_t code = gp[mq];
-    SlotMasks mk = mp[mq];
-    for (uint32_t cb = c0; cb < c1; cb += 32) {
-        const uint32_t m_raw = cb + lane;
-        const bool valid = m_raw < c1;
-        const uint32_t m = valid ? m_raw : c1 - 1;  // lanes past the run repeat its last marker
-        const uint8_t code_c = code;
-        const SlotMasks mk_c = mk;
-        {
-            const uint32_t mn = min(m_raw + 32, c1 - 1);
-            code = gp[mn];
-            mk = mp[mn];
+        for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
+    }
+
+    float ap[LM], wp[LM];  // a' and w' of the current run
+    uint2 fr = make_uint2(0u, kNegInfHi);
+    uint32_t k = w0 * C, p0 = 0, p1 = 0, m = 0, mend = 0;
+#pragma unroll
+    for (int l = 0; l < LM; ++l) { ap[l] = 0.f; wp[l] = 0.f; }
+    auto load_record = [&](uint32_t r) {
+#pragma unroll
+        for (uint32_t q = 0; q < Q4; ++q) {
+            const float4 x = recW[(r * Q4 + q) * 32 + lane];
+            wp[4 * q] = x.x; wp[4 * q + 1] = x.y; wp[4 * q + 2] = x.z; wp[4 * q + 3] = x.w;
         }
-        const bool is_anchor = valid && (m == 0 || code_c < 3);
-        const uint32_t bal = __ballot_sync(0xffffffffu, is_anchor);
-        // the codes' anchors are the list's, except in a job a plan cut to its
-        // capacity: stay on the run's records there
-        const uint32_t u = min(cu + __popc(bal & le_mask), umax);
-        cu += __popc(bal);
-        const uint4 meta = recM[u];
-        float2 qi, qj;
-        if (__all_sync(0xffffffffu, meta.y - meta.x < tb.NT)) {  // every run of the step is in the table
-            qi = __ldg(tb.QS + (m - meta.x));
-            qj = __ldg(tb.QS + (meta.y - m));
-        } else {
-            qi = tabQS(tb, m - meta.x);
-            qj = tabQS(tb, meta.y - m);
+        fr = recF[r * 32 + lane];
+    };
+    if (live) {
+        const float4* src = reinterpret_cast<const float4*>(A.ckptF + (wb + w0) * LM);
+#pragma unroll
+        for (uint32_t q = 0; q < Q4; ++q) {
+            const float4 x = src[q];
+            ap[4 * q] = x.x; ap[4 * q + 1] = x.y; ap[4 * q + 2] = x.z; ap[4 * q + 3] = x.w;
         }
-        const bool uni = meta.w == kInfHi;                  // beta uniform
-        const bool fin = (meta.w & kInfHi) != kInfHi;       // finite farg': floor term per marker
-        float xb = uni ? 0.f : qj.x, yb = uni ? 1.f : qj.y;
-        if (__any_sync(0xffffffffu, fin)) {
-            if (fin) {
+        const float inv = rcp_approx(vsum<LM>(ap));
+#pragma unroll
+        for (int l = 0; l < LM; ++l) ap[l] *= inv;
+        p0 = pos[k];
+        p1 = k + 1 < NA ? pos[k + 1] : v.len;
+        mend = wend * C < NA ? pos[wend * C] : v.len;
+        m = p0;
+        rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, v.len, w0, recW, recF, lane);
+        load_record(0);
+    }
+    bool in_tab = p1 - p0 < tb.NT;  // every i, j of the run index the tables
+
+    // flush the tile's valid columns (a prefix per lane) as row segments
+    uint32_t tstart = m, tcnt = 0;
+    auto flush = [&]() {
+        __syncwarp();
+        const unsigned long long od = v.out + tstart, oh = 2ull * v.out + tstart;
+        meta[lane] = make_uint4((uint32_t)od, (uint32_t)(od >> 32), (uint32_t)oh, (uint32_t)(oh >> 32));
+        meta[32 + lane] = make_uint4(v.len, live ? tcnt : 0u, 0u, 0u);
+        __syncwarp();
+        for (uint32_t r = 0; r < 32; ++r) {
+            const uint4 m1 = meta[32 + r];
+            if (m1.y == 0) continue;  // same value in every lane
+            const uint4 m0 = meta[r];
+            if (lane < m1.y) {
+                const unsigned long long rd = ((unsigned long long)m0.y << 32) | m0.x;
+                const unsigned long long rh = ((unsigned long long)m0.w << 32) | m0.z;
+                if (w_dos) A.dosage[rd + lane] = tD[r * 33 + lane];
+                if (w_hap) {
+                    const uint32_t h = tH[r * 34 + lane];
+                    A.haps[rh + lane] = (uint8_t)(h & 0xffu);
+                    A.haps[rh + m1.x + lane] = (uint8_t)(h >> 8);
+                }
+                if (w_hp) reinterpret_cast<float2*>(A.hprob)[rd + lane] = tP[r * 33 + lane];
+            }
+        }
+        __syncwarp();
+        tstart = m;
+        tcnt = 0;
+    };
+
+    for (uint32_t step = 0;; ++step) {
+        const bool on = live && m < mend;
+        if (!__any_sync(kAll, on)) break;
+        if (on && m == p1) {
+            // anchor k + 1: alpha steps over the run and takes its emission
+            const uint32_t kn = k + 1, n = p1 - p0;
+            if (kn % C == 0) rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, v.len, kn / C, recW, recF, lane);
+            const float2 qs = tabQS(tb, n);
+            const float base = vsum<LM>(ap) * qs.y;
+            const uint32_t em = aem[kn];
+#pragma unroll
+            for (int l = 0; l < LM; ++l) ap[l] = ((em >> l) & 1u) ? fmaf(qs.x, ap[l], base) : 0.f;
+            const float inv = rcp_approx(vsum<LM>(ap));
+#pragma unroll
+            for (int l = 0; l < LM; ++l) ap[l] *= inv;
+            load_record(kn % C);
+            k = kn;
+            p0 = p1;
+            p1 = kn + 1 < NA ? pos[kn + 1] : v.len;
+            in_tab = p1 - p0 < tb.NT;
+        }
+        const bool all_tab = __all_sync(kAll, !on || in_tab);
+        const bool fin = (fr.y & kInfHi) != kInfHi;  // finite farg': floor term per marker
+        const bool any_fin = __any_sync(kAll, on && fin);
+        const uint32_t col = step & 31;
+        if (on) {
+            const uint32_t i = m - p0, j = p1 - m;
+            float2 qi, qj;
+            if (all_tab) {
+                qi = __ldg(tb.QS + i);
+                qj = __ldg(tb.QS + j);
+            } else {
+                qi = tabQS(tb, i);
+                qj = tabQS(tb, j);
+            }
+            float xb = qj.x, yb = fr.y == kInfHi ? 1.f : qj.y;  // uniform run: w' = 0, beta = 1
+            if (any_fin && fin) {
                 // floor e^ft beside Q w' + S; when it dominates (ft > 0) scale both by e^-ft
-                const float ft = (float)(__longlong_as_double(((long long)meta.w << 32) | meta.z) +
-                                         tabG(tb, meta.y - m));
+                const float ft = (float)(__hiloint2double((int)fr.y, (int)fr.x) + tabG(tb, j));
                 const float e = expf(-fminf(fabsf(ft), 104.f));
                 const bool big = ft > 0.f;
                 const float xs = big ? e : 1.f;
@@ -613,207 +801,97 @@ __device__ __forceinline__ void posterior_run(const TypedArgs& A, const View& v,
                 xb = qj.x * xs;
                 yb = fmaf(qj.y, xs, F);
             }
-        }
-        const float4* RA = reinterpret_cast<const float4*>(recA + (size_t)u * LM);
-        const float4* RW = reinterpret_cast<const float4*>(recW + (size_t)u * LM);
-        const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
-        const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
-        // beta uniform in every lane: w' is multiplied by 0, so it need not be read
-        const bool all_uni = __all_sync(0xffffffffu, uni);
-        float pr[LM];
-        float2 tot2 = make_float2(0.f, 0.f), q02 = tot2, q12 = tot2;
+            const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
+            const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
+            const float4* gr = reinterpret_cast<const float4*>(v.r.g + (size_t)m * v.r.gs);
+            float p[LM];
+            float2 tot2 = make_float2(0.f, 0.f), d2 = tot2;
 #pragma unroll
-        for (int q4 = 0; q4 < LM / 4; ++q4) {
-            const float4 av = RA[q4], wv = all_uni ? make_float4(0.f, 0.f, 0.f, 0.f) : RW[q4];
-            float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.x, av.y), YF),
-                                    __ffma2_rn(XB, make_float2(wv.x, wv.y), YB));
-            float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(av.z, av.w), YF),
-                                    __ffma2_rn(XB, make_float2(wv.z, wv.w), YB));
-            if (!kFull) {
-                p01 = __fmul2_rn(p01, make_float2(act[4 * q4], act[4 * q4 + 1]));
-                p23 = __fmul2_rn(p23, make_float2(act[4 * q4 + 2], act[4 * q4 + 3]));
+            for (uint32_t q = 0; q < Q4; ++q) {
+                float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(ap[4 * q], ap[4 * q + 1]), YF),
+                                        __ffma2_rn(XB, make_float2(wp[4 * q], wp[4 * q + 1]), YB));
+                float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(ap[4 * q + 2], ap[4 * q + 3]), YF),
+                                        __ffma2_rn(XB, make_float2(wp[4 * q + 2], wp[4 * q + 3]), YB));
+                if (!kFull) {
+                    p01 = __fmul2_rn(p01, make_float2(act[4 * q], act[4 * q + 1]));
+                    p23 = __fmul2_rn(p23, make_float2(act[4 * q + 2], act[4 * q + 3]));
+                }
+                p[4 * q] = p01.x; p[4 * q + 1] = p01.y; p[4 * q + 2] = p23.x; p[4 * q + 3] = p23.y;
+                tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
+                if (kFull || 4 * q < v.r.gs) {
+                    const float4 gv = __ldg(gr + q);
+                    d2 = __ffma2_rn(p01, make_float2(gv.x, gv.y), d2);
+                    d2 = __ffma2_rn(p23, make_float2(gv.z, gv.w), d2);
+                }
             }
-            pr[4 * q4] = p01.x; pr[4 * q4 + 1] = p01.y; pr[4 * q4 + 2] = p23.x; pr[4 * q4 + 3] = p23.y;
-            tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
-            const float4 m0 = lut[((mk_c.a0 >> (4 * q4)) & 15u) * 8 + lj];
-            const float4 m1 = lut[((mk_c.a1 >> (4 * q4)) & 15u) * 8 + lj];
-            q02 = __ffma2_rn(p01, make_float2(m0.x, m0.y), q02);
-            q02 = __ffma2_rn(p23, make_float2(m0.z, m0.w), q02);
-            q12 = __ffma2_rn(p01, make_float2(m1.x, m1.y), q12);
-            q12 = __ffma2_rn(p23, make_float2(m1.z, m1.w), q12);
-        }
-        const float tot = tot2.x + tot2.y, q0 = q02.x + q02.y, q1 = q12.x + q12.y;
-        uint32_t pick;
-        if (kFast || argmax) {
-            float pmax = pr[0];
+            const float tot = tot2.x + tot2.y;
+            const SlotMasks mk = v.r.masks[m];
+            uint32_t pick;
+            if (argmax) {
+                const float thr = vmax<LM>(p) * keep;
+                pick = 0;
 #pragma unroll
-            for (int l = 1; l < LM; ++l) pmax = fmaxf(pmax, pr[l]);
-            const float thr = pmax * keep;
-            pick = 0;
+                for (int l = LM - 1; l >= 1; --l) pick = (p[l] >= thr) ? (uint32_t)l : pick;
+                if (p[0] >= thr) pick = 0;
+            } else {
+                const float target = cell_uniform(A.seed, v.sid, v.m0 + m) * tot;
+                float cum = 0.f;
+                uint32_t last_nz = 0;
+                pick = LM;
 #pragma unroll
-            for (int l = LM - 1; l >= 1; --l) pick = (pr[l] >= thr) ? (uint32_t)l : pick;
-            if (pr[0] >= thr) pick = 0;
-        } else {
-            const float target = cell_uniform(A.seed, v.sid, v.m0 + m) * tot;
-            float cum = 0.f;
-            uint32_t last_nz = 0;
-            pick = LM;
-#pragma unroll
-            for (int l = 0; l < LM; ++l) {
-                cum += pr[l];
-                if (pr[l] > 0.f) last_nz = (uint32_t)l;
-                if (pick == LM && target < cum) pick = (uint32_t)l;
+                for (int l = 0; l < LM; ++l) {
+                    cum += p[l];
+                    if (p[l] > 0.f) last_nz = (uint32_t)l;
+                    if (pick == LM && target < cum) pick = (uint32_t)l;
+                }
+                if (pick == LM) pick = last_nz;
             }
-            if (pick == LM) pick = last_nz;
+            const float inv = rcp_approx(tot);
+            tD[lane * 33 + col] = (d2.x + d2.y) * inv;
+            tH[lane * 34 + col] = (uint16_t)(((mk.a0 >> pick) & 1u) | (((mk.a1 >> pick) & 1u) << 8));
+            if (w_hp) {
+                float q0 = 0.f, q1 = 0.f;
+#pragma unroll
+                for (int l = 0; l < LM; ++l) {
+                    q0 += ((mk.a0 >> l) & 1u) ? p[l] : 0.f;
+                    q1 += ((mk.a1 >> l) & 1u) ? p[l] : 0.f;
+                }
+                tP[lane * 33 + col] = make_float2(q0 * inv, q1 * inv);
+            }
+            ++m;
+            ++tcnt;
         }
-        const float inv = rcp_approx(tot);
-        // lanes past the run recomputed its last marker: they store the same bytes there
-        if (kFast || w_dos) dos[m] = (q0 + q1) * inv;
-        if (kFast || w_hap) {
-            h0[m] = (uint8_t)((mk_c.a0 >> pick) & 1u);
-            h1[m] = (uint8_t)((mk_c.a1 >> pick) & 1u);
-        }
-        if (!kFast && w_hp) hp[m] = make_float2(q0 * inv, q1 * inv);
+        if (col == 31) flush();
     }
+    flush();
 }
 
-// kFull: every sample of the launch uses all LM slots (no active-slot masking).
-template <int LM, bool kFull>
-__global__ void __launch_bounds__(128, (LM <= 8 ? 7 : 4)) anchor_posterior_kernel(TypedArgs A) {
-    extern __shared__ __align__(16) unsigned char smem[];
-    const uint32_t t = threadIdx.x, C = A.C, lane = t & 31, warp = t >> 5;
-    // nibble -> four 0/1 floats, 8 copies so that the 8 lanes of a quarter warp
-    // read distinct banks: entry e, copy j at float4 index 8 e + j
-    float4* lut = reinterpret_cast<float4*>(smem);
-    const size_t per_warp = (size_t)32 * C * post_record_bytes<LM>();
-    unsigned char* wbase = smem + 2048 + (size_t)warp * per_warp;
-    float* recA = reinterpret_cast<float*>(wbase);                            // [32 C][LM]
-    float* recW = recA + (size_t)32 * C * LM;                                  // [32 C][LM]
-    uint4* recM = reinterpret_cast<uint4*>(recW + (size_t)32 * C * LM);        // [32 C] {p0, p1, farg' lo, hi}
-    for (uint32_t e = t; e < 128; e += blockDim.x) {
-        const uint32_t n = e >> 3;
-        lut[e] = make_float4((float)(n & 1), (float)((n >> 1) & 1), (float)((n >> 2) & 1), (float)(n >> 3));
-    }
-    __syncthreads();
-
-    // ---- phase 1
-    const unsigned long long g = (unsigned long long)blockIdx.x * blockDim.x + t;
-    bool live = g < A.total_windows;
-    uint32_t s = 0xffffffffu, cstart = 0, cend = 0, nrec = 0;
-    if (live) {
-        s = A.wsample[g];
-        // a plan's capacity windows past the job's anchors hold nothing
-        if ((g - A.woff[s]) * C >= A.counts[s]) {
-            live = false;
-            s = 0xffffffffu;
-        }
-    }
-    if (live) {
-        const View v = view_of(A, s);
-        const Tabs& tb = v.r.tabs;
-        const unsigned long long base = A.aoff[s], wb = A.woff[s], w = g - wb;
-        const unsigned long long NA = A.counts[s];
-        const uint32_t* pos = A.apos + base;
-        const uint32_t* aem = A.aem + base;
-        const uint8_t* ash = A.ashift + base;
-        const unsigned long long k0 = w * C, k1 = min(k0 + C, NA);
-        const uint32_t u0 = lane * C;  // this window's first record
-        nrec = (uint32_t)(k1 - k0);
-        cstart = pos[k0];
-        cend = k1 < NA ? pos[k1] : v.len;
-        // backward: records k0 .. k1-1 take w' from anchor k+1
-        float bv[LM];
-        double logU;
-        unsigned long long kstart;
-        if (k1 < NA) {
-#pragma unroll
-            for (int l = 0; l < LM; ++l) bv[l] = A.ckptB[(wb + w + 1) * LM + l];
-            logU = A.ckptU[wb + w + 1];
-            kstart = k1;
-        } else {
-            logU = chain_end_logU(tb, v.len - 1 - pos[NA - 1]) - 999.0 * (double)ash[NA - 1];
-            init_forward<LM>(bv, aem[NA - 1]);
-            kstart = NA - 1;
-            const uint32_t u = u0 + (uint32_t)(NA - 1 - k0);
-#pragma unroll
-            for (int l = 0; l < LM; ++l) recW[(size_t)u * LM + l] = 0.f;
-            recM[u] = make_uint4(pos[NA - 1], v.len, 0u, kInfHi);  // beta uniform
-        }
-        for (unsigned long long k = kstart; k > k0; --k) {
-            const uint32_t p0 = pos[k - 1], p1 = pos[k], n = p1 - p0;
-            const float sw = vsum<LM>(bv);
-            const double farg = -999.0 - logU;
-            uint32_t lo = 0u, hi;
-            if (farg + tabG(tb, n) < -104.0) hi = kInfHi | 0x80000000u;  // floor negligible: -inf
-            else if (farg + tabG(tb, 1) > 60.0) hi = kInfHi;               // floor dominates: uniform
-            else {
-                const double f = farg - log((double)sw);
-                lo = (uint32_t)__double_as_longlong(f);
-                hi = (uint32_t)((unsigned long long)__double_as_longlong(f) >> 32);
-            }
-            const uint32_t u = u0 + (uint32_t)(k - 1 - k0);
-            const float inv = rcp_approx(sw);
-#pragma unroll
-            for (int l = 0; l < LM; ++l) recW[(size_t)u * LM + l] = bv[l] * inv;
-            recM[u] = make_uint4(p0, p1, lo, hi);
-            if (k - 1 > k0) backward_step<LM>(tb, n, bv, logU, aem[k - 1], ash[k - 1], 0u);
-        }
-        // forward: records take a' at anchor k
-        float a[LM];
-#pragma unroll
-        for (int l = 0; l < LM; ++l) a[l] = A.ckptF[(wb + w) * LM + l];
-        for (unsigned long long k = k0; k < k1; ++k) {
-            const uint32_t u = u0 + (uint32_t)(k - k0);
-            const float inv = rcp_approx(vsum<LM>(a));
-#pragma unroll
-            for (int l = 0; l < LM; ++l) recA[(size_t)u * LM + l] = a[l] * inv;
-            if (k + 1 < k1) forward_step<LM>(tb, pos[k + 1] - pos[k], a, aem[k + 1]);
-        }
-    }
-    __syncwarp();
-
-    // ---- phase 2
-    const uint32_t live_mask = __ballot_sync(0xffffffffu, live);
-    const bool fast = A.dosage && A.haps && !A.hprob && A.sampling == SI_SAMPLE_ARGMAX;
-    uint32_t rest = live_mask;
-    while (rest) {
-        const uint32_t r = __ffs(rest) - 1;
-        const uint32_t sr = __shfl_sync(0xffffffffu, s, r);
-        const uint32_t same = __ballot_sync(0xffffffffu, live && s == sr);
-        const uint32_t r2 = 31 - __clz(same);  // windows of a sample are consecutive
-        const uint32_t c0 = __shfl_sync(0xffffffffu, cstart, r), c1 = __shfl_sync(0xffffffffu, cend, r2);
-        const View v = view_of(A, sr);
-        const uint32_t cu = r * C - 1u;  // record of the marker before c0 (wraps for r = 0)
-        const uint32_t umax = r2 * C + __shfl_sync(0xffffffffu, nrec, r2) - 1u;  // the run's last record
-        if (fast) posterior_run<LM, kFull, true>(A, v, c0, c1, cu, umax, recA, recW, recM, lut, lane);
-        else posterior_run<LM, kFull, false>(A, v, c0, c1, cu, umax, recA, recW, recM, lut, lane);
-        rest &= ~((2u << r2) - 1u);  // lanes up to r2 are done (r2 = 31 clears all)
-    }
-}
-
-template <int LM>
-size_t post_smem(uint32_t T, uint32_t C) {
-    return 2048 + (size_t)T * C * post_record_bytes<LM>();
-}
-
-template <int LM, bool kFull>
-cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
+template <int LM, bool kFull, bool kFast>
+cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     const uint32_t T = a.threads;
-    const size_t sm = post_smem<LM>(T, a.C);
+    const size_t sm = (size_t)(T / 32) * post_warp_bytes(LM, a.C, !kFast);
     // set outside stream capture only (a plan launches once before it is captured)
     cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
     cudaError_t e = cudaStreamIsCapturing(s, &cs);
     if (e != cudaSuccess) return e;
     if (cs == cudaStreamCaptureStatusNone) {
-        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                 (int)sm);
+        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull, kFast>,
+                                 cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
-    const unsigned long long grid = (a.total_windows + T - 1) / T;
+    const unsigned long long groups = ((unsigned long long)a.max_windows + a.K - 1) / a.K;
+    const unsigned long long warps = (unsigned long long)((a.B + 31) / 32) * groups;
+    const unsigned long long grid = (warps + T / 32 - 1) / (T / 32);
     if (grid == 0) return cudaSuccess;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    anchor_posterior_kernel<LM, kFull><<<(uint32_t)grid, T, sm, s>>>(a);
+    anchor_posterior_kernel<LM, kFull, kFast><<<(uint32_t)grid, T, sm, s>>>(a);
     return cudaGetLastError();
+}
+
+template <int LM, bool kFull>
+cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
+    const bool fast = a.dosage && a.haps && !a.hprob && a.sampling == SI_SAMPLE_ARGMAX;
+    return fast ? launch_post_v<LM, kFull, true>(a, s) : launch_post_v<LM, kFull, false>(a, s);
 }
 
 template <int LM>
@@ -831,17 +909,12 @@ cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
 
 // The window (anchors rebuilt from one checkpoint) fixes where rounding
 // restarts, so it must not depend on the batch: one value for every L. The
-// CTA size changes nothing numerically and shrinks as the records grow.
+// CTA size changes nothing numerically.
 uint32_t typed_default_window(uint32_t) { return 2u; }
-uint32_t typed_default_threads(uint32_t lmax) { return lmax <= 8 ? 128u : (lmax <= 16 ? 64u : 32u); }
+uint32_t typed_default_threads(uint32_t lmax) { return lmax <= 16 ? 128u : 64u; }
 
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C) {
-    switch (fb_lmax(L)) {
-        case 4: return post_smem<4>(T, C);
-        case 8: return post_smem<8>(T, C);
-        case 16: return post_smem<16>(T, C);
-        default: return post_smem<32>(T, C);
-    }
+    return (size_t)(T / 32) * post_warp_bytes(fb_lmax(L), C, true);
 }
 
 cudaError_t launch_anchor_lists_count(const TypedArgs& a, cudaStream_t s) {

@@ -31,7 +31,7 @@ struct si_plan {
     bool all_full = true;
     uint32_t B = 0;
     std::vector<unsigned long long> cap;  // anchor capacity per job
-    si::DeviceBuffer regions, samples, counts, aoff, woff, apos, aem, acode, wsample, ckF, ckB, ckU, err;
+    si::DeviceBuffer regions, samples, counts, aoff, woff, apos, aem, acode, ckF, ckB, ckU, err;
     uint32_t C = 2, T = 128;
     float best_ms = 0.f;
     cudaStream_t capture_stream = nullptr;
@@ -49,7 +49,7 @@ void free_plan(si_plan* P) {
     if (P->graph) cudaGraphDestroy(P->graph);
     if (P->capture_stream) cudaStreamDestroy(P->capture_stream);
     for (DeviceBuffer* b : {&P->regions, &P->samples, &P->counts, &P->aoff, &P->woff, &P->apos, &P->aem, &P->acode,
-                            &P->wsample, &P->ckF, &P->ckB, &P->ckU, &P->err})
+                            &P->ckF, &P->ckB, &P->ckU, &P->err})
         si::dev_free(c, *b);
     delete P;
 }
@@ -78,8 +78,12 @@ si_status use_tiles(si_plan* P, uint32_t C, uint32_t T, cudaStream_t s) {
     } else {
         return si::cuda_fail(P->ctx, e, "plan window offsets");
     }
+    unsigned long long most = 0;
+    for (unsigned long long c : P->cap) most = std::max(most, (c + C - 1) / C);
     P->a.C = C;
     P->a.threads = T;
+    P->a.K = si::kPostGroup;
+    P->a.max_windows = (uint32_t)most;
     P->a.total_windows = w.back();
     P->C = C;
     P->T = T;
@@ -133,7 +137,6 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
     alloc(P->apos, (size_t)NA * 4);
     alloc(P->aem, (size_t)NA * 4);
     alloc(P->acode, (size_t)NA);
-    alloc(P->wsample, (size_t)NWmax * 4);
     alloc(P->ckF, (size_t)NWmax * lm * 4);
     alloc(P->ckB, (size_t)NWmax * lm * 4);
     alloc(P->ckU, (size_t)NWmax * 8);
@@ -170,7 +173,6 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
     a.apos = (uint32_t*)P->apos.ptr;
     a.aem = (uint32_t*)P->aem.ptr;
     a.ashift = (uint8_t*)P->acode.ptr;
-    a.wsample = (uint32_t*)P->wsample.ptr;
     a.ckptF = (float*)P->ckF.ptr;
     a.ckptB = (float*)P->ckB.ptr;
     a.ckptU = (double*)P->ckU.ptr;
@@ -183,8 +185,7 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
     if ((flags & SI_PLAN_AUTOTUNE) && !p->checkpoint_interval && !p->block_threads) {
         // candidates: window size x posterior CTA size, each timed on this batch
         std::vector<uint32_t> Cs = {1, 2, 4};
-        std::vector<uint32_t> Ts = lm <= 8 ? std::vector<uint32_t>{64, 128} : (lm <= 16 ? std::vector<uint32_t>{32, 64}
-                                                                                       : std::vector<uint32_t>{32});
+        std::vector<uint32_t> Ts = lm <= 16 ? std::vector<uint32_t>{64, 128} : std::vector<uint32_t>{32, 64};
         cudaEvent_t e0, e1;
         cudaEventCreate(&e0);
         cudaEventCreate(&e1);

@@ -17,9 +17,12 @@
 namespace si {
 namespace {
 
+// Outputs (each may be null): pairs [M][L][2]; masks [M]; g [M][gs], the ALT
+// allele count a(h0_k) + a(h1_k) of each slot as a float (0 past L), which the
+// posterior pass weighs by slot to form the dosage.
 __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t* __restrict__ panel, uint32_t M,
                               uint32_t N, uint32_t W, uint32_t L, int kind, uint32_t* __restrict__ pairs,
-                              SlotMasks* __restrict__ masks) {
+                              SlotMasks* __restrict__ masks, float* __restrict__ g, uint32_t gs) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     const uint32_t* hrow = head ? head + (uint64_t)m * kHead : nullptr;
@@ -43,14 +46,18 @@ __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t*
         }
     }
     if (masks) masks[m] = SlotMasks{a0, a1};
+    if (g)
+        for (uint32_t k = 0; k < gs; ++k)
+            g[(uint64_t)m * gs + k] = k < L ? (float)(((a0 >> k) & 1u) + ((a1 >> k) & 1u)) : 0.f;
 }
 
 }  // namespace
 
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
-                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, cudaStream_t s) {
+                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint32_t gs,
+                          cudaStream_t s) {
     const uint32_t bs = 128;
-    select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_pairs, d_masks);
+    select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_pairs, d_masks, d_g, gs);
     return cudaGetLastError();
 }
 

@@ -160,7 +160,7 @@ uint64_t reclaimable(const si_server* S, int k) {
     const auto& z = S->slot[k];
     uint64_t b = 0;
     for (const si::DeviceBuffer* x : {&c->t_counts, &c->t_aoff, &c->t_woff, &c->t_apos, &c->t_acode, &c->t_aem,
-                                      &c->t_wsample, &c->t_ckF, &c->t_ckB, &c->t_ckU, &c->job_regions,
+                                      &c->t_ckF, &c->t_ckB, &c->t_ckU, &c->job_regions,
                                       &c->job_samples, &z.d_geno, &z.d_dos, &z.d_haps, &z.d_hp})
         b += x->bytes;
     return b;
@@ -192,9 +192,12 @@ void add_need(const si_server* S, Need& n, const si_request& q) {
 void trim_region_cache(si_server* S) {
     si_ctx* c = S->ctx;
     uint64_t b = 0;
-    for (auto& kv : c->region_sel) b += kv.second.masks.bytes;
+    for (auto& kv : c->region_sel) b += kv.second.masks.bytes + kv.second.g.bytes;
     if (b <= c->budget / 8) return;
-    for (auto& kv : c->region_sel) si::dev_free(c, kv.second.masks);
+    for (auto& kv : c->region_sel) {
+        si::dev_free(c, kv.second.masks);
+        si::dev_free(c, kv.second.g);
+    }
     c->region_sel.clear();
 }
 

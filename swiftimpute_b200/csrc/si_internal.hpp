@@ -65,6 +65,7 @@ struct SelectionCache {
     int kind = 0;
     DeviceBuffer pairs;  // [M][L][2] u32
     DeviceBuffer masks;  // [M] SlotMasks
+    DeviceBuffer g;      // [M][fb_lmax(L)] f32 ALT allele count per slot
 };
 
 }  // namespace si
@@ -104,7 +105,7 @@ struct si_ctx {
     si::LinTrans trans0{1.f, 0.f};  // host copy of the first gap's transition
     si::DeviceBuffer ckpt;           // forward checkpoints (full-chain kernel)
     // typed-marker kernel scratch and tables
-    si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_aem, t_wsample, t_ckF, t_ckB, t_ckU;
+    si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_aem, t_ckF, t_ckB, t_ckU;
     struct TableSet {
         si::DeviceBuffer QS, G;
         double consts[4] = {0, 0, 0, 0};  // log2q, lr, lgc, regime
@@ -113,10 +114,11 @@ struct si_ctx {
     // region-local selection tables (index restarted at the region start), per (m_begin, m_end, L, kind)
     struct RegionSel {
         si::DeviceBuffer masks;
+        si::DeviceBuffer g;
     };
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, RegionSel> region_sel;
     si::DeviceBuffer job_regions, job_samples;  // uploaded descriptors of the last uneven batch
-    unsigned long long* pinned_totals = nullptr;  // mapped: written by the scan kernel
+    unsigned long long* pinned_totals = nullptr;  // mapped [4]: written by the scan kernel
     unsigned long long* pinned_totals_dev = nullptr;
     cudaEvent_t totals_ev = nullptr;
     si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
@@ -149,7 +151,8 @@ cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, u
                               uint32_t* d_perm_scratch, cudaStream_t s);
 size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W);
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
-                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, cudaStream_t s);
+                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint32_t gs,
+                          cudaStream_t s);
 
 struct FbLaunch {
     const uint8_t* geno;   // [B][M]

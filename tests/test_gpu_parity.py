@@ -170,9 +170,9 @@ def test_fb_tiles_do_not_change_results(engine):
             assert np.abs(alt["dosage"] - base["dosage"]).max() <= 2e-5
     ms = engine.last_kernel_ms()
     assert len(ms) == 4 and ms[3] > 0
-    # a typed tile whose interval records exceed shared memory is refused, not truncated
+    # a typed tile whose window records exceed shared memory is refused, not truncated
     with pytest.raises(N.SIError) as e:
-        engine.impute(codes, N.default_params(checkpoint_interval=32, block_threads=128))
+        engine.impute(codes, N.default_params(num_states=32, checkpoint_interval=32, block_threads=128))
     assert e.value.status == 4  # SI_ERR_UNSUPPORTED
 
 
