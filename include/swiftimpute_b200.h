@@ -103,13 +103,22 @@ si_status si_ctx_memory(const si_ctx* ctx, uint64_t* used_bytes, uint64_t* budge
 /* Panel ------------------------------------------------------------------ */
 
 /* Upload a u8 panel [M][N] (ReferencePanel::haplotypes(), imputer.hpp:86).
- * Alleles must be 0 or 1; it is stored bit-packed on the device. Replaces the
- * panel copies of EmissionComputer::set_reference_panel (emission.cu:189) and
- * HaplotypeSampler::set_reference_panel (sampling.cu:219). */
+ * Any byte is accepted, as the reference stores it (imputer.cpp:85-112):
+ * ALLELE_MISSING = 255 for '.', the allele index for multi-allelic calls. The
+ * device keeps one bit per allele (set for a non-zero byte, the side the
+ * reference's PBWT sorts it to, pbwt_index.cpp:183) and, per marker, a list of
+ * the bytes other than 0 and 1 (N < 2^24 when there are any). Emission classes
+ * follow the byte sum (emission.cu:35-54), sampled haplotypes carry the panel
+ * byte (sampling.cu:121-126), and dosage and P(hap=1) count non-zero alleles.
+ * Replaces the panel copies of EmissionComputer::set_reference_panel
+ * (emission.cu:189) and HaplotypeSampler::set_reference_panel (sampling.cu:219). */
 si_status si_panel_upload_u8(si_ctx* ctx, const uint8_t* alleles, uint32_t M, uint32_t N);
 
+/* Number of panel entries other than 0 and 1 in the uploaded panel. */
+si_status si_panel_exception_count(const si_ctx* ctx, uint64_t* count);
+
 /* Upload an already bit-packed panel [M][words_per_row] u32: bit i of word w
- * is haplotype 32 w + i. words_per_row >= ceil(N / 32). */
+ * is haplotype 32 w + i (alleles 0 and 1 only). words_per_row >= ceil(N / 32). */
 si_status si_panel_upload_packed(si_ctx* ctx, const uint32_t* words, uint32_t M, uint32_t N,
                                  uint32_t words_per_row);
 

@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstring>
 #include <new>
+#include <thread>
 
 namespace si {
 
@@ -86,15 +87,59 @@ void reset_index(si_ctx* ctx) {
         dev_free(ctx, kv.second.pairs);
         dev_free(ctx, kv.second.masks);
         dev_free(ctx, kv.second.g);
+        dev_free(ctx, kv.second.raw);
     }
     ctx->sel.clear();
     for (auto& kv : ctx->region_sel) {
         dev_free(ctx, kv.second.masks);
         dev_free(ctx, kv.second.g);
+        dev_free(ctx, kv.second.raw);
     }
     ctx->region_sel.clear();
     ctx->has_index = false;
     ctx->pbwt_flags = 0;
+}
+
+void clear_exceptions(si_ctx* ctx) {
+    dev_free(ctx, ctx->ex_off);
+    dev_free(ctx, ctx->ex_ent);
+    ctx->n_ex = 0;
+}
+
+// Alleles other than 0 and 1 of a u8 panel [M][N], per marker in haplotype
+// order: off[M + 1] and entries h << 8 | byte. Rows are scanned eight bytes at
+// a time on several host threads; a 0/1 panel yields none.
+void panel_exceptions(const uint8_t* a, uint32_t M, uint32_t N, std::vector<unsigned long long>& off,
+                      std::vector<uint32_t>& ent) {
+    off.assign((size_t)M + 1, 0);
+    ent.clear();
+    const uint32_t nt = std::max(1u, std::min<uint32_t>({std::thread::hardware_concurrency(), 16u, M}));
+    std::vector<std::vector<uint32_t>> part(nt);
+    auto scan = [&](uint32_t t) {
+        const uint32_t r0 = (uint32_t)((uint64_t)M * t / nt), r1 = (uint32_t)((uint64_t)M * (t + 1) / nt);
+        for (uint32_t m = r0; m < r1; ++m) {
+            const uint8_t* row = a + (size_t)m * N;
+            uint64_t n = 0;
+            uint32_t h = 0;
+            for (; h + 8 <= N; h += 8) {
+                uint64_t w;
+                std::memcpy(&w, row + h, 8);
+                if (!(w & 0xFEFEFEFEFEFEFEFEull)) continue;
+                for (uint32_t j = 0; j < 8; ++j)
+                    if (row[h + j] > 1) { part[t].push_back((h + j) << 8 | row[h + j]); ++n; }
+            }
+            for (; h < N; ++h)
+                if (row[h] > 1) { part[t].push_back(h << 8 | row[h]); ++n; }
+            off[m + 1] = n;
+        }
+    };
+    std::vector<std::thread> th;
+    for (uint32_t t = 1; t < nt; ++t) th.emplace_back(scan, t);
+    scan(0);
+    for (auto& x : th) x.join();
+    for (uint32_t m = 0; m < M; ++m) off[m + 1] += off[m];
+    ent.reserve(off[M]);
+    for (auto& p : part) ent.insert(ent.end(), p.begin(), p.end());
 }
 
 // Li–Stephens transition between genetic positions (Morgans), as
@@ -167,11 +212,13 @@ si_status ensure_selection(si_ctx* ctx, uint32_t L, int kind, SelectionCache** o
             SI_TRY(dev_alloc(ctx, c.pairs, (size_t)ctx->M * L * 2 * sizeof(uint32_t)));
             SI_TRY(dev_alloc(ctx, c.masks, (size_t)ctx->M * sizeof(SlotMasks)));
             SI_TRY(dev_alloc(ctx, c.g, (size_t)ctx->M * fb_lmax(L) * sizeof(float)));
+            if (ctx->n_ex) SI_TRY(dev_alloc(ctx, c.raw, (size_t)ctx->M * fb_lmax(L) * 2));
         }
         SI_CUDA(ctx,
                 launch_select((const uint32_t*)ctx->head.ptr, (const uint32_t*)ctx->panel.ptr, ctx->M, ctx->N, ctx->W,
-                              L, kind, (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, (float*)c.g.ptr, fb_lmax(L),
-                              s ? s : ctx->stream),
+                              L, kind, (const unsigned long long*)ctx->ex_off.ptr, (const uint32_t*)ctx->ex_ent.ptr,
+                              (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, (float*)c.g.ptr, (uint8_t*)c.raw.ptr,
+                              fb_lmax(L), s ? s : ctx->stream),
                 "select kernel");
     }
     *out = &c;
@@ -318,6 +365,7 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
     a.sid_base = p->sample_id_base;
     a.reg0.masks = (const SlotMasks*)sel->masks.ptr;
     a.reg0.g = (const float*)sel->g.ptr;
+    a.reg0.raw = (const uint8_t*)sel->raw.ptr;
     a.reg0.gs = fb_lmax(p->num_states);
     a.reg0.L = p->num_states;
     SI_TRY(tables_for(ctx, ctx->trans0, p->num_states, &a.reg0.tabs));
@@ -360,7 +408,8 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
                         std::to_string(fb_smem_bytes(p->num_states, T, C)) + " bytes of shared memory (max 227 KB)");
     SI_TRY(dev_reserve(ctx, ctx->ckpt, fb_ckpt_bytes(B, ctx->M, p->num_states, C)));
     FbLaunch l;
-    l.geno = d_geno; l.masks = (const SlotMasks*)sel->masks.ptr; l.trans = (const LinTrans*)ctx->trans.ptr;
+    l.geno = d_geno; l.masks = (const SlotMasks*)sel->masks.ptr; l.raw = (const uint8_t*)sel->raw.ptr;
+    l.trans = (const LinTrans*)ctx->trans.ptr;
     l.B = B; l.M = ctx->M; l.L = p->num_states; l.C = C; l.threads = T;
     l.sampling = p->sampling; l.tie_eps = (float)p->tie_eps; l.seed = p->seed; l.sample_id_base = p->sample_id_base;
     l.ckpt = (float*)ctx->ckpt.ptr; l.dosage = d_dosage; l.hprob = d_hprob; l.haps = d_haps;
@@ -472,14 +521,18 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             auto& rs = ctx->region_sel[key];
             st = dev_alloc(ctx, rs.masks, (size_t)(g.m_end - g.m_begin) * sizeof(SlotMasks));
             if (st == SI_OK) st = dev_alloc(ctx, rs.g, (size_t)(g.m_end - g.m_begin) * fb_lmax(L) * sizeof(float));
+            if (st == SI_OK && ctx->n_ex) st = dev_alloc(ctx, rs.raw, (size_t)(g.m_end - g.m_begin) * fb_lmax(L) * 2);
             if (st != SI_OK) {
                 dev_free(ctx, rs.masks);
+                dev_free(ctx, rs.g);
                 ctx->region_sel.erase(key);
                 break;
             }
             e = launch_select((const uint32_t*)head.ptr + sweeps[j].head_off,
                               (const uint32_t*)ctx->panel.ptr + (size_t)g.m_begin * W, g.m_end - g.m_begin, N, W, L,
-                              kind, nullptr, (SlotMasks*)rs.masks.ptr, (float*)rs.g.ptr, fb_lmax(L), s);
+                              kind, ctx->n_ex ? (const unsigned long long*)ctx->ex_off.ptr + g.m_begin : nullptr,
+                              (const uint32_t*)ctx->ex_ent.ptr, nullptr, (SlotMasks*)rs.masks.ptr, (float*)rs.g.ptr,
+                              (uint8_t*)rs.raw.ptr, fb_lmax(L), s);
         }
         if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);  // scratch reuse below
         dev_free(ctx, head);
@@ -497,6 +550,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             SI_TRY(ensure_selection(ctx, L, p->selection_kind, &sel, false, s));
             tr[r].masks = (const SlotMasks*)sel->masks.ptr + g.m_begin;
             tr[r].g = (const float*)sel->g.ptr + (size_t)g.m_begin * fb_lmax(L);
+            tr[r].raw = sel->raw.ptr ? (const uint8_t*)sel->raw.ptr + (size_t)g.m_begin * fb_lmax(L) * 2 : nullptr;
             tr[r].gs = fb_lmax(L);
             SI_TRY(tables_for(ctx, ctx->trans0, L, &tr[r].tabs));
         } else {
@@ -504,6 +558,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             const auto& rs = ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)];
             tr[r].masks = (const SlotMasks*)rs.masks.ptr;
             tr[r].g = (const float*)rs.g.ptr;
+            tr[r].raw = (const uint8_t*)rs.raw.ptr;
             tr[r].gs = fb_lmax(L);
             if (!region_first_gap_ok(ctx, p, g.m_begin, g.m_end))
                 return fail(ctx, SI_ERR_UNSUPPORTED, "region " + std::to_string(r) +
@@ -596,7 +651,10 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     for (auto& kv : ctx->region_sel) {
         dev_free(ctx, kv.second.masks);
         dev_free(ctx, kv.second.g);
+        dev_free(ctx, kv.second.raw);
     }
+    dev_free(ctx, ctx->ex_off);
+    dev_free(ctx, ctx->ex_ent);
     if (ctx->pinned_totals) cudaFreeHost(ctx->pinned_totals);
     if (ctx->totals_ev) cudaEventDestroy(ctx->totals_ev);
     for (auto& e : ctx->ev) if (e) cudaEventDestroy(e);
@@ -624,6 +682,7 @@ si_status si_panel_upload_packed(si_ctx* ctx, const uint32_t* words, uint32_t M,
         return fail(ctx, SI_ERR_INVALID_ARG, "bad packed panel arguments (need M >= 1, N >= 2)");
     SI_TRY(set_device(ctx));
     reset_index(ctx);
+    clear_exceptions(ctx);
     const uint32_t W = words_per_row_pad(N);
     SI_TRY(dev_alloc(ctx, ctx->panel, (size_t)M * W * 4));
     SI_CUDA(ctx,
@@ -660,38 +719,52 @@ si_status si_panel_upload_u8(si_ctx* ctx, const uint8_t* alleles, uint32_t M, ui
     if (!alleles || M == 0 || N < 2) return fail(ctx, SI_ERR_INVALID_ARG, "bad panel arguments (need M >= 1, N >= 2)");
     SI_TRY(set_device(ctx));
     reset_index(ctx);
+    clear_exceptions(ctx);
+    std::vector<unsigned long long> ex_off;
+    std::vector<uint32_t> ex_ent;
+    panel_exceptions(alleles, M, N, ex_off, ex_ent);
+    if (!ex_ent.empty() && N >= (1u << 24))
+        return fail(ctx, SI_ERR_UNSUPPORTED, "panels with alleles other than 0/1 need N < 2^24 haplotypes");
     const uint32_t W = words_per_row_pad(N);
     SI_TRY(dev_alloc(ctx, ctx->panel, (size_t)M * W * 4));
     SI_CUDA(ctx, cudaMemsetAsync(ctx->panel.ptr, 0, (size_t)M * W * 4, ctx->stream), "memset panel");
     // stream the u8 panel through a bounded staging buffer
     const size_t row_bytes = N;
     const uint32_t rows_per_chunk = (uint32_t)std::max<size_t>(1, std::min<size_t>(M, (256u << 20) / row_bytes));
-    DeviceBuffer stage, bad;
+    DeviceBuffer stage;
     SI_TRY(dev_alloc(ctx, stage, (size_t)rows_per_chunk * row_bytes));
-    si_status st = dev_alloc(ctx, bad, 4);
-    if (st != SI_OK) { dev_free(ctx, stage); return st; }
-    cudaError_t e = cudaMemsetAsync(bad.ptr, 0, 4, ctx->stream);
+    cudaError_t e = cudaSuccess;
     for (uint32_t m0 = 0; m0 < M && e == cudaSuccess; m0 += rows_per_chunk) {
         const uint32_t rows = std::min(rows_per_chunk, M - m0);
         e = cudaMemcpyAsync(stage.ptr, alleles + (size_t)m0 * N, (size_t)rows * N, cudaMemcpyHostToDevice, ctx->stream);
         if (e == cudaSuccess)
             e = launch_pack_panel((const uint8_t*)stage.ptr, rows, N, W, (uint32_t*)ctx->panel.ptr + (size_t)m0 * W,
-                                  (uint32_t*)bad.ptr, ctx->stream);
+                                  ctx->stream);
         if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);  // staging buffer reuse
     }
-    uint32_t h_bad = 0;
-    if (e == cudaSuccess) e = cudaMemcpy(&h_bad, bad.ptr, 4, cudaMemcpyDeviceToHost);
     dev_free(ctx, stage);
-    dev_free(ctx, bad);
     if (e != cudaSuccess) return cuda_fail(ctx, e, "panel upload");
-    if (h_bad) {
-        dev_free(ctx, ctx->panel);
-        return fail(ctx, SI_ERR_UNSUPPORTED,
-                    "panel alleles must be 0 or 1 (missing or multi-allelic panel entries are not supported)");
+    if (!ex_ent.empty()) {
+        si_status st = dev_alloc(ctx, ctx->ex_off, ex_off.size() * 8);
+        if (st == SI_OK) st = dev_alloc(ctx, ctx->ex_ent, ex_ent.size() * 4);
+        if (st != SI_OK) {
+            clear_exceptions(ctx);
+            dev_free(ctx, ctx->panel);
+            return st;
+        }
+        SI_CUDA(ctx, cudaMemcpy(ctx->ex_off.ptr, ex_off.data(), ex_off.size() * 8, cudaMemcpyHostToDevice), "copy exceptions");
+        SI_CUDA(ctx, cudaMemcpy(ctx->ex_ent.ptr, ex_ent.data(), ex_ent.size() * 4, cudaMemcpyHostToDevice), "copy exceptions");
+        ctx->n_ex = ex_ent.size();
     }
     ctx->M = M; ctx->N = N; ctx->W = W;
     ctx->has_map = false;
     ctx->trans_key = ~0ull;
+    return SI_OK;
+}
+
+si_status si_panel_exception_count(const si_ctx* ctx, uint64_t* count) {
+    if (!ctx || !count) return SI_ERR_INVALID_ARG;
+    *count = ctx->n_ex;
     return SI_OK;
 }
 

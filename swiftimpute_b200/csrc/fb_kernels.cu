@@ -28,6 +28,7 @@
 // coalesced row segments.
 #include "philox.cuh"
 #include "si_internal.hpp"
+#include "slots.cuh"
 
 namespace si {
 namespace {
@@ -35,6 +36,7 @@ namespace {
 struct FbArgs {
     const uint8_t* geno;
     const SlotMasks* masks;
+    const uint8_t* raw;
     const LinTrans* trans;
     uint32_t B, M, L, C, nseg;
     int sampling;
@@ -51,19 +53,6 @@ __device__ __forceinline__ int exp2_of(float x) {  // floor(log2 x) for positive
 }
 __device__ __forceinline__ float pow2_neg(int e) {  // 2^-e, |e| <= 126
     return __int_as_float((127 - e) << 23);
-}
-
-// Emission mask of slots matching genotype code g; all slots (and *shift = 1)
-// when the call matches none; all slots (shift 0) when missing.
-__device__ __forceinline__ uint32_t emission_mask(uint32_t g, SlotMasks mk, uint32_t lmask, uint32_t* shift) {
-    uint32_t mg;
-    if (g == 0) mg = ~(mk.a0 | mk.a1);
-    else if (g == 1) mg = mk.a0 ^ mk.a1;
-    else if (g == 2) mg = mk.a0 & mk.a1;
-    else { *shift = 0; return lmask; }
-    mg &= lmask;
-    *shift = mg ? 0u : 1u;
-    return mg ? mg : lmask;
 }
 
 template <int LM>
@@ -243,8 +232,9 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
             dbuf[t * DS + i] = (q0 + q1) * inv;
             hbuf[t * HS + 2 * i] = q0 * inv;
             hbuf[t * HS + 2 * i + 1] = q1 * inv;
-            pbuf[(t * 2 + 0) * PS + i] = (uint8_t)((mk.a0 >> pick) & 1u);
-            pbuf[(t * 2 + 1) * PS + i] = (uint8_t)((mk.a1 >> pick) & 1u);
+            const uint32_t hv = slot_alleles(mk, a.raw, fb_lmax(L), m, pick);
+            pbuf[(t * 2 + 0) * PS + i] = (uint8_t)(hv & 0xffu);
+            pbuf[(t * 2 + 1) * PS + i] = (uint8_t)(hv >> 8);
             // this marker's emission/transition drive beta_{m-1}
             uint32_t sh;
             em_next = emission_mask(gbuf[t * GS + i], mk, lmask, &sh);
@@ -289,7 +279,6 @@ cudaError_t launch_lm(const FbArgs& fa, uint32_t T, cudaStream_t s) {
 
 }  // namespace
 
-uint32_t fb_lmax(uint32_t L) { return L <= 4 ? 4 : L <= 8 ? 8 : L <= 16 ? 16 : 32; }
 
 size_t fb_smem_bytes(uint32_t L, uint32_t T, uint32_t C) {
     switch (fb_lmax(L)) {
@@ -307,7 +296,7 @@ size_t fb_ckpt_bytes(uint32_t B, uint32_t M, uint32_t L, uint32_t C) {
 
 cudaError_t launch_fb(const FbLaunch& l, cudaStream_t s) {
     FbArgs fa;
-    fa.geno = l.geno; fa.masks = l.masks; fa.trans = l.trans;
+    fa.geno = l.geno; fa.masks = l.masks; fa.raw = l.raw; fa.trans = l.trans;
     fa.B = l.B; fa.M = l.M; fa.L = l.L; fa.C = l.C; fa.nseg = (l.M + l.C - 1) / l.C;
     fa.sampling = l.sampling; fa.tie_eps = l.tie_eps; fa.seed = l.seed; fa.sid_base = l.sample_id_base;
     fa.ckpt = l.ckpt; fa.dosage = l.dosage; fa.hprob = l.hprob; fa.haps = l.haps;

@@ -1,6 +1,7 @@
 // fb_typed.hpp — launch interface of the typed-marker forward-backward.
 #pragma once
 #include "si_internal.hpp"
+#include "slots.cuh"
 
 namespace si {
 
@@ -18,12 +19,14 @@ struct TypedTables {
     int regime;  // 0: rho < 1, 1: rho > 1, 2: rho == 1
 };
 
-// A panel slice imputed with L slots: its slot masks and per-slot ALT counts
-// g [marker][gs] (index 0 = the slice's first marker), and the closed-form
-// tables of its transition.
+// A panel slice imputed with L slots: its slot masks, per-slot ALT counts
+// g [marker][gs] and allele bytes raw [marker][gs][2] (null for a 0/1 panel;
+// index 0 = the slice's first marker), and the closed-form tables of its
+// transition.
 struct TypedRegion {
     const SlotMasks* masks;
     const float* g;
+    const uint8_t* raw;
     uint32_t gs;
     uint32_t L;
     TypedTables tabs;

@@ -33,17 +33,6 @@ namespace {
 __device__ __forceinline__ int exp2_of(float x) { return ((__float_as_int(x) >> 23) & 0xff) - 127; }
 __device__ __forceinline__ float pow2_neg(int e) { return __int_as_float((127 - e) << 23); }
 
-__device__ __forceinline__ uint32_t emission_mask(uint32_t g, SlotMasks mk, uint32_t lmask, uint32_t* shift) {
-    uint32_t mg;
-    if (g == 0) mg = ~(mk.a0 | mk.a1);
-    else if (g == 1) mg = mk.a0 ^ mk.a1;
-    else if (g == 2) mg = mk.a0 & mk.a1;
-    else { *shift = 0; return lmask; }
-    mg &= lmask;
-    *shift = mg ? 0u : 1u;
-    return mg ? mg : lmask;
-}
-
 using Tabs = TypedTables;
 
 // Per-sample view: a plain batch is B rows of M codes sharing reg0; an uneven
@@ -848,7 +837,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
             }
             const float inv = rcp_approx(tot);
             tD[lane * 33 + col] = (d2.x + d2.y) * inv;
-            tH[lane * 34 + col] = (uint16_t)(((mk.a0 >> pick) & 1u) | (((mk.a1 >> pick) & 1u) << 8));
+            tH[lane * 34 + col] = (uint16_t)slot_alleles(mk, v.r.raw, v.r.gs, m, pick);
             if (w_hp) {
                 float q0 = 0.f, q1 = 0.f;
 #pragma unroll

@@ -345,11 +345,17 @@ void check_magic(std::istream& in, const char* magic, const char* what, const st
 
 // Binary panel: magic "SIPANEL1", M and N (u32), the markers and sample ids,
 // then the alleles bit-packed per marker: ceil(N/8) bytes, haplotype h at bit
-// h%8 of byte h/8
+// h%8 of byte h/8 (bit set for a non-zero allele). A panel with alleles other
+// than 0 and 1 (ALLELE_MISSING, multi-allelic indices) is written as
+// "SIPANEL2": the same, followed by their count (u64) and, in marker then
+// haplotype order, each as marker (u32), haplotype (u32) and byte (u8).
 void ReferencePanel::save_binary(const std::string& filename) const {
     std::ofstream o(filename, std::ios::binary);
     if (!o) throw ImputationError("Cannot write " + filename);
-    o.write("SIPANEL1", 8);
+    const size_t cells = (size_t)num_markers() * num_haplotypes_;
+    uint64_t n_other = 0;
+    for (size_t i = 0; i < cells; ++i) n_other += haplotypes_[i] > 1;
+    o.write(n_other ? "SIPANEL2" : "SIPANEL1", 8);
     put_u32(o, num_markers());
     put_u32(o, num_haplotypes_);
     put_meta(o, markers_, samples_);
@@ -357,12 +363,20 @@ void ReferencePanel::save_binary(const std::string& filename) const {
     std::vector<char> row(rb);
     for (marker_t m = 0; m < num_markers(); ++m) {
         std::fill(row.begin(), row.end(), 0);
-        for (haplotype_t h = 0; h < num_haplotypes_; ++h) {
-            const allele_t a = haplotypes_[(size_t)m * num_haplotypes_ + h];
-            if (a > 1) throw ImputationError("binary panel format stores 0/1 alleles only");
-            if (a) row[h / 8] |= (char)(1u << (h % 8));
-        }
+        for (haplotype_t h = 0; h < num_haplotypes_; ++h)
+            if (haplotypes_[(size_t)m * num_haplotypes_ + h]) row[h / 8] |= (char)(1u << (h % 8));
         o.write(row.data(), rb);
+    }
+    if (n_other) {
+        o.write(reinterpret_cast<const char*>(&n_other), 8);
+        for (marker_t m = 0; m < num_markers(); ++m)
+            for (haplotype_t h = 0; h < num_haplotypes_; ++h) {
+                const allele_t a = haplotypes_[(size_t)m * num_haplotypes_ + h];
+                if (a <= 1) continue;
+                put_u32(o, m);
+                put_u32(o, h);
+                o.write(reinterpret_cast<const char*>(&a), 1);
+            }
     }
     if (!o) throw ImputationError("write failed: " + filename);
 }
@@ -370,7 +384,10 @@ void ReferencePanel::save_binary(const std::string& filename) const {
 std::unique_ptr<ReferencePanel> ReferencePanel::load_binary(const std::string& filename) {
     std::ifstream in(filename, std::ios::binary);
     if (!in) throw ImputationError("Cannot open " + filename);
-    check_magic(in, "SIPANEL1", "binary panel", filename);
+    char magic[8];
+    in.read(magic, 8);
+    const bool v1 = in && std::memcmp(magic, "SIPANEL1", 8) == 0, v2 = in && std::memcmp(magic, "SIPANEL2", 8) == 0;
+    if (!v1 && !v2) throw ImputationError("not a binary panel: " + filename);
     const uint32_t M = get_u32(in), N = get_u32(in);
     std::vector<Marker> ms;
     std::vector<std::string> names;
@@ -384,6 +401,21 @@ std::unique_ptr<ReferencePanel> ReferencePanel::load_binary(const std::string& f
         for (uint32_t j = 0; j < N; ++j) h[(size_t)m * N + j] = (row[j / 8] >> (j % 8)) & 1u;
     }
     if (!in) throw ImputationError("truncated binary panel: " + filename);
+    if (v2) {
+        uint64_t n_other = 0;
+        in.read(reinterpret_cast<char*>(&n_other), 8);
+        check_body(in, n_other, 9, "binary panel", filename);
+        for (uint64_t i = 0; i < n_other && in; ++i) {
+            const uint32_t m = get_u32(in), j = get_u32(in);
+            unsigned char a = 0;
+            in.read(reinterpret_cast<char*>(&a), 1);
+            if (!in) break;
+            if (m >= M || j >= N || a <= 1 || !h[(size_t)m * N + j])
+                throw ImputationError("corrupt allele entry in binary panel: " + filename);
+            h[(size_t)m * N + j] = a;
+        }
+        if (!in) throw ImputationError("truncated binary panel: " + filename);
+    }
     return from_haplotypes(std::move(ms), to_samples(names), N, std::move(h));
 }
 

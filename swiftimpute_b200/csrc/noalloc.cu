@@ -101,6 +101,7 @@ extern "C" si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_param
     FbLaunch l;
     l.geno = d_geno;
     l.masks = (const SlotMasks*)it->second.masks.ptr;
+    l.raw = (const uint8_t*)it->second.raw.ptr;
     l.trans = (const LinTrans*)ctx->trans.ptr;
     l.B = B; l.M = ctx->M; l.L = L; l.C = C; l.threads = T;
     l.sampling = p->sampling; l.tie_eps = (float)p->tie_eps; l.seed = p->seed; l.sample_id_base = p->sample_id_base;

@@ -11,11 +11,12 @@
 namespace si {
 namespace {
 
-// u8 [M][N] -> bit-packed [M][W]. One warp builds one 32-haplotype word with
-// a ballot, so loads are coalesced bytes. Any value other than 0/1 raises
-// *bad (the bit-packed path stores one bit per allele).
+// u8 [M][N] -> bit-packed [M][W]: bit set for a non-zero allele, the side
+// the reference's sweep sends it to (pbwt_index.cpp:183). One warp builds one
+// 32-haplotype word with a ballot, so loads are coalesced bytes. Alleles other
+// than 0 and 1 are kept beside the bits in the panel's exception lists.
 __global__ void pack_panel_kernel(const uint8_t* __restrict__ u8, uint32_t M, uint32_t N, uint32_t W,
-                                  uint32_t* __restrict__ words, uint32_t* __restrict__ bad) {
+                                  uint32_t* __restrict__ words) {
     const uint64_t gtid = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x;
     const uint64_t word = gtid >> 5;
     const uint32_t lane = threadIdx.x & 31;
@@ -24,7 +25,6 @@ __global__ void pack_panel_kernel(const uint8_t* __restrict__ u8, uint32_t M, ui
     const uint32_t h = w * 32 + lane;
     uint8_t v = 0;
     if (h < N) v = u8[(uint64_t)m * N + h];
-    if (v > 1) atomicOr(bad, 1u);
     const uint32_t bits = __ballot_sync(0xffffffffu, v != 0);
     if (lane == 0) words[word] = bits;
 }
@@ -187,12 +187,12 @@ pbwt_sweep_kernel(const uint32_t* __restrict__ panel_all, const SweepJob* __rest
 }  // namespace
 
 cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,
-                              uint32_t* d_bad, cudaStream_t s) {
+                              cudaStream_t s) {
     const uint64_t threads = (uint64_t)M * W * 32;
     const uint32_t bs = 256;
     const uint64_t grid = (threads + bs - 1) / bs;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    pack_panel_kernel<<<(uint32_t)grid, bs, 0, s>>>(d_u8, M, N, W, d_words, d_bad);
+    pack_panel_kernel<<<(uint32_t)grid, bs, 0, s>>>(d_u8, M, N, W, d_words);
     return cudaGetLastError();
 }
 

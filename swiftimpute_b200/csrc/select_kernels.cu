@@ -17,19 +17,37 @@
 namespace si {
 namespace {
 
-// Outputs (each may be null): pairs [M][L][2]; masks [M]; g [M][gs], the ALT
-// allele count a(h0_k) + a(h1_k) of each slot as a float (0 past L), which the
-// posterior pass weighs by slot to form the dosage.
+// Allele byte of haplotype h in a panel row: 0 for a clear bit; for a set bit
+// the row's exception entry (sorted by haplotype) if there is one, else 1.
+__device__ __forceinline__ uint32_t allele_of(const uint32_t* prow, uint32_t h, const uint32_t* ex, uint32_t nex) {
+    if (!((prow[h >> 5] >> (h & 31)) & 1u)) return 0u;
+    uint32_t lo = 0, hi = nex;
+    while (lo < hi) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if ((ex[mid] >> 8) < h) lo = mid + 1;
+        else hi = mid;
+    }
+    return (lo < nex && (ex[lo] >> 8) == h) ? (ex[lo] & 0xffu) : 1u;
+}
+
+// Outputs (each may be null): pairs [M][L][2]; masks [M]; g [M][gs], the
+// number of non-zero alleles of each slot's pair as a float (0 past L), which
+// the posterior pass weighs by slot to form the dosage; raw [M][gs][2], the
+// pair's allele bytes (panels with alleles other than 0/1).
 __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t* __restrict__ panel, uint32_t M,
-                              uint32_t N, uint32_t W, uint32_t L, int kind, uint32_t* __restrict__ pairs,
-                              SlotMasks* __restrict__ masks, float* __restrict__ g, uint32_t gs) {
+                              uint32_t N, uint32_t W, uint32_t L, int kind,
+                              const unsigned long long* __restrict__ ex_off, const uint32_t* __restrict__ ex_ent,
+                              uint32_t* __restrict__ pairs, SlotMasks* __restrict__ masks, float* __restrict__ g,
+                              uint8_t* __restrict__ raw, uint32_t gs) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
     const uint32_t* hrow = head ? head + (uint64_t)m * kHead : nullptr;
     const uint32_t* prow = panel + (uint64_t)m * W;
     const uint32_t lane0 = min(4u, (N + 31) / 32);
     const uint32_t top = min(N, L);
-    uint32_t a0 = 0, a1 = 0;
+    const uint32_t* ex = ex_ent ? ex_ent + ex_off[m] : nullptr;
+    const uint32_t nex = ex_ent ? (uint32_t)(ex_off[m + 1] - ex_off[m]) : 0u;
+    uint32_t a0 = 0, a1 = 0, x = 0;
     for (uint32_t k = 0; k < L; ++k) {
         uint32_t h;
         if (kind == SI_SEL_WARP) h = (k < lane0) ? hrow[32 * k] : (k % N);
@@ -41,23 +59,36 @@ __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t*
             pairs[((uint64_t)m * L + k) * 2 + 1] = h1;
         }
         if (k < 32) {
-            a0 |= ((prow[h >> 5] >> (h & 31)) & 1u) << k;
-            a1 |= ((prow[h1 >> 5] >> (h1 & 31)) & 1u) << k;
+            const uint32_t v0 = allele_of(prow, h, ex, nex), v1 = allele_of(prow, h1, ex, nex);
+            a0 |= (v0 != 0u ? 1u : 0u) << k;
+            a1 |= (v1 != 0u ? 1u : 0u) << k;
+            x |= (v0 > 1u || v1 > 1u ? 1u : 0u) << k;
+            if (raw && k < gs) {
+                raw[((uint64_t)m * gs + k) * 2 + 0] = (uint8_t)v0;
+                raw[((uint64_t)m * gs + k) * 2 + 1] = (uint8_t)v1;
+            }
         }
     }
-    if (masks) masks[m] = SlotMasks{a0, a1};
+    if (masks) masks[m] = SlotMasks{a0, a1, x, 0u};
     if (g)
         for (uint32_t k = 0; k < gs; ++k)
             g[(uint64_t)m * gs + k] = k < L ? (float)(((a0 >> k) & 1u) + ((a1 >> k) & 1u)) : 0.f;
+    if (raw)
+        for (uint32_t k = L; k < gs; ++k) {
+            raw[((uint64_t)m * gs + k) * 2 + 0] = 0;
+            raw[((uint64_t)m * gs + k) * 2 + 1] = 0;
+        }
 }
 
 }  // namespace
 
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
-                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint32_t gs,
+                          uint32_t L, int kind, const unsigned long long* d_ex_off, const uint32_t* d_ex_ent,
+                          uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint8_t* d_raw, uint32_t gs,
                           cudaStream_t s) {
     const uint32_t bs = 128;
-    select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_pairs, d_masks, d_g, gs);
+    select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_ex_off, d_ex_ent, d_pairs,
+                                                   d_masks, d_g, d_raw, gs);
     return cudaGetLastError();
 }
 

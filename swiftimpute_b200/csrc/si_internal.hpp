@@ -34,10 +34,15 @@ inline uint32_t words_per_row_pad(uint32_t N) { return ((N + 31) / 32 + 3) & ~3u
 constexpr uint32_t kHead = 128;
 
 // Per-marker slot data consumed by the forward-backward kernels: for slot k,
-// bit k of a0 / a1 is the panel allele of the pair's first / second haplotype.
+// bit k of a0 / a1 is set when the pair's first / second haplotype carries a
+// non-zero allele (the PBWT's "1" side), and bit k of x when either of its
+// alleles is neither 0 nor 1 (missing, 255, or multi-allelic); such slots take
+// their allele bytes from the selection's raw table.
 struct SlotMasks {
     uint32_t a0;
     uint32_t a1;
+    uint32_t x;
+    uint32_t pad;
 };
 
 // Linear-space transition into a marker: T[i][j] = c + delta * [i == j], with
@@ -66,6 +71,7 @@ struct SelectionCache {
     DeviceBuffer pairs;  // [M][L][2] u32
     DeviceBuffer masks;  // [M] SlotMasks
     DeviceBuffer g;      // [M][fb_lmax(L)] f32 ALT allele count per slot
+    DeviceBuffer raw;    // [M][fb_lmax(L)][2] u8 allele bytes (panels with alleles other than 0/1 only)
 };
 
 }  // namespace si
@@ -84,7 +90,11 @@ struct si_ctx {
 
     // panel
     uint32_t M = 0, N = 0, W = 0;
-    si::DeviceBuffer panel;          // [M][W] u32 bit-packed
+    si::DeviceBuffer panel;          // [M][W] u32 bit-packed (bit set: non-zero allele)
+    // alleles other than 0 and 1, per marker sorted by haplotype: entry h << 8 | byte
+    si::DeviceBuffer ex_off;         // [M + 1] u64 offsets into ex_ent
+    si::DeviceBuffer ex_ent;         // [n_ex] u32
+    uint64_t n_ex = 0;
     std::vector<double> morgans;     // genetic position per marker
     bool has_map = false;
 
@@ -115,6 +125,7 @@ struct si_ctx {
     struct RegionSel {
         si::DeviceBuffer masks;
         si::DeviceBuffer g;
+        si::DeviceBuffer raw;
     };
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, RegionSel> region_sel;
     si::DeviceBuffer job_regions, job_samples;  // uploaded descriptors of the last uneven batch
@@ -145,18 +156,22 @@ bool region_first_gap_ok(const si_ctx* ctx, const si_impute_params* p, uint32_t 
 
 // Kernel launchers (pbwt_kernels.cu, select_kernels.cu, fb_kernels.cu).
 cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,
-                              uint32_t* d_bad, cudaStream_t s);
+                              cudaStream_t s);
 cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, uint32_t n_jobs, uint32_t N,
                               uint32_t W, uint32_t* d_head, uint32_t* d_prefix, unsigned long long* d_hash,
                               uint32_t* d_perm_scratch, cudaStream_t s);
 size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W);
+// Selection over markers [0, M) of the given panel rows; ex_off/ex_ent (may be
+// null) are the rows' exception lists, raw (may be null) receives allele bytes.
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
-                          uint32_t L, int kind, uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint32_t gs,
+                          uint32_t L, int kind, const unsigned long long* d_ex_off, const uint32_t* d_ex_ent,
+                          uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint8_t* d_raw, uint32_t gs,
                           cudaStream_t s);
 
 struct FbLaunch {
     const uint8_t* geno;   // [B][M]
     const SlotMasks* masks;
+    const uint8_t* raw;    // [M][fb_lmax(L)][2] allele bytes, or null (0/1 panel)
     const LinTrans* trans;
     uint32_t B, M, L, C;
     uint32_t threads;
@@ -170,7 +185,8 @@ struct FbLaunch {
 };
 cudaError_t launch_fb(const FbLaunch& a, cudaStream_t s);
 size_t fb_ckpt_bytes(uint32_t B, uint32_t M, uint32_t L, uint32_t C);
-uint32_t fb_lmax(uint32_t L);
+// slots held per thread (and the stride of per-slot tables) for L slots
+inline __host__ __device__ uint32_t fb_lmax(uint32_t L) { return L <= 4 ? 4 : L <= 8 ? 8 : L <= 16 ? 16 : 32; }
 size_t fb_smem_bytes(uint32_t L, uint32_t T, uint32_t C);
 
 }  // namespace si

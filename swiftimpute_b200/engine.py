@@ -77,6 +77,12 @@ class Engine:
         self._check(self.lib.si_panel_upload_u8(self.h, _ptr(panel), M, N_))
         self.M, self.N = M, N_
 
+    def exception_count(self) -> int:
+        """Panel entries other than 0 and 1 (missing or multi-allelic) of the uploaded panel."""
+        n = c_uint64()
+        self._check(self.lib.si_panel_exception_count(self.h, byref(n)))
+        return n.value
+
     def upload_packed(self, words: np.ndarray, n_haplotypes: int) -> None:
         words = np.ascontiguousarray(words, dtype=np.uint32)
         M, W = words.shape

@@ -65,6 +65,47 @@ def test_vcf_parse_binary_roundtrip_and_writer(api_tool, vcfs):
     assert len(lines) == 9 + panel.shape[0]
 
 
+@pytest.fixture(scope="module")
+def vcfs_other(tmp_path_factory):
+    """A panel VCF with '.' calls (ALLELE_MISSING, 255) and allele-2 calls at multi-allelic sites."""
+    d = tmp_path_factory.mktemp("vcf_other")
+    panel, pos, _ = synth.make_panel(160, 300, 10, seed=33, spacing=150)
+    codes, _, _ = synth.make_targets(panel, 9, synth.typed_every(160, 4), seed=34)
+    rng = np.random.default_rng(35)
+    u = rng.random(panel.shape)
+    panel = panel.copy()
+    panel[u < 0.01] = 255
+    panel[(u >= 0.01) & (u < 0.015)] = 2
+    write_panel_vcf(d / "ref.vcf", panel, pos)
+    write_target_vcf(d / "tgt.vcf", codes, pos)
+    return d, panel, pos, codes
+
+
+def test_vcf_panel_with_missing_and_multiallelic_calls(api_tool, vcfs_other):
+    """ReferencePanel::load_vcf keeps '.' as 255 and allele indices as they are
+    (imputer.cpp:85-112); the binary panel format carries them."""
+    d, panel, pos, codes = vcfs_other
+    r = subprocess.run([str(api_tool), "parse", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "p")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    assert "roundtrip=1" in r.stdout
+    assert np.array_equal(np.fromfile(d / "p.panel", np.uint8).reshape(panel.shape), panel)
+    assert (d / "p.sipanel").read_bytes()[:8] == b"SIPANEL2"
+
+
+@pytest.mark.gpu
+def test_imputer_with_missing_and_multiallelic_panel(api_tool, vcfs_other):
+    d, panel, pos, codes = vcfs_other
+    r = subprocess.run([str(api_tool), "impute", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "o.vcf"),
+                        str(d / "o"), "1", "8", "10000", "1"], capture_output=True, text=True)
+    assert r.returncode == 0, r.stdout + r.stderr
+    B, M = codes.shape
+    pairs = oracle.select_pairs(oracle.pbwt_build(panel), 8)
+    want = oracle.fb_batch(codes, pairs, panel, pos, 8, 10000.0)
+    assert np.abs(np.fromfile(d / "o.dosage", np.float32).reshape(B, M) - want["dosage"]).max() <= 1e-4
+    assert np.array_equal(np.fromfile(d / "o.haps", np.uint8).reshape(B, 2, M), want["haps_argmax"])
+
+
 def test_binary_loaders_refuse_damaged_files(api_tool, vcfs):
     d, panel, pos, codes = vcfs
     r = subprocess.run([str(api_tool), "parse", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "b")],

@@ -48,12 +48,24 @@ def test_pbwt_packed_upload_equals_u8(engine):
     assert np.array_equal(engine.prefix_rows(), oracle.pbwt_build(panel))
 
 
-def test_panel_rejects_non_binary_alleles(engine):
-    panel = np.zeros((4, 64), np.uint8)
-    panel[2, 5] = 255
-    with pytest.raises(N.SIError) as e:
-        engine.upload_panel(panel)
-    assert e.value.status == 4
+def with_other_alleles(panel, seed, missing=0.01, multi=0.004):
+    """A panel as a VCF with '.' calls and multi-allelic sites loads it: ALLELE_MISSING (255) and allele 2."""
+    rng = np.random.default_rng(seed)
+    out = panel.copy()
+    u = rng.random(out.shape)
+    out[u < missing] = 255
+    out[(u >= missing) & (u < missing + multi)] = 2
+    return out
+
+
+def test_pbwt_with_missing_and_multiallelic_alleles(engine):
+    # every non-zero byte goes to the "1" side (pbwt_index.cpp:183)
+    rng = np.random.default_rng(60)
+    panel = with_other_alleles((rng.random((400, 2000)) < 0.3).astype(np.uint8), 61)
+    load(engine, panel, 1 + np.arange(400, dtype=np.uint64) * 100)
+    assert engine.exception_count() == int((panel > 1).sum())
+    assert np.array_equal(engine.prefix_rows(), oracle.pbwt_build(panel))
+    assert np.array_equal(engine.row_hashes(), oracle.pbwt_build_packed(synth.pack_panel(panel != 0), 2000)[1])
 
 
 # ----------------------------------------------------------------------------- selection
@@ -139,6 +151,20 @@ def test_fb_floor_regime(engine):
     compare(engine, panel, pos, codes, 8, 10000)
     panel, pos, codes, _ = workload(3000, 300, 40, np.array([0, 5, 2990]), 30, 10)
     compare(engine, panel, pos, codes, 16, 20000)
+
+
+@pytest.mark.parametrize("L,flags", [(8, 0), (16, 0), (8, N.IMPUTE_FULL_CHAIN)])
+def test_fb_panel_with_missing_and_multiallelic_alleles(engine, L, flags):
+    # emission classes by the pair's byte sum (emission.cu:35-54), argmax
+    # haplotypes carry the panel byte (sampling.cu:121-126); dosage and
+    # P(hap=1) count non-zero alleles
+    panel, pos, codes, _ = workload(900, 700, 48, synth.typed_every(900, 4), 100, 62)
+    panel = with_other_alleles(panel, 63)
+    got, want = compare(engine, panel, pos, codes, L, 10000, flags=flags)
+    assert np.isin(got["haps"], [2, 255]).any()
+    # a 0/1 panel uploaded after it carries no exception lists
+    engine.upload_panel((panel == 1).astype(np.uint8))
+    assert engine.exception_count() == 0
 
 
 def test_fb_unmatched_calls(engine):
