@@ -60,8 +60,12 @@ enum {
 
 /* si_impute_params.flags */
 enum {
-    SI_IMPUTE_RESELECT = 1u,   /* recompute the per-marker selection tables in this call (else cached per L) */
-    SI_IMPUTE_FULL_CHAIN = 2u  /* use the marker-by-marker kernel even where the typed-marker kernel applies */
+    SI_IMPUTE_RESELECT = 1u,    /* recompute the per-marker selection tables in this call (else cached per L) */
+    SI_IMPUTE_FULL_CHAIN = 2u,  /* use the marker-by-marker kernel even where the typed-marker kernel applies */
+    /* Compact host formats of si_impute (host-buffer call only): */
+    SI_IMPUTE_CODES_2BIT = 4u,  /* geno is [B][ceil(M/4)] bytes, cell m at bits 2 (m % 4) of byte m / 4 */
+    SI_IMPUTE_HAPS_BITS = 8u    /* haps is [B][2][ceil(M/32)] u32 words, allele of marker m at bit m % 32 of
+                                   word m / 32 (set for a non-zero allele; 0/1 panels only) */
 };
 
 /* Genotype codes for si_impute: 0, 1, 2 = ALT allele count of a hard call,
@@ -160,10 +164,14 @@ si_status si_select_states(si_ctx* ctx, uint32_t L, int32_t kind, uint32_t m0, u
 si_status si_impute_params_default(si_impute_params* p);
 
 /* Impute B samples over all M markers from HOST buffers (copies inside).
- * geno [B][M] genotype codes. Outputs (each may be NULL):
+ * geno [B][M] genotype codes (with SI_IMPUTE_CODES_2BIT: [B][ceil(M/4)] bytes,
+ * four codes per byte). Outputs (each may be NULL):
  *   dosage   [B][M]     posterior ALT dosage
  *   hap_prob [B][M][2]  P(hap0 = 1), P(hap1 = 1) (ImputationResult::posteriors_, imputer.hpp:192)
- *   haps     [B][2][M]  phased alleles (ImputationResult::haplotypes_, imputer.hpp:191)
+ *   haps     [B][2][M]  phased alleles (ImputationResult::haplotypes_, imputer.hpp:191); with
+ *                       SI_IMPUTE_HAPS_BITS: [B][2][ceil(M/32)] u32 words (cast the pointer)
+ * The compact formats are converted on the device, so only their bytes cross
+ * the host link (0.5 B per cell for codes in and haplotypes out).
  * Replaces Imputer::impute_batch (imputer.cpp:787-1042): selection, emission
  * (emission.cu:208), forward/backward (forward_backward.cu:321,356) and
  * HaplotypeSampler::sample (sampling.cu:269) run as one fused device pass. */

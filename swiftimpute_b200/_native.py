@@ -25,6 +25,8 @@ PBWT_STORE_INDEX, PBWT_ROW_HASHES = 1, 2
 GENO_MISSING = 3
 IMPUTE_RESELECT = 1
 IMPUTE_FULL_CHAIN = 2
+IMPUTE_CODES_2BIT = 4
+IMPUTE_HAPS_BITS = 8
 
 
 class NativeLibraryError(RuntimeError):

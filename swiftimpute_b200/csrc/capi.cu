@@ -236,7 +236,7 @@ si_status check_params(si_ctx* ctx, const si_impute_params* p) {
         return fail(ctx, SI_ERR_INVALID_ARG, "bad sampling mode");
     if (!(p->tie_eps >= 0.0 && p->tie_eps < 1.0)) return fail(ctx, SI_ERR_INVALID_ARG, "tie_eps must be in [0, 1)");
     if (p->checkpoint_interval > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "checkpoint_interval must be <= 32");
-    if (p->flags & ~(uint32_t)(SI_IMPUTE_RESELECT | SI_IMPUTE_FULL_CHAIN))
+    if (p->flags & ~(uint32_t)(SI_IMPUTE_RESELECT | SI_IMPUTE_FULL_CHAIN | SI_IMPUTE_CODES_2BIT | SI_IMPUTE_HAPS_BITS))
         return fail(ctx, SI_ERR_INVALID_ARG, "unknown flag bits");
     if (p->block_threads && (p->block_threads % 32 || p->block_threads > 128))
         return fail(ctx, SI_ERR_UNSUPPORTED, "block_threads must be a multiple of 32, <= 128");
@@ -640,6 +640,8 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     dev_free(ctx, ctx->io_dosage);
     dev_free(ctx, ctx->io_hprob);
     dev_free(ctx, ctx->io_haps);
+    dev_free(ctx, ctx->io_geno2);
+    dev_free(ctx, ctx->io_hbits);
     for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_acode, &ctx->t_aem,
                                 &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->job_regions,
                                 &ctx->job_samples})
@@ -880,6 +882,8 @@ si_status si_impute_device(si_ctx* ctx, const si_impute_params* p, const uint8_t
     if (!ctx) return SI_ERR_INVALID_ARG;
     SI_TRY(check_params(ctx, p));
     if (!d_geno || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "geno is NULL or B == 0");
+    if (p->flags & (SI_IMPUTE_CODES_2BIT | SI_IMPUTE_HAPS_BITS))
+        return fail(ctx, SI_ERR_UNSUPPORTED, "compact formats are formats of host buffers (si_impute)");
     SI_TRY(set_device(ctx));
     cudaStream_t s = stream ? (cudaStream_t)stream : ctx->stream;
     SI_CUDA(ctx, cudaEventRecord(ctx->ev[0], s), "event");
@@ -895,6 +899,10 @@ si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno,
     SI_TRY(set_device(ctx));
     const uint32_t M = ctx->M;
     const size_t cells = (size_t)B * M;
+    const bool codes2 = (p->flags & SI_IMPUTE_CODES_2BIT) != 0, hbits = (p->flags & SI_IMPUTE_HAPS_BITS) != 0;
+    if (hbits && ctx->n_ex)
+        return fail(ctx, SI_ERR_UNSUPPORTED, "haplotype bits hold 0/1 alleles: this panel has others (use bytes)");
+    const size_t Mb = (M + 3) / 4, Mw = (M + 31) / 32;  // bytes of a 2-bit row, words of a bit row
     cudaStream_t s = ctx->stream;
     if (!ctx->copy_in) SI_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_in, cudaStreamNonBlocking), "copy stream");
     if (!ctx->copy_out) SI_CUDA(ctx, cudaStreamCreateWithFlags(&ctx->copy_out, cudaStreamNonBlocking), "copy stream");
@@ -902,11 +910,15 @@ si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno,
     if (dosage) SI_TRY(dev_reserve(ctx, ctx->io_dosage, cells * 4));
     if (hap_prob) SI_TRY(dev_reserve(ctx, ctx->io_hprob, cells * 8));
     if (haps) SI_TRY(dev_reserve(ctx, ctx->io_haps, cells * 2));
+    if (codes2) SI_TRY(dev_reserve(ctx, ctx->io_geno2, (size_t)B * Mb));
+    if (haps && hbits) SI_TRY(dev_reserve(ctx, ctx->io_hbits, (size_t)B * 2 * Mw * 4));
     // Samples in chunks of about 64 MB of codes: chunk k's codes go in on the
     // copy-in stream, it is imputed on the ctx stream, and its outputs come
     // back on the copy-out stream while chunk k+1 is imputed. A chunk keeps the
     // global sample ids of its rows, so its draws do not depend on the split.
-    const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(B, ((size_t)64 << 20) / std::max<uint32_t>(M, 1)));
+    // (64 MB of the codes as they cross the link: 2-bit rows make fewer, larger chunks)
+    const size_t row_in = codes2 ? Mb : (size_t)M;
+    const uint32_t per = (uint32_t)std::max<size_t>(1, std::min<size_t>(B, ((size_t)64 << 20) / std::max<size_t>(row_in, 1)));
     const uint32_t K = (B + per - 1) / per;
     std::vector<cudaEvent_t> ev(2 * (size_t)K + 2, nullptr);
     for (auto& x : ev) SI_CUDA(ctx, cudaEventCreateWithFlags(&x, cudaEventDefault), "event");
@@ -919,17 +931,25 @@ si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno,
     if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_in, ev[2 * K], 0);
     for (uint32_t k = 0; k < K && e == cudaSuccess; ++k) {
         const size_t r0 = (size_t)k * per, rows = std::min<size_t>(per, B - r0);
-        e = cudaMemcpyAsync((uint8_t*)ctx->io_geno.ptr + r0 * M, geno + r0 * M, rows * M, cudaMemcpyHostToDevice,
-                            ctx->copy_in);
+        if (codes2)
+            e = cudaMemcpyAsync((uint8_t*)ctx->io_geno2.ptr + r0 * Mb, geno + r0 * Mb, rows * Mb,
+                                cudaMemcpyHostToDevice, ctx->copy_in);
+        else
+            e = cudaMemcpyAsync((uint8_t*)ctx->io_geno.ptr + r0 * M, geno + r0 * M, rows * M, cudaMemcpyHostToDevice,
+                                ctx->copy_in);
         if (e == cudaSuccess) e = cudaEventRecord(ev[k], ctx->copy_in);
     }
     for (uint32_t k = 0; k < K && e == cudaSuccess && st == SI_OK; ++k) {
         const size_t r0 = (size_t)k * per, rows = std::min<size_t>(per, B - r0);
         e = cudaStreamWaitEvent(s, ev[k], 0);
+        if (e == cudaSuccess && codes2)
+            e = launch_unpack_codes((const uint8_t*)ctx->io_geno2.ptr + r0 * Mb, rows, M,
+                                    (uint8_t*)ctx->io_geno.ptr + r0 * M, s);
         if (e != cudaSuccess) break;
         if (k + 1 == K) e = cudaEventRecord(ctx->ev[0], s);  // stage timings describe the last chunk
         if (e != cudaSuccess) break;
         si_impute_params pk = *p;
+        pk.flags &= ~(uint32_t)(SI_IMPUTE_CODES_2BIT | SI_IMPUTE_HAPS_BITS);
         pk.sample_id_base = p->sample_id_base + r0;
         if (k) pk.flags &= ~(uint32_t)SI_IMPUTE_RESELECT;  // the first chunk rebuilt the selection
         st = run_device(ctx, &pk, (const uint8_t*)ctx->io_geno.ptr + r0 * M, (uint32_t)rows,
@@ -937,6 +957,10 @@ si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno,
                         hap_prob ? (float*)ctx->io_hprob.ptr + 2 * r0 * M : nullptr,
                         haps ? (uint8_t*)ctx->io_haps.ptr + 2 * r0 * M : nullptr, s);
         if (st != SI_OK) break;
+        if (haps && hbits)
+            e = launch_pack_haps((const uint8_t*)ctx->io_haps.ptr + 2 * r0 * M, 2 * rows, M,
+                                 (uint32_t*)ctx->io_hbits.ptr + 2 * r0 * Mw, s);
+        if (e != cudaSuccess) break;
         e = cudaEventRecord(ev[K + k], s);
         if (e == cudaSuccess) e = cudaStreamWaitEvent(ctx->copy_out, ev[K + k], 0);
         if (e == cudaSuccess && dosage)
@@ -945,7 +969,10 @@ si_status si_impute(si_ctx* ctx, const si_impute_params* p, const uint8_t* geno,
         if (e == cudaSuccess && hap_prob)
             e = cudaMemcpyAsync(hap_prob + 2 * r0 * M, (const float*)ctx->io_hprob.ptr + 2 * r0 * M, rows * M * 8,
                                 cudaMemcpyDeviceToHost, ctx->copy_out);
-        if (e == cudaSuccess && haps)
+        if (e == cudaSuccess && haps && hbits)
+            e = cudaMemcpyAsync(haps + 2 * r0 * Mw * 4, (const uint32_t*)ctx->io_hbits.ptr + 2 * r0 * Mw,
+                                rows * Mw * 8, cudaMemcpyDeviceToHost, ctx->copy_out);
+        else if (e == cudaSuccess && haps)
             e = cudaMemcpyAsync(haps + 2 * r0 * M, (const uint8_t*)ctx->io_haps.ptr + 2 * r0 * M, rows * M * 2,
                                 cudaMemcpyDeviceToHost, ctx->copy_out);
     }

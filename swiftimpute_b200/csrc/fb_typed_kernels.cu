@@ -632,7 +632,7 @@ __device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& t
 }
 
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
-// kFast: dosage and haplotypes are written, argmax picks, no P(hap=1).
+// kFast: argmax picks, no P(hap=1).
 template <int LM, bool kFull, bool kFast>
 __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kernel(TypedArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -672,7 +672,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     const uint32_t* pos = A.apos + ab;
     const uint32_t* aem = A.aem + ab;
     const uint8_t* ash = A.ashift + ab;
-    const bool w_dos = kFast || A.dosage != nullptr, w_hap = kFast || A.haps != nullptr;
+    const bool w_dos = A.dosage != nullptr, w_hap = A.haps != nullptr;
     const bool w_hp = !kFast && A.hprob != nullptr;
     const bool argmax = kFast || A.sampling == SI_SAMPLE_ARGMAX;
     const float keep = 1.0f - A.tie_eps;
@@ -879,7 +879,7 @@ cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
 
 template <int LM, bool kFull>
 cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
-    const bool fast = a.dosage && a.haps && !a.hprob && a.sampling == SI_SAMPLE_ARGMAX;
+    const bool fast = !a.hprob && a.sampling == SI_SAMPLE_ARGMAX;
     return fast ? launch_post_v<LM, kFull, true>(a, s) : launch_post_v<LM, kFull, false>(a, s);
 }
 

@@ -133,6 +133,7 @@ struct si_ctx {
     unsigned long long* pinned_totals_dev = nullptr;
     cudaEvent_t totals_ev = nullptr;
     si::DeviceBuffer io_geno, io_dosage, io_hprob, io_haps;  // staging for host-buffer calls
+    si::DeviceBuffer io_geno2, io_hbits;                     // compact host formats (2-bit codes, haplotype bits)
     float last_ms[3] = {0.f, 0.f, 0.f};
     bool timings_pending = false;
     void* noalloc_scratch = nullptr;  // device address of the allocation-free path's fixed array
@@ -167,6 +168,11 @@ cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint3
                           uint32_t L, int kind, const unsigned long long* d_ex_off, const uint32_t* d_ex_ent,
                           uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint8_t* d_raw, uint32_t gs,
                           cudaStream_t s);
+
+// Compact host formats (formats.cu): 2-bit codes [rows][ceil(M/4)] -> bytes
+// [rows][M]; allele bytes [rows][M] -> bit words [rows][ceil(M/32)].
+cudaError_t launch_unpack_codes(const uint8_t* d_in, uint64_t rows, uint32_t M, uint8_t* d_out, cudaStream_t s);
+cudaError_t launch_pack_haps(const uint8_t* d_in, uint64_t rows, uint32_t M, uint32_t* d_out, cudaStream_t s);
 
 struct FbLaunch {
     const uint8_t* geno;   // [B][M]

@@ -121,6 +121,25 @@ class Engine:
         return out
 
     # -- imputation ---------------------------------------------------------------
+    def impute_compact(self, codes2: np.ndarray, params: N.ImputeParams | None = None, *, dosage: bool = False):
+        """Impute from 2-bit packed codes ([B][ceil(M/4)], see pack_codes) and
+        return bit-packed haplotypes ([B][2][ceil(M/32)] u32, see unpack_hap_bits)
+        and, when asked, the dosage."""
+        params = params or N.default_params()
+        p = N.ImputeParams.from_buffer_copy(params)
+        p.flags |= N.IMPUTE_CODES_2BIT | N.IMPUTE_HAPS_BITS
+        codes2 = np.ascontiguousarray(codes2, dtype=np.uint8)
+        if codes2.ndim != 2 or codes2.shape[1] != (self.M + 3) // 4:
+            raise ValueError(f"codes must have shape [B][{(self.M + 3) // 4}]")
+        B = codes2.shape[0]
+        bits = np.empty((B, 2, (self.M + 31) // 32), np.uint32)
+        d = np.empty((B, self.M), np.float32) if dosage else None
+        self._check(self.lib.si_impute(self.h, byref(p), _ptr(codes2), B, _ptr(d), None, _ptr(bits)))
+        out = {"hap_bits": bits}
+        if dosage:
+            out["dosage"] = d
+        return out
+
     def impute(self, geno: np.ndarray, params: N.ImputeParams | None = None, *, dosage: bool = True,
                hap_prob: bool = False, haps: bool = True, gl: bool = False):
         """Impute rows of ``geno`` ([B][M] codes, or [B][M][3] log10 GL when gl=True).
@@ -368,3 +387,20 @@ class Plan:
         if getattr(self, "h", None):
             self.lib.si_plan_destroy(self.h)
             self.h = None
+
+
+def pack_codes(codes: np.ndarray) -> np.ndarray:
+    """[B][M] genotype codes (0..3) -> [B][ceil(M/4)] bytes, cell m at bits 2 (m % 4) of byte m / 4."""
+    codes = np.asarray(codes, dtype=np.uint8)
+    B, M = codes.shape
+    pad = np.zeros((B, 4 * ((M + 3) // 4)), np.uint8)
+    pad[:, :M] = codes & 3
+    q = pad.reshape(B, -1, 4)
+    return (q[..., 0] | (q[..., 1] << 2) | (q[..., 2] << 4) | (q[..., 3] << 6)).astype(np.uint8)
+
+
+def unpack_hap_bits(bits: np.ndarray, M: int) -> np.ndarray:
+    """[B][2][ceil(M/32)] u32 words -> [B][2][M] alleles (0/1)."""
+    bits = np.asarray(bits, dtype=np.uint32)
+    b = np.unpackbits(bits.view(np.uint8).reshape(bits.shape[:-1] + (-1,)), axis=-1, bitorder="little")
+    return b[..., :M].astype(np.uint8)

@@ -167,6 +167,27 @@ def test_fb_panel_with_missing_and_multiallelic_alleles(engine, L, flags):
     assert engine.exception_count() == 0
 
 
+def test_compact_host_formats(engine):
+    # 2-bit codes in and haplotype bits out give the byte path's results bit for bit
+    from swiftimpute_b200.engine import pack_codes, unpack_hap_bits
+    panel, pos, codes, _ = workload(700, 500, 40, synth.typed_every(700, 5), 100, 70)
+    load(engine, panel, pos, store=False)
+    p = N.default_params()
+    full = engine.impute(codes, p)
+    got = engine.impute_compact(pack_codes(codes), p, dosage=True)
+    assert np.array_equal(unpack_hap_bits(got["hap_bits"], 700), full["haps"])
+    assert np.array_equal(got["dosage"], full["dosage"])
+    only = engine.impute_compact(pack_codes(codes), p)
+    assert np.array_equal(only["hap_bits"], got["hap_bits"])
+    # a panel with alleles other than 0/1 needs the byte output
+    engine.upload_panel(with_other_alleles(panel, 71))
+    engine.set_map(pos)
+    engine.pbwt_build()
+    with pytest.raises(N.SIError) as e:
+        engine.impute_compact(pack_codes(codes), p)
+    assert e.value.status == 4
+
+
 def test_fb_unmatched_calls(engine):
     # typed calls that no selected pair can produce scale every slot alike
     panel, pos, codes, _ = workload(400, 256, 20, synth.typed_every(400, 2), 120, 11)
