@@ -262,7 +262,8 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
 
 template <int LM>
 size_t smem_bytes(uint32_t T, uint32_t C) {
-    return (size_t)C * LM * T * 4 + (size_t)T * (C + 1) * 4 + (size_t)T * (2 * C + 1) * 4 + (size_t)C * 16 +
+    return (size_t)C * LM * T * 4 + (size_t)T * (C + 1) * 4 + (size_t)T * (2 * C + 1) * 4 +
+           (size_t)C * (sizeof(SlotMasks) + sizeof(LinTrans)) +
            (size_t)T * (C + 4) + (size_t)T * 2 * (C + 4) + 16;
 }
 
