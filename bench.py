@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--e2e-steps", type=int, default=3)
     ap.add_argument("--cpu-seconds", type=float, default=12.0)
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-legs", action="store_true", help="skip the uneven-batch, large-panel and serving keys")
+    ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving key: length of the arrival window")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: request arrivals per second")
     ap.add_argument("--seconds", type=float, default=0.0, help="serving: length of the arrival window")
     return ap.parse_args()
@@ -377,6 +379,259 @@ def run_serving(args, cfg):
     print(json.dumps(line), flush=True)
 
 
+# ---------------------------------------------------------------- extra legs (N = 1)
+#
+# The other BASELINE workloads, timed on the same GPU after the headline and
+# added to the line as extra keys: the uneven batch in one graph-captured,
+# autotuned plan launch; the large panel (PBWT build time and imputation);
+# the serving loop at 200 requests/s for 60 s beside the reference's own path
+# run one request at a time. Panels and targets are generated on the device
+# (swiftimpute_b200.synth_device): a host generator would take minutes.
+
+def _events_ms(fn, steps, stream):
+    """Mean milliseconds of fn() over `steps` launches, CUDA events on `stream`."""
+    import torch
+    a, b = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    torch.cuda.synchronize()
+    a.record(stream)
+    for _ in range(steps):
+        fn()
+    b.record(stream)
+    torch.cuda.synchronize()
+    return a.elapsed_time(b) / steps
+
+
+def uneven_panel(local, seed=2):
+    """The uneven-batch panel: 8,000 x 120,000, MAF ~ Beta(0.3, 0.6), switch 0.002, 0.5 cM map."""
+    import torch
+    from swiftimpute_b200 import synth_device
+    M, Nh = 120_000, 8000
+    panel = synth_device.make_panel(M, Nh, 200, (0.3, 0.6), 0.002, 0.005, seed=seed, device=torch.device("cuda", local))
+    pos = (1 + np.arange(M, dtype=np.uint64) * np.uint64(500_000)).astype(np.uint64)
+    return panel, pos
+
+
+def leg_uneven(local, steps, peak, panel, pos):
+    """4,096 targets over 64 regions (500-20,000 markers, log-uniform; uniform
+    start), L in {4, 8, 16} per region, typed every 5th marker, each region
+    indexed from its own first marker; one autotuned plan, graph-launched."""
+    import torch
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200 import synth_device
+    from swiftimpute_b200.engine import Engine
+    M = panel.shape[0]
+    rng = np.random.default_rng(2)
+    regions = []
+    for _ in range(64):
+        length = int(np.exp(rng.uniform(np.log(500), np.log(20_000))))
+        m0 = int(rng.integers(0, M - length))
+        regions.append((m0, m0 + length, int(rng.choice([4, 8, 16])), N.INDEX_REGION))
+    assign = rng.integers(0, 64, size=4096)
+    per_region = {}
+    for r, (m0, m1, _, _) in enumerate(regions):
+        n = int((assign == r).sum())
+        if n:
+            per_region[r] = synth_device.make_targets(panel[m0:m1].contiguous(), n, 5, seed=100 + r).cpu().numpy()
+    jobs, seen = [], {r: 0 for r in per_region}
+    for j, r in enumerate(assign):
+        r = int(r)
+        jobs.append((r, per_region[r][seen[r]], j))
+        seen[r] += 1
+    cells = sum(len(c) for _, c, _ in jobs)
+    masked = sum(int((c == 3).sum()) for _, c, _ in jobs)
+    with Engine(local) as eng:
+        eng.upload_panel(panel.cpu().numpy())
+        eng.set_map(pos)
+        t0 = time.perf_counter()
+        plan = eng.plan(regions, jobs, N.default_params(), autotune=True)
+        create_s = time.perf_counter() - t0
+        stream = torch.cuda.Stream(torch.device("cuda", local))
+        plan.launch(graph=True, stream=stream.cuda_stream)
+        ms = _events_ms(lambda: plan.launch(graph=True, stream=stream.cuda_stream), steps, stream)
+        plan.check()
+        info = plan.info()
+        plan.destroy()
+    achieved = ALGO_BYTES_PER_CELL * cells / (ms / 1e3) / 1e9
+    return {"workload": "uneven batch: 8000 haplotypes x 120000 markers, 4096 targets over 64 regions of "
+                        "500-20000 markers, L in {4, 8, 16}, typed every 5th, region-local index",
+            "value": masked / (ms / 1e3), "unit": "imputed genotypes/s", "ms_per_launch": ms,
+            "cells": int(cells), "imputed_cells": int(masked), "launch": "one CUDA graph (4 kernels), autotuned plan",
+            "autotuned": info, "plan_create_s": create_s,
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "note": "7 B per cell over the graph launch"}}
+
+
+def leg_large_panel(local, steps, peak):
+    """100,000 x 100,000 panel (1-bit packed on the device), 50,000 targets
+    typed every 20th marker, L = 16, 0.5 cM map: PBWT build and imputation."""
+    import torch
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200 import synth_device
+    from swiftimpute_b200.engine import Engine
+    dev = torch.device("cuda", local)
+    M = Nh = 100_000
+    B, L = 50_000, 16
+    panel = synth_device.make_panel(M, Nh, 500, (0.5, 0.5), 0.001, 0.005, seed=3, device=dev)
+    words = synth_device.pack_panel(panel)
+    codes = synth_device.make_targets(panel, B, 20, seed=3)
+    del panel
+    torch.cuda.empty_cache()
+    pos = (1 + np.arange(M, dtype=np.uint64) * np.uint64(500_000)).astype(np.uint64)
+    out = {}
+    with Engine(local) as eng:
+        eng.upload_packed(words, Nh)
+        eng.set_map(pos)
+        out["pbwt_build_ms"] = eng.pbwt_build()
+        params = N.default_params(num_states=L, ne=10_000)
+        dos = torch.empty((B, M), dtype=torch.float32, device=dev)
+        haps = torch.empty((B, 2, M), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.Stream(dev)
+
+        def step():
+            eng.impute_device(codes.data_ptr(), B, params, dos.data_ptr(), None, haps.data_ptr(), stream.cuda_stream)
+        step()
+        torch.cuda.synchronize(dev)
+        kms = []
+
+        def timed():
+            step()
+            kms.append(eng.last_kernel_ms())
+        ms = _events_ms(timed, steps, stream)
+        kavg = [sum(k[i] for k in kms) / len(kms) for i in range(4)]
+        typed = (M + 19) // 20
+        masked = B * (M - typed)
+        post = POST_BYTES_PER_CELL * B * M / (kavg[3] / 1e3) / 1e9
+        out.update({
+            "workload": "large panel: 100000 haplotypes x 100000 markers, 50000 targets typed every 20th, L=16",
+            "value": masked / (ms / 1e3), "unit": "imputed genotypes/s", "ms_per_step": ms,
+            "kernels_ms": dict(zip(KERNELS, kavg)),
+            "roofline": {"bound": "hbm", "kernel": "anchor_posterior_kernel", "achieved": post, "peak": peak,
+                         "unit": "GB/s", "frac": post / peak, "note": "6 B per cell written"},
+            "step_roofline_frac": ALGO_BYTES_PER_CELL * B * M / (ms / 1e3) / 1e9 / peak})
+        del dos, haps, codes
+    torch.cuda.empty_cache()
+    return out
+
+
+def serving_requests(M, pool, rate, seconds, seed):
+    """Poisson arrivals; each request 1-512 samples (log-uniform) over
+    1,000-50,000 markers (log-uniform length, uniform start), L from {4, 8, 16}."""
+    rng = np.random.default_rng(seed)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, size=int(rate * seconds * 1.5) + 16))
+    arrivals = arrivals[arrivals < seconds]
+    reqs = []
+    for _ in range(len(arrivals)):
+        n = int(np.exp(rng.uniform(0, np.log(512))))
+        length = int(np.exp(rng.uniform(np.log(1000), np.log(50_000))))
+        m0 = int(rng.integers(0, M - length))
+        rows = rng.integers(0, pool.shape[0], size=n)
+        reqs.append((m0, m0 + length, int(rng.choice([4, 8, 16])), np.ascontiguousarray(pool[rows, m0:m0 + length])))
+    return arrivals, reqs
+
+
+def serve_replay(eng, params, arrivals, reqs, max_batch_requests=0):
+    """Replay the arrivals through a server; returns (statistics, wall seconds)."""
+    import threading
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200.engine import Server
+    outs = [{"dosage": np.zeros(r[3].shape, np.float32), "haps": np.zeros((r[3].shape[0], 2, r[3].shape[1]), np.uint8)}
+            for r in reqs]
+    srv = Server(eng, params, max_batch_requests=max_batch_requests)
+    tickets = [None] * len(reqs)
+    t0 = time.perf_counter()
+
+    def submitter():
+        for i, (a, b, L, codes) in enumerate(reqs):
+            d = t0 + arrivals[i] - time.perf_counter()
+            if d > 0:
+                time.sleep(d)
+            tickets[i] = srv.submit(a, b, codes, num_states=L, index_origin=N.INDEX_GLOBAL,
+                                    sample_id_base=i << 10, out=outs[i])
+
+    th = threading.Thread(target=submitter)
+    th.start()
+    th.join()
+    for t in tickets:
+        srv.wait(t)
+    wall = time.perf_counter() - t0
+    st = srv.stats()
+    srv.stop()
+    return st, wall
+
+
+def reference_plain_serving(panel_host, pos, arrivals, reqs, ne, budget_s):
+    """The reference's own path, one request at a time (Imputer::impute_batch
+    steps with window_size = 0 on the request's region-sliced panel: CPU PBWT
+    build, selection, emission, forward-backward, sampler), compiled from its
+    sources (oracle/_ref). The first requests in arrival order are replayed
+    sequentially until `budget_s` of work; latency = finish - arrival."""
+    import oracle
+    if not oracle.ref_gpu_available():
+        return {"unavailable": "oracle/_ref/libref_gpu.so is not built"}
+    done, lat, cells, masked = 0, [], 0, 0
+    t_start = time.perf_counter()
+    finish = 0.0
+    for i, (m0, m1, L, codes) in enumerate(reqs):
+        if time.perf_counter() - t_start > budget_s:
+            break
+        gl = oracle.codes_to_gl(codes)
+        t0 = time.perf_counter()
+        oracle.ref_gpu_impute(panel_host[m0:m1], pos[m0:m1], gl, L, ne, want_logpost=False)
+        service = time.perf_counter() - t0
+        finish = max(arrivals[i], finish) + service
+        lat.append(finish - arrivals[i])
+        cells += codes.size
+        masked += int((codes == 3).sum())
+        done += 1
+    busy = time.perf_counter() - t_start
+    lat_ms = np.array(lat) * 1e3
+    return {"requests": done, "of": len(reqs), "imputed_genotypes_per_s": masked / busy,
+            "cells_per_s": cells / busy,
+            "latency_ms": {"p50": float(np.percentile(lat_ms, 50)), "p99": float(np.percentile(lat_ms, 99)),
+                           "max": float(lat_ms.max())},
+            "offered_load_fraction": (sum(r[3].size for r in reqs) / arrivals[-1]) / (cells / busy),
+            "note": "sequential per-request runs of the reference's path on the same GPU; latencies of the first "
+                    "requests in arrival order (a queue that never drains has latencies growing with the run)"}
+
+
+def leg_serving(local, peak, panel, pos, rate=200.0, seconds=60.0, ref_budget_s=20.0):
+    """Serving at `rate` requests/s for `seconds` over the uneven-batch panel
+    with its resident index, under a 120 GB HBM budget."""
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200 import synth_device
+    from swiftimpute_b200.engine import Engine, Server
+    M = panel.shape[0]
+    pool = synth_device.make_targets(panel, 1024, 20, seed=5).cpu().numpy()
+    panel_host = panel.cpu().numpy()
+    arrivals, reqs = serving_requests(M, pool, rate, seconds, seed=6)
+    cells = sum(r[3].size for r in reqs)
+    masked = sum(int((r[3] == 3).sum()) for r in reqs)
+    params = N.default_params(ne=20_000)
+    with Engine(local, hbm_budget_bytes=120 << 30) as eng:
+        eng.upload_panel(panel_host)
+        eng.set_map(pos)
+        eng.pbwt_build()
+        with Server(eng, params) as srv:  # warm-up: tables, selections, scratch at full size
+            for L in (4, 8, 16):
+                srv.wait(srv.submit(0, 50_000, pool[:512, :50_000], num_states=L, index_origin=N.INDEX_GLOBAL))
+        st, wall = serve_replay(eng, params, arrivals, reqs)
+    busy_s = st["busy_ms"] / 1e3
+    ref = reference_plain_serving(panel_host, pos, arrivals, reqs, 20_000, ref_budget_s)
+    return {"workload": f"serving: 8000 haplotypes x {M} markers, resident index, Poisson {rate:g} req/s for "
+                        f"{seconds:g} s, 1-512 samples x 1000-50000 markers, typed every 20th, L in {{4, 8, 16}}, "
+                        "120 GB HBM budget",
+            "requests": len(reqs), "completed": st["completed"], "failed": st["failed"],
+            "imputed_genotypes_per_s": masked / wall, "cells_per_s": st["cells"] / wall,
+            "offered_imputed_genotypes_per_s": masked / seconds,
+            "latency_ms": {"p50": st["latency_p50_ms"], "p99": st["latency_p99_ms"], "max": st["latency_max_ms"]},
+            "busy_fraction": busy_s / wall, "launches": st["batches"],
+            "busy_roofline": {"bound": "hbm", "achieved": ALGO_BYTES_PER_CELL * st["cells"] / busy_s / 1e9,
+                              "peak": peak, "unit": "GB/s",
+                              "frac": ALGO_BYTES_PER_CELL * st["cells"] / busy_s / 1e9 / peak,
+                              "note": "7 B per cell over the worker's busy time (host copies included)"},
+            "reference_plain_per_request": ref}
+
+
 def run_ours(args, cfg):
     import torch
     from swiftimpute_b200 import _native as N
@@ -534,6 +789,26 @@ def run_ours(args, cfg):
                                                             gpu_dosage=dos, gpu_haps=d_haps.cpu().numpy())
         line["pbwt_cpu_reference"] = pbwt_reference_time(panel)
     eng.close()
+    if world == 1 and not args.no_legs and args.config == "dense-cohort":
+        del d_geno, d_dos, d_haps, h_geno, h_dos, h_haps, h_codes2, h_bits
+        torch.cuda.empty_cache()
+        legs = [("uneven_batch", lambda up: leg_uneven(local, max(3, args.steps), peak, *up)),
+                ("serving", lambda up: leg_serving(local, peak, *up, seconds=args.serve_seconds)),
+                ("large_panel", lambda up: leg_large_panel(local, max(3, args.steps // 2), peak))]
+        up = None
+        for name, fn in legs:
+            try:
+                if up is None and name != "large_panel":
+                    up = uneven_panel(local)
+                if name == "large_panel" and up is not None:
+                    up = None
+                    torch.cuda.empty_cache()
+                t0 = time.perf_counter()
+                line[name] = fn(up)
+                line[name]["leg_wall_s"] = time.perf_counter() - t0
+            except Exception as e:  # noqa: BLE001 - a failed leg is reported, the headline stands
+                line[name] = {"error": f"{type(e).__name__}: {e}"}
+            print(f"[bench] {name} done", file=sys.stderr, flush=True)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()

@@ -632,9 +632,10 @@ __device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& t
 }
 
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
-// kFast: argmax picks, no P(hap=1).
-template <int LM, bool kFull, bool kFast>
-__global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kernel(TypedArgs A) {
+// kFast: argmax picks, no P(hap=1). kPlain: every sample covers the whole
+// panel with the launch's one region (read from the kernel parameters).
+template <int LM, bool kFull, bool kFast, bool kPlain>
+__global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kernel(const __grid_constant__ TypedArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr uint32_t Q4 = LM / 4;
     constexpr uint32_t kAll = 0xffffffffu;
@@ -657,7 +658,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     uint32_t NA = 0;
     unsigned long long ab = 0, wb = 0;
     if (live) {
-        v = view_of(A, s);
+        if (!kPlain) v = view_of(A, s);
         NA = A.counts[s];
         ab = A.aoff[s];
         wb = A.woff[s];
@@ -668,7 +669,10 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     live = live && w0 < wend;
     if (!__any_sync(kAll, live)) return;  // whole warp
 
-    const Tabs& tb = v.r.tabs;
+    const TypedRegion& R = kPlain ? A.reg0 : v.r;
+    const uint32_t len = kPlain ? A.M : len;
+    const unsigned long long out = kPlain ? (unsigned long long)s * A.M : v.out;
+    const Tabs& tb = R.tabs;
     const uint32_t* pos = A.apos + ab;
     const uint32_t* aem = A.aem + ab;
     const uint8_t* ash = A.ashift + ab;
@@ -678,7 +682,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     const float keep = 1.0f - A.tie_eps;
     float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
     {
-        const uint32_t lmask = lmask_of(v.r.L);
+        const uint32_t lmask = lmask_of(R.L);
 #pragma unroll
         for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
     }
@@ -707,10 +711,10 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
 #pragma unroll
         for (int l = 0; l < LM; ++l) ap[l] *= inv;
         p0 = pos[k];
-        p1 = k + 1 < NA ? pos[k + 1] : v.len;
-        mend = wend * C < NA ? pos[wend * C] : v.len;
+        p1 = k + 1 < NA ? pos[k + 1] : len;
+        mend = wend * C < NA ? pos[wend * C] : len;
         m = p0;
-        rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, v.len, w0, recW, recF, lane);
+        rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, len, w0, recW, recF, lane);
         load_record(0);
     }
     bool in_tab = p1 - p0 < tb.NT;  // every i, j of the run index the tables
@@ -719,9 +723,9 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     uint32_t tstart = m, tcnt = 0;
     auto flush = [&]() {
         __syncwarp();
-        const unsigned long long od = v.out + tstart, oh = 2ull * v.out + tstart;
+        const unsigned long long od = out + tstart, oh = 2ull * out + tstart;
         meta[lane] = make_uint4((uint32_t)od, (uint32_t)(od >> 32), (uint32_t)oh, (uint32_t)(oh >> 32));
-        meta[32 + lane] = make_uint4(v.len, live ? tcnt : 0u, 0u, 0u);
+        meta[32 + lane] = make_uint4(len, live ? tcnt : 0u, 0u, 0u);
         __syncwarp();
         for (uint32_t r = 0; r < 32; ++r) {
             const uint4 m1 = meta[32 + r];
@@ -750,7 +754,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
         if (on && m == p1) {
             // anchor k + 1: alpha steps over the run and takes its emission
             const uint32_t kn = k + 1, n = p1 - p0;
-            if (kn % C == 0) rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, v.len, kn / C, recW, recF, lane);
+            if (kn % C == 0) rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, len, kn / C, recW, recF, lane);
             const float2 qs = tabQS(tb, n);
             const float base = vsum<LM>(ap) * qs.y;
             const uint32_t em = aem[kn];
@@ -762,7 +766,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
             load_record(kn % C);
             k = kn;
             p0 = p1;
-            p1 = kn + 1 < NA ? pos[kn + 1] : v.len;
+            p1 = kn + 1 < NA ? pos[kn + 1] : len;
             in_tab = p1 - p0 < tb.NT;
         }
         const bool all_tab = __all_sync(kAll, !on || in_tab);
@@ -792,7 +796,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
             }
             const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
             const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
-            const float4* gr = reinterpret_cast<const float4*>(v.r.g + (size_t)m * v.r.gs);
+            const float4* gr = reinterpret_cast<const float4*>(R.g + (size_t)m * R.gs);
             float p[LM];
             float2 tot2 = make_float2(0.f, 0.f), d2 = tot2;
 #pragma unroll
@@ -807,14 +811,14 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
                 }
                 p[4 * q] = p01.x; p[4 * q + 1] = p01.y; p[4 * q + 2] = p23.x; p[4 * q + 3] = p23.y;
                 tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
-                if (kFull || 4 * q < v.r.gs) {
+                if (kFull || 4 * q < R.gs) {
                     const float4 gv = __ldg(gr + q);
                     d2 = __ffma2_rn(p01, make_float2(gv.x, gv.y), d2);
                     d2 = __ffma2_rn(p23, make_float2(gv.z, gv.w), d2);
                 }
             }
             const float tot = tot2.x + tot2.y;
-            const SlotMasks mk = v.r.masks[m];
+            const SlotMasks mk = R.masks[m];
             uint32_t pick;
             if (argmax) {
                 const float thr = vmax<LM>(p) * keep;
@@ -823,7 +827,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
                 for (int l = LM - 1; l >= 1; --l) pick = (p[l] >= thr) ? (uint32_t)l : pick;
                 if (p[0] >= thr) pick = 0;
             } else {
-                const float target = cell_uniform(A.seed, v.sid, v.m0 + m) * tot;
+                const float target = cell_uniform(A.seed, kPlain ? A.sid_base + s : v.sid, (kPlain ? 0u : v.m0) + m) * tot;
                 float cum = 0.f;
                 uint32_t last_nz = 0;
                 pick = LM;
@@ -837,7 +841,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
             }
             const float inv = rcp_approx(tot);
             tD[lane * 33 + col] = (d2.x + d2.y) * inv;
-            tH[lane * 34 + col] = (uint16_t)slot_alleles(mk, v.r.raw, v.r.gs, m, pick);
+            tH[lane * 34 + col] = (uint16_t)slot_alleles(mk, R.raw, R.gs, m, pick);
             if (w_hp) {
                 float q0 = 0.f, q1 = 0.f;
 #pragma unroll
@@ -855,7 +859,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     flush();
 }
 
-template <int LM, bool kFull, bool kFast>
+template <int LM, bool kFull, bool kFast, bool kPlain>
 cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     const uint32_t T = a.threads;
     const size_t sm = (size_t)(T / 32) * post_warp_bytes(LM, a.C, !kFast);
@@ -864,7 +868,7 @@ cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     cudaError_t e = cudaStreamIsCapturing(s, &cs);
     if (e != cudaSuccess) return e;
     if (cs == cudaStreamCaptureStatusNone) {
-        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull, kFast>,
+        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull, kFast, kPlain>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
@@ -873,14 +877,16 @@ cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     const unsigned long long grid = (warps + T / 32 - 1) / (T / 32);
     if (grid == 0) return cudaSuccess;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    anchor_posterior_kernel<LM, kFull, kFast><<<(uint32_t)grid, T, sm, s>>>(a);
+    anchor_posterior_kernel<LM, kFull, kFast, kPlain><<<(uint32_t)grid, T, sm, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int LM, bool kFull>
 cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
     const bool fast = !a.hprob && a.sampling == SI_SAMPLE_ARGMAX;
-    return fast ? launch_post_v<LM, kFull, true>(a, s) : launch_post_v<LM, kFull, false>(a, s);
+    if (!a.samples)
+        return fast ? launch_post_v<LM, kFull, true, true>(a, s) : launch_post_v<LM, kFull, false, true>(a, s);
+    return fast ? launch_post_v<LM, kFull, true, false>(a, s) : launch_post_v<LM, kFull, false, false>(a, s);
 }
 
 template <int LM>

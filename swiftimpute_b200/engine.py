@@ -357,9 +357,9 @@ class Plan:
         self.d_geno[: flat.size].copy_(torch.from_numpy(flat))
         torch.cuda.synchronize(self.d_geno.device)
 
-    def launch(self, graph: bool = False) -> None:
+    def launch(self, graph: bool = False, stream: int | None = None) -> None:
         fn = self.lib.si_plan_graph_launch if graph else self.lib.si_plan_launch
-        self.engine._check(fn(self.h, None))
+        self.engine._check(fn(self.h, c_void_p(stream) if stream else None))
 
     def check(self) -> None:
         self.engine._check(self.lib.si_plan_check(self.h))

@@ -30,63 +30,19 @@ NE = 10_000
 EVERY = 20
 
 
-def _panel(dev, seed=3, founders=500, switch=0.001, flip=0.005, chunk=2048):
-    import torch
-    rng = np.random.default_rng(seed)
-    p = rng.beta(0.5, 0.5, size=M)
-    fnd = torch.from_numpy((rng.random((founders, M)) < p[None, :]).astype(np.uint8)).to(dev)
-    g = torch.Generator(device=dev).manual_seed(seed)
-    panel = torch.empty((M, NH), dtype=torch.uint8, device=dev)
-    carry = torch.randint(0, founders, (NH,), generator=g, device=dev)
-    for m0 in range(0, M, chunk):
-        c = min(M, m0 + chunk) - m0
-        ar = torch.arange(c, device=dev)[:, None]
-        sw = torch.rand((c, NH), generator=g, device=dev) < switch
-        new = torch.randint(0, founders, (c, NH), generator=g, device=dev)
-        last = torch.cummax(torch.where(sw, ar, torch.full_like(ar, -1)).expand(c, NH), dim=0).values
-        idx = torch.where(last >= 0, torch.gather(new, 0, last.clamp(min=0)), carry[None, :])
-        carry = idx[-1].clone()
-        alle = fnd[idx, (m0 + ar).expand(c, NH)]
-        alle ^= (torch.rand((c, NH), generator=g, device=dev) < flip).to(torch.uint8)
-        panel[m0:m0 + c] = alle
-    return panel
+def _panel(dev):
+    from swiftimpute_b200 import synth_device
+    return synth_device.make_panel(M, NH, 500, (0.5, 0.5), 0.001, 0.005, seed=3, device=dev)
 
 
-def _pack(panel, chunk=1024):
-    import torch
-    W = NH // 32
-    shifts = torch.arange(32, device=panel.device, dtype=torch.int64)
-    out = np.empty((M, W), dtype=np.uint32)
-    for m0 in range(0, M, chunk):
-        rows = panel[m0:m0 + chunk].view(-1, W, 32).to(torch.int64)
-        words = (rows << shifts).sum(-1)  # distinct bits: the sum is the 32-bit word
-        out[m0:m0 + chunk] = words.cpu().numpy().astype(np.uint32)
-    return out
+def _pack(panel):
+    from swiftimpute_b200 import synth_device
+    return synth_device.pack_panel(panel)
 
 
-def _targets(panel, seed=3, n_mosaic=8, switch=0.005, chunk=1024):
-    """codes [B][M] u8 on the device: h0 + h1 at typed markers, 3 elsewhere."""
-    import torch
-    dev = panel.device
-    g = torch.Generator(device=dev).manual_seed(seed + 1000)
-    H = 2 * B
-    src = torch.randint(0, NH, (H, n_mosaic), generator=g, device=dev)
-    codes = torch.full((B, M), 3, dtype=torch.uint8, device=dev)
-    carry = torch.randint(0, n_mosaic, (H,), generator=g, device=dev)
-    for m0 in range(0, M, chunk):
-        c = min(M, m0 + chunk) - m0
-        ar = torch.arange(c, device=dev)[:, None]
-        sw = torch.rand((c, H), generator=g, device=dev) < switch
-        new = torch.randint(0, n_mosaic, (c, H), generator=g, device=dev)
-        last = torch.cummax(torch.where(sw, ar, torch.full_like(ar, -1)).expand(c, H), dim=0).values
-        k = torch.where(last >= 0, torch.gather(new, 0, last.clamp(min=0)), carry[None, :])
-        carry = k[-1].clone()
-        hap = torch.gather(src.t(), 0, k)                   # [c][H] panel haplotype per marker
-        alle = torch.gather(panel[m0:m0 + c], 1, hap)       # [c][H]
-        geno = alle[:, 0::2] + alle[:, 1::2]                # [c][B]
-        typed = ((m0 + ar) % EVERY == 0).expand(c, B)
-        codes[:, m0:m0 + c] = torch.where(typed, geno, torch.full_like(geno, 3)).t()
-    return codes
+def _targets(panel):
+    from swiftimpute_b200 import synth_device
+    return synth_device.make_targets(panel, B, EVERY, seed=3)
 
 
 @pytest.fixture(scope="module")
