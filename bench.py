@@ -49,6 +49,7 @@ CONFIGS = {
     "serving": dict(M=120_000, N=8000, founders=200, beta=(0.3, 0.6), switch=0.002, every=20, ne=20000, seed=4,
                     pool=1024, rate=200.0, seconds=10.0, hbm_budget=120 << 30),
 }
+LEGS = ["dense_map", "uneven_batch", "serving", "large_panel"]
 ALGO_BYTES_PER_CELL = 7  # 1 B genotype code in, 4 B dosage + 2 B haplotype alleles out
 POST_BYTES_PER_CELL = 6  # the posterior pass writes the outputs: 4 B dosage + 2 B alleles
 KERNELS = ["select_kernel", "anchor_lists (count+scan+fill)", "anchor_chain_kernel", "anchor_posterior_kernel"]
@@ -68,6 +69,7 @@ def parse():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-legs", action="store_true", help="skip the uneven-batch, large-panel and serving keys")
     ap.add_argument("--serve-seconds", type=float, default=60.0, help="serving key: length of the arrival window")
+    ap.add_argument("--leg", choices=LEGS, default=None, help="run one extra key alone and print its JSON")
     ap.add_argument("--rate", type=float, default=0.0, help="serving: request arrivals per second")
     ap.add_argument("--seconds", type=float, default=0.0, help="serving: length of the arrival window")
     return ap.parse_args()
@@ -399,6 +401,65 @@ def _events_ms(fn, steps, stream):
     b.record(stream)
     torch.cuda.synchronize()
     return a.elapsed_time(b) / steps
+
+
+def leg_dense_map(local, steps, peak, cpu_targets=1024):
+    """The dense-cohort shape on a map with memory (markers 1 kb apart, so the
+    transition is not the memoryless one of the 0.5 cM map): the step timed as
+    the headline, and the first `cpu_targets` targets against the FP64 oracle."""
+    import torch
+    import oracle
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200 import synth, synth_device
+    from swiftimpute_b200.engine import Engine
+    dev = torch.device("cuda", local)
+    M, Nh, B, L, NE = 50_000, 4432, 10_000, 8, 20_000
+    panel_d = synth_device.make_panel(M, Nh, 100, seed=11, device=dev)
+    typed = synth.typed_evenly(M, 3000)
+    codes = synth_device.make_targets(panel_d, B, typed=typed, seed=11)
+    panel = panel_d.cpu().numpy()
+    del panel_d
+    pos = (1 + np.arange(M, dtype=np.uint64) * np.uint64(1000)).astype(np.uint64)
+    with Engine(local) as eng:
+        eng.upload_panel(panel)
+        eng.set_map(pos)
+        eng.pbwt_build()
+        params = N.default_params(num_states=L, ne=NE)
+        dos = torch.empty((B, M), dtype=torch.float32, device=dev)
+        haps = torch.empty((B, 2, M), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.Stream(dev)
+        kms = []
+
+        def step():
+            eng.impute_device(codes.data_ptr(), B, params, dos.data_ptr(), None, haps.data_ptr(), stream.cuda_stream)
+            kms.append(eng.last_kernel_ms())
+        step()
+        kms.clear()
+        ms = _events_ms(step, steps, stream)
+        kavg = [sum(k[i] for k in kms) / len(kms) for i in range(4)]
+        pairs = eng.select_states(L)
+        c = codes[:cpu_targets].cpu().numpy()
+        got_d, got_h = dos[:cpu_targets].cpu().numpy(), haps[:cpu_targets].cpu().numpy()
+    del dos, haps, codes
+    torch.cuda.empty_cache()
+    threads = os.cpu_count() or 1
+    t0 = time.perf_counter()
+    want = oracle.fb_batch(c, pairs, panel, pos, L, float(NE), threads=threads)
+    cpu_s = time.perf_counter() - t0
+    masked = c == 3
+    x, y = got_d[masked].astype(np.float64), want["dosage"][masked].astype(np.float64)
+    post = POST_BYTES_PER_CELL * B * M / (kavg[3] / 1e3) / 1e9
+    return {"workload": "dense cohort on a 1 kb map: 4432 haplotypes x 50000 markers, 10000 targets typed at "
+                        "3000 markers, L=8, Ne=20000",
+            "value": B * (M - len(typed)) / (ms / 1e3), "unit": "imputed genotypes/s", "ms_per_step": ms,
+            "kernels_ms": dict(zip(KERNELS, kavg)),
+            "roofline": {"bound": "hbm", "kernel": "anchor_posterior_kernel", "achieved": post, "peak": peak,
+                         "unit": "GB/s", "frac": post / peak},
+            "parity": {"targets": int(cpu_targets), "cells": int(c.size),
+                       "max_abs_dosage_diff_vs_fp64_oracle": float(np.abs(got_d - want["dosage"]).max()),
+                       "dosage_r2_vs_fp64_oracle_masked": float(np.corrcoef(x, y)[0, 1] ** 2),
+                       "argmax_haplotype_cells_differing": int((got_h != want["haps_argmax"]).sum())},
+            "cpu_port_imputed_genotypes_per_s": int(masked.sum()) / cpu_s}
 
 
 def uneven_panel(local, seed=2):
@@ -792,30 +853,49 @@ def run_ours(args, cfg):
     if world == 1 and not args.no_legs and args.config == "dense-cohort":
         del d_geno, d_dos, d_haps, h_geno, h_dos, h_haps, h_codes2, h_bits
         torch.cuda.empty_cache()
-        legs = [("uneven_batch", lambda up: leg_uneven(local, max(3, args.steps), peak, *up)),
-                ("serving", lambda up: leg_serving(local, peak, *up, seconds=args.serve_seconds)),
-                ("large_panel", lambda up: leg_large_panel(local, max(3, args.steps // 2), peak))]
-        up = None
-        for name, fn in legs:
+        # each extra key in a process of its own: its memory is returned, and a
+        # failure in one leaves the others and the headline standing
+        import subprocess
+        for name in LEGS:
+            t0 = time.perf_counter()
+            cmd = [sys.executable, str(Path(__file__).resolve()), "--leg", name, "--steps", str(args.steps),
+                   "--serve-seconds", str(args.serve_seconds)]
             try:
-                if up is None and name != "large_panel":
-                    up = uneven_panel(local)
-                if name == "large_panel" and up is not None:
-                    up = None
-                    torch.cuda.empty_cache()
-                t0 = time.perf_counter()
-                line[name] = fn(up)
-                line[name]["leg_wall_s"] = time.perf_counter() - t0
+                r = subprocess.run(cmd, capture_output=True, text=True, timeout=1200)
+                last = [x for x in r.stdout.splitlines() if x.startswith("{")]
+                line[name] = json.loads(last[-1]) if r.returncode == 0 and last else \
+                    {"error": f"exit {r.returncode}: " + (r.stderr or r.stdout)[-600:]}
             except Exception as e:  # noqa: BLE001 - a failed leg is reported, the headline stands
                 line[name] = {"error": f"{type(e).__name__}: {e}"}
+            line[name]["leg_wall_s"] = time.perf_counter() - t0
             print(f"[bench] {name} done", file=sys.stderr, flush=True)
     print(json.dumps(line), flush=True)
     if dist:
         dist.destroy_process_group()
 
 
+def run_leg(args):
+    """One extra key alone (a child of the headline run)."""
+    import torch
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    peak, _ = peaks()
+    if args.leg == "dense_map":
+        out = leg_dense_map(local, max(3, args.steps // 2), peak)
+    elif args.leg == "large_panel":
+        out = leg_large_panel(local, max(3, args.steps // 2), peak)
+    else:
+        up = uneven_panel(local)
+        out = leg_uneven(local, max(3, args.steps), peak, *up) if args.leg == "uneven_batch" else \
+            leg_serving(local, peak, *up, seconds=args.serve_seconds)
+    print(json.dumps(out), flush=True)
+
+
 def main():
     args = parse()
+    if args.leg:
+        run_leg(args)
+        return
     cfg = dict(CONFIGS[args.config])
     if args.samples:
         cfg["B"] = args.samples

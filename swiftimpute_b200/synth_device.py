@@ -49,12 +49,18 @@ def pack_panel(panel, chunk: int = 1024) -> np.ndarray:
     return out
 
 
-def make_targets(panel, B: int, every: int, n_mosaic: int = 8, switch: float = 0.005, seed: int = 0,
-                 chunk: int = 1024):
-    """Genotype codes [B][M] u8 on the device: h0 + h1 at markers m % every == 0, 3 elsewhere."""
+def make_targets(panel, B: int, every: int = 0, n_mosaic: int = 8, switch: float = 0.005, seed: int = 0,
+                 chunk: int = 1024, typed=None):
+    """Genotype codes [B][M] u8 on the device: h0 + h1 at the typed markers
+    (m % every == 0, or the marker indices in ``typed``), 3 elsewhere."""
     import torch
     dev = panel.device
     M, N = panel.shape
+    mask = torch.zeros(M, dtype=torch.bool, device=dev)
+    if typed is not None:
+        mask[torch.as_tensor(np.asarray(typed, dtype=np.int64), device=dev)] = True
+    else:
+        mask[::every] = True
     g = torch.Generator(device=dev).manual_seed(seed + 1000)
     H = 2 * B
     src = torch.randint(0, N, (H, n_mosaic), generator=g, device=dev)
@@ -71,6 +77,6 @@ def make_targets(panel, B: int, every: int, n_mosaic: int = 8, switch: float = 0
         hap = torch.gather(src.t(), 0, k)                   # [c][H] panel haplotype per marker
         alle = torch.gather(panel[m0:m0 + c], 1, hap)       # [c][H]
         geno = alle[:, 0::2] + alle[:, 1::2]                # [c][B]
-        typed = ((m0 + ar) % every == 0).expand(c, B)
+        typed = mask[m0:m0 + c, None].expand(c, B)
         codes[:, m0:m0 + c] = torch.where(typed, geno, torch.full_like(geno, 3)).t()
     return codes

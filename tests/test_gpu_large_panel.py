@@ -11,7 +11,8 @@ heterozygosity resampling. Checks:
     hash of every prefix row, all 100,000 rows);
   * every output of all 50,000 targets is finite and in range;
   * dosage and argmax haplotypes of a seeded subset of 512 targets equal the
-    FP64 oracle (1e-4; argmax up to threshold flips). The oracle reads the
+    FP64 oracle (1e-4; argmax up to threshold flips), on the 0.5 cM map and
+    on a 1 kb map. The oracle reads the
     device's slot table through a compact panel of the 32 selected haplotype
     columns per marker, which gives it the same emissions as the full panel.
 """
@@ -67,9 +68,9 @@ def test_pbwt_rows_equal_oracle_streaming_sweep(engine, large):
     assert np.array_equal(engine.row_hashes(), want)
 
 
-def test_all_targets_and_oracle_subset(engine, large):
+def _impute_and_check_subset(engine, large, pos, name):
     import torch
-    panel, _, pos, codes = large
+    panel, _, _, codes = large
     dev = codes.device
     params = N.default_params(num_states=L, ne=NE)
     dos = torch.empty((B, M), dtype=torch.float32, device=dev)
@@ -89,10 +90,12 @@ def test_all_targets_and_oracle_subset(engine, large):
     c_sub = codes.index_select(0, idx).cpu().numpy()
     got_d = dos.index_select(0, idx).cpu().numpy()
     got_h = haps.index_select(0, idx).cpu().numpy()
+    del dos, haps
+    torch.cuda.empty_cache()
     want = oracle.fb_batch(c_sub, cpairs, compact, pos, L, float(NE))
     from conftest import r2_masked, report
     r2 = r2_masked(got_d, want["dosage"], c_sub)
-    report("large panel 100,000 x 100,000, 512 targets", targets=512,
+    report(name, targets=512,
            max_abs_dosage_diff=np.abs(got_d - want["dosage"]).max(), dosage_r2_vs_oracle=r2,
            argmax_cells_differing=int((got_h != want["haps_argmax"]).sum()), cells=int(512 * M))
     assert r2 >= 1 - 1e-6
@@ -104,3 +107,14 @@ def test_all_targets_and_oracle_subset(engine, large):
         hi = oracle.fb_batch(c_sub[rows], cpairs, compact, pos, L, float(NE), tie_eps=1e-4 + 1e-5)
         flip = ((lo["haps_argmax"] != want["haps_argmax"][rows]) | (hi["haps_argmax"] != want["haps_argmax"][rows])).any(axis=1)
         assert not (diff[rows] & ~flip).any()
+
+
+def test_all_targets_and_oracle_subset(engine, large):
+    _impute_and_check_subset(engine, large, large[2], "large panel 100,000 x 100,000, 0.5 cM map, 512 targets")
+
+
+def test_dense_map_oracle_subset(engine, large):
+    # markers 1 kb apart: the transition keeps memory (rho < 1)
+    pos = (1 + np.arange(M, dtype=np.uint64) * np.uint64(1000)).astype(np.uint64)
+    engine.set_map(pos)
+    _impute_and_check_subset(engine, large, pos, "large panel 100,000 x 100,000, 1 kb map, 512 targets")

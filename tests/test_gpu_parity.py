@@ -118,14 +118,15 @@ def compare(engine, panel, pos, codes, L, ne, per_gap=False, sampling=N.SAMPLE_A
     return got, want
 
 
-@pytest.mark.parametrize("spacing", [500_000, 100])
+@pytest.mark.parametrize("spacing", [500_000, 1000, 100])
 def test_fb_plain_small_shape(engine, spacing):
-    # the plain-method config (4,432 haplotypes x 1,644 markers, every 5th typed, L=8, Ne=1e4), 96 targets
-    panel, pos, codes, _ = workload(1644, 4432, 96, synth.typed_every(1644, 5), spacing, 0, founders=40)
+    # the plain-method config (4,432 haplotypes x 1,644 markers, every 5th typed, L=8, Ne=1e4), all 444
+    # targets, on the 0.5 cM map (memoryless: rho clamps to 1) and on 1 kb and 100 bp maps
+    panel, pos, codes, _ = workload(1644, 4432, 444, synth.typed_every(1644, 5), spacing, 0, founders=40)
     got, want = compare(engine, panel, pos, codes, 8, 10000)
     from conftest import r2_masked, report
     r2 = r2_masked(got["dosage"], want["dosage"], codes)
-    report(f"plain-small spacing {spacing}", targets=96, max_abs_dosage_diff=np.abs(got["dosage"] - want["dosage"]).max(),
+    report(f"plain-small spacing {spacing}", targets=444, max_abs_dosage_diff=np.abs(got["dosage"] - want["dosage"]).max(),
            max_abs_hap_prob_diff=np.abs(got["hap_prob"] - want["hap_prob"]).max(), dosage_r2_vs_oracle=r2,
            argmax_cells_differing=int((got["haps"] != want["haps_argmax"]).sum()))
     assert r2 >= 1 - 1e-6
