@@ -247,6 +247,11 @@ public:
 
     void build_index();
     bool has_index() const { return has_index_; }
+    /* Stored index (save_pbwt_index / load_pbwt_index, pbwt_index.hpp:257-258):
+     * the built index to a file, or a file's index for this panel instead of
+     * build_index(); a file built on another panel is refused. */
+    void save_index(const std::string& filename);
+    void load_index(const std::string& filename);
     std::unique_ptr<ImputationResult> impute(const TargetData& targets);
     std::unique_ptr<ImputationResult> impute_with_progress(const TargetData& targets,
                                                            std::function<void(uint32_t, uint32_t)> progress_callback);

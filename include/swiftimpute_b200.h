@@ -150,6 +150,15 @@ si_status si_pbwt_row_hashes(si_ctx* ctx, uint64_t* out);
 /* Milliseconds of the last si_pbwt_build sweep (CUDA events). */
 si_status si_pbwt_last_ms(const si_ctx* ctx, float* ms);
 
+/* Stored index. Replace save_pbwt_index / load_pbwt_index (declared in
+ * pbwt_index.hpp:257-258, never defined by the reference). The stored form is
+ * the part of the index selection reads, the first 128 prefix entries of every
+ * marker (M * 512 bytes plus a 32-byte header), with the panel's shape and a
+ * checksum of its bits: si_pbwt_load refuses it for any other panel. */
+si_status si_pbwt_stored_bytes(const si_ctx* ctx, uint64_t* bytes);
+si_status si_pbwt_save(si_ctx* ctx, void* out, uint64_t bytes);
+si_status si_pbwt_load(si_ctx* ctx, const void* in, uint64_t bytes);
+
 /* Selection -------------------------------------------------------------- */
 
 /* Slots of markers [m0, m1) as haplotype pairs out [m1-m0][L][2], the result

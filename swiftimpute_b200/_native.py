@@ -105,6 +105,9 @@ SIGNATURES = [
     ("si_ctx_memory", c_int, [c_void_p, POINTER(c_uint64), POINTER(c_uint64)]),
     ("si_panel_upload_u8", c_int, [c_void_p, c_void_p, c_uint32, c_uint32]),
     ("si_panel_exception_count", c_int, [c_void_p, POINTER(c_uint64)]),
+    ("si_pbwt_stored_bytes", c_int, [c_void_p, POINTER(c_uint64)]),
+    ("si_pbwt_save", c_int, [c_void_p, c_void_p, c_uint64]),
+    ("si_pbwt_load", c_int, [c_void_p, c_void_p, c_uint64]),
     ("si_panel_upload_packed", c_int, [c_void_p, c_void_p, c_uint32, c_uint32, c_uint32]),
     ("si_panel_set_map", c_int, [c_void_p, c_void_p, c_void_p]),
     ("si_pbwt_build", c_int, [c_void_p, c_uint32]),

@@ -817,6 +817,79 @@ si_status si_pbwt_build(si_ctx* ctx, uint32_t flags) {
     return SI_OK;
 }
 
+namespace {
+
+// Stored index: header {magic, M, N, head width, panel checksum} then the
+// head rows [M][kHead] u32, the only part of the index selection reads.
+struct StoredIndexHeader {
+    char magic[8];
+    uint32_t M, N, head;
+    uint32_t reserved;
+    uint64_t checksum;
+};
+
+si_status panel_checksum(si_ctx* ctx, uint64_t* out) {
+    DeviceBuffer d;
+    SI_TRY(dev_alloc(ctx, d, 8));
+    cudaError_t e = launch_panel_checksum((const uint32_t*)ctx->panel.ptr, (uint64_t)ctx->M * ctx->W,
+                                          (unsigned long long*)d.ptr, ctx->stream);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(out, d.ptr, 8, cudaMemcpyDeviceToHost, ctx->stream);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    dev_free(ctx, d);
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "panel checksum");
+    return SI_OK;
+}
+
+}  // namespace
+
+si_status si_pbwt_stored_bytes(const si_ctx* ctx, uint64_t* bytes) {
+    if (!ctx || !bytes) return SI_ERR_INVALID_ARG;
+    *bytes = sizeof(StoredIndexHeader) + (uint64_t)ctx->M * kHead * 4;
+    return SI_OK;
+}
+
+si_status si_pbwt_save(si_ctx* ctx, void* out, uint64_t bytes) {
+    Range range("si_pbwt_save");
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!ctx->has_index) return fail(ctx, SI_ERR_STATE, "PBWT index not built (si_pbwt_build)");
+    const uint64_t need = sizeof(StoredIndexHeader) + (uint64_t)ctx->M * kHead * 4;
+    if (!out || bytes < need) return fail(ctx, SI_ERR_INVALID_ARG, "output smaller than si_pbwt_stored_bytes");
+    SI_TRY(set_device(ctx));
+    StoredIndexHeader h{};
+    std::memcpy(h.magic, "SIINDEX1", 8);
+    h.M = ctx->M; h.N = ctx->N; h.head = kHead;
+    SI_TRY(panel_checksum(ctx, &h.checksum));
+    std::memcpy(out, &h, sizeof h);
+    SI_CUDA(ctx, cudaMemcpy((char*)out + sizeof h, ctx->head.ptr, (size_t)ctx->M * kHead * 4, cudaMemcpyDeviceToHost),
+            "copy index");
+    return SI_OK;
+}
+
+si_status si_pbwt_load(si_ctx* ctx, const void* in, uint64_t bytes) {
+    Range range("si_pbwt_load");
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    StoredIndexHeader h{};
+    if (!in || bytes < sizeof h) return fail(ctx, SI_ERR_INVALID_ARG, "stored index too short");
+    std::memcpy(&h, in, sizeof h);
+    if (std::memcmp(h.magic, "SIINDEX1", 8) != 0) return fail(ctx, SI_ERR_INVALID_ARG, "not a stored PBWT index");
+    if (h.M != ctx->M || h.N != ctx->N || h.head != kHead)
+        return fail(ctx, SI_ERR_INVALID_ARG, "stored index shape differs from the uploaded panel");
+    if (bytes < sizeof h + (uint64_t)h.M * kHead * 4) return fail(ctx, SI_ERR_INVALID_ARG, "stored index truncated");
+    SI_TRY(set_device(ctx));
+    uint64_t sum = 0;
+    SI_TRY(panel_checksum(ctx, &sum));
+    if (sum != h.checksum)
+        return fail(ctx, SI_ERR_INVALID_ARG, "stored index was built on a different panel (checksum differs)");
+    reset_index(ctx);
+    SI_TRY(dev_alloc(ctx, ctx->head, (size_t)ctx->M * kHead * 4));
+    SI_CUDA(ctx, cudaMemcpy(ctx->head.ptr, (const char*)in + sizeof h, (size_t)ctx->M * kHead * 4,
+                            cudaMemcpyHostToDevice), "copy index");
+    ctx->has_index = true;
+    ctx->pbwt_flags = 0;
+    return SI_OK;
+}
+
 si_status si_pbwt_get_prefix_rows(si_ctx* ctx, uint32_t m0, uint32_t count, uint32_t* out) {
     if (!ctx) return SI_ERR_INVALID_ARG;
     if (!ctx->has_index || !ctx->prefix.ptr)

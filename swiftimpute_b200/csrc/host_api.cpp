@@ -697,6 +697,33 @@ void Imputer::build_index() {
     has_index_ = true;
 }
 
+void Imputer::save_index(const std::string& filename) {
+    ensure_panel();
+    if (!has_index_) throw ImputationError("PBWT index not built");
+    uint64_t n = 0;
+    check(si_pbwt_stored_bytes(ctx_, &n), "stored index size");
+    std::vector<char> buf(n);
+    check(si_pbwt_save(ctx_, buf.data(), n), "save index");
+    std::ofstream o(filename, std::ios::binary);
+    if (!o) throw ImputationError("Cannot write " + filename);
+    o.write(buf.data(), (std::streamsize)n);
+    if (!o) throw ImputationError("write failed: " + filename);
+}
+
+void Imputer::load_index(const std::string& filename) {
+    ensure_panel();
+    std::ifstream in(filename, std::ios::binary | std::ios::ate);
+    if (!in) throw ImputationError("Cannot open " + filename);
+    const std::streamoff n = in.tellg();
+    if (n <= 0) throw ImputationError("empty index file: " + filename);
+    in.seekg(0);
+    std::vector<char> buf((size_t)n);
+    in.read(buf.data(), n);
+    if (!in) throw ImputationError("truncated index file: " + filename);
+    check(si_pbwt_load(ctx_, buf.data(), (uint64_t)n), "load index");
+    has_index_ = true;
+}
+
 std::unique_ptr<ImputationResult> Imputer::impute(const TargetData& targets) {
     return impute_with_progress(targets, nullptr);
 }

@@ -37,6 +37,18 @@ __device__ __forceinline__ unsigned long long mix_entry(uint32_t value, uint32_t
     return x;
 }
 
+// Order-dependent 64-bit checksum of the bit-packed panel (word value mixed
+// with its index, summed): identifies the panel a stored index was built on.
+__global__ void panel_checksum_kernel(const uint32_t* __restrict__ words, uint64_t n,
+                                      unsigned long long* __restrict__ out) {
+    unsigned long long acc = 0;
+    for (uint64_t i = (uint64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (uint64_t)gridDim.x * blockDim.x)
+        acc += mix_entry(words[i], (uint32_t)(i ^ (i >> 32)));
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) acc += __shfl_xor_sync(0xffffffffu, acc, o);
+    if ((threadIdx.x & 31) == 0) atomicAdd(out, acc);
+}
+
 constexpr int kSweepThreads = 1024;
 
 // Sequential sweep over all markers in one CTA. Thread t owns the contiguous
@@ -193,6 +205,13 @@ cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint3
     const uint64_t grid = (threads + bs - 1) / bs;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
     pack_panel_kernel<<<(uint32_t)grid, bs, 0, s>>>(d_u8, M, N, W, d_words);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_panel_checksum(const uint32_t* d_words, uint64_t n, unsigned long long* d_out, cudaStream_t s) {
+    cudaError_t e = cudaMemsetAsync(d_out, 0, 8, s);
+    if (e != cudaSuccess) return e;
+    panel_checksum_kernel<<<148 * 8, 256, 0, s>>>(d_words, n, d_out);
     return cudaGetLastError();
 }
 

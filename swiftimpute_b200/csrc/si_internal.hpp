@@ -162,6 +162,7 @@ cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, u
                               uint32_t W, uint32_t* d_head, uint32_t* d_prefix, unsigned long long* d_hash,
                               uint32_t* d_perm_scratch, cudaStream_t s);
 size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W);
+cudaError_t launch_panel_checksum(const uint32_t* d_words, uint64_t n, unsigned long long* d_out, cudaStream_t s);
 // Selection over markers [0, M) of the given panel rows; ex_off/ex_ent (may be
 // null) are the rows' exception lists, raw (may be null) receives allele bytes.
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,

@@ -77,6 +77,19 @@ class Engine:
         self._check(self.lib.si_panel_upload_u8(self.h, _ptr(panel), M, N_))
         self.M, self.N = M, N_
 
+    def save_index(self) -> bytes:
+        """The built PBWT index in its stored form (si_pbwt_save)."""
+        n = c_uint64()
+        self._check(self.lib.si_pbwt_stored_bytes(self.h, byref(n)))
+        buf = np.empty(n.value, np.uint8)
+        self._check(self.lib.si_pbwt_save(self.h, _ptr(buf), n.value))
+        return buf.tobytes()
+
+    def load_index(self, blob: bytes) -> None:
+        """Load a stored index for the uploaded panel (si_pbwt_load)."""
+        buf = np.frombuffer(blob, np.uint8)
+        self._check(self.lib.si_pbwt_load(self.h, _ptr(buf), buf.size))
+
     def exception_count(self) -> int:
         """Panel entries other than 0 and 1 (missing or multi-allelic) of the uploaded panel."""
         n = c_uint64()

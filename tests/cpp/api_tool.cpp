@@ -5,6 +5,7 @@
 //   api_tool parse  <ref.vcf> <tgt.vcf> <prefix>     (no GPU) dump panel / GL, binary round trips
 //   api_tool impute <ref.vcf> <tgt.vcf> <out.vcf> <prefix> <deterministic> <L> <ne> [posteriors]
 //   api_tool loadbin <panel|target> <file>           (no GPU) load a binary file, print its shape
+//   api_tool index  <ref.vcf> <tgt.vcf> <index file> build, save and reload the PBWT index
 //   api_tool multi  <ref.vcf> <tgt.vcf> <devices> <prefix> <deterministic> <L> <ne>
 //                   MultiGPUImputer over a comma-separated device list (repeats allowed),
 //                   compared with one Imputer over all targets
@@ -133,6 +134,22 @@ int main(int argc, char** argv) {
             dump(pre + ".dosage", ds.data(), n * 4);
             dump(pre + ".haps", res->haplotype0(0), 2 * n);
             std::printf("multi ok: replicas=%u identical=%d\n", multi.num_gpus(), same ? 1 : 0);
+            return same ? 0 : 3;
+        }
+        if (cmd == "index") {
+            // build, store to a file, and impute again through a second Imputer that loads it
+            ImputationConfig cfg;
+            cfg.hmm_params.num_states = 8;
+            Imputer a(*ref, cfg);
+            a.build_index();
+            a.save_index(argv[4]);
+            auto ra = a.impute(*tgt);
+            Imputer b(*ref, cfg);
+            b.load_index(argv[4]);
+            auto rb = b.impute(*tgt);
+            const size_t n = (size_t)ra->num_samples() * ra->num_markers();
+            const bool same = std::memcmp(ra->haplotype0(0), rb->haplotype0(0), 2 * n) == 0;
+            std::printf("index same=%d has_index=%d\n", same ? 1 : 0, b.has_index() ? 1 : 0);
             return same ? 0 : 3;
         }
         if (cmd == "impute") {

@@ -169,6 +169,16 @@ def test_imputer_end_to_end(api_tool, vcfs, deterministic, posteriors):
     assert len(lines) == 9 + M
 
 
+@pytest.mark.gpu
+def test_imputer_stored_index(api_tool, vcfs):
+    """Imputer::save_index / load_index (pbwt_index.hpp:257-258): a second
+    Imputer that loads the stored index gives the same haplotypes."""
+    d, *_ = vcfs
+    r = subprocess.run([str(api_tool), "index", str(d / "ref.vcf"), str(d / "tgt.vcf"), str(d / "p.siindex")],
+                       capture_output=True, text=True)
+    assert r.returncode == 0 and "index same=1 has_index=1" in r.stdout, r.stdout + r.stderr
+
+
 def test_multi_gpu_imputer_refusals_without_device(api_tool, vcfs):
     d, *_ = vcfs
     args = [str(api_tool), "multi", str(d / "ref.vcf"), str(d / "tgt.vcf")]

@@ -168,6 +168,31 @@ def test_fb_panel_with_missing_and_multiallelic_alleles(engine, L, flags):
     assert engine.exception_count() == 0
 
 
+def test_stored_index_roundtrip(engine):
+    # si_pbwt_save / si_pbwt_load: a ctx that loads the stored index selects and imputes as the one that built it
+    from swiftimpute_b200.engine import Engine
+    panel, pos, codes, _ = workload(900, 600, 30, synth.typed_every(900, 4), 100, 80)
+    load(engine, panel, pos, store=False)
+    blob = engine.save_index()
+    assert len(blob) == 32 + 900 * 128 * 4
+    pairs = {L: engine.select_states(L) for L in (8, 16)}
+    want = engine.impute(codes)
+    with Engine(0) as other:
+        other.upload_panel(panel)
+        other.set_map(pos)
+        other.load_index(blob)
+        for L in (8, 16):
+            assert np.array_equal(other.select_states(L), pairs[L])
+        got = other.impute(codes)
+        assert np.array_equal(got["dosage"], want["dosage"]) and np.array_equal(got["haps"], want["haps"])
+        changed = panel.copy()
+        changed[450, 17] ^= 1
+        other.upload_panel(changed)
+        with pytest.raises(N.SIError) as e:
+            other.load_index(blob)
+        assert e.value.status == 1 and "different panel" in e.value.args[-1]
+
+
 def test_compact_host_formats(engine):
     # 2-bit codes in and haplotype bits out give the byte path's results bit for bit
     from swiftimpute_b200.engine import pack_codes, unpack_hap_bits
