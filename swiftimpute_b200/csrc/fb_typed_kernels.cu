@@ -670,7 +670,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     if (!__any_sync(kAll, live)) return;  // whole warp
 
     const TypedRegion& R = kPlain ? A.reg0 : v.r;
-    const uint32_t len = kPlain ? A.M : len;
+    const uint32_t len = kPlain ? A.M : v.len;
     const unsigned long long out = kPlain ? (unsigned long long)s * A.M : v.out;
     const Tabs& tb = R.tabs;
     const uint32_t* pos = A.apos + ab;
