@@ -86,13 +86,13 @@ void reset_index(si_ctx* ctx) {
     for (auto& kv : ctx->sel) {
         dev_free(ctx, kv.second.pairs);
         dev_free(ctx, kv.second.masks);
-        dev_free(ctx, kv.second.g);
+        dev_free(ctx, kv.second.g2);
         dev_free(ctx, kv.second.raw);
     }
     ctx->sel.clear();
     for (auto& kv : ctx->region_sel) {
         dev_free(ctx, kv.second.masks);
-        dev_free(ctx, kv.second.g);
+        dev_free(ctx, kv.second.g2);
         dev_free(ctx, kv.second.raw);
     }
     ctx->region_sel.clear();
@@ -211,13 +211,13 @@ si_status ensure_selection(si_ctx* ctx, uint32_t L, int kind, SelectionCache** o
         if (!c.pairs.ptr) {
             SI_TRY(dev_alloc(ctx, c.pairs, (size_t)ctx->M * L * 2 * sizeof(uint32_t)));
             SI_TRY(dev_alloc(ctx, c.masks, (size_t)ctx->M * sizeof(SlotMasks)));
-            SI_TRY(dev_alloc(ctx, c.g, (size_t)ctx->M * fb_lmax(L) * sizeof(float)));
+            SI_TRY(dev_alloc(ctx, c.g2, (size_t)ctx->M * fb_lmax(L) * sizeof(float2)));
             if (ctx->n_ex) SI_TRY(dev_alloc(ctx, c.raw, (size_t)ctx->M * fb_lmax(L) * 2));
         }
         SI_CUDA(ctx,
                 launch_select((const uint32_t*)ctx->head.ptr, (const uint32_t*)ctx->panel.ptr, ctx->M, ctx->N, ctx->W,
                               L, kind, (const unsigned long long*)ctx->ex_off.ptr, (const uint32_t*)ctx->ex_ent.ptr,
-                              (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, (float*)c.g.ptr, (uint8_t*)c.raw.ptr,
+                              (uint32_t*)c.pairs.ptr, (SlotMasks*)c.masks.ptr, (float2*)c.g2.ptr, (uint8_t*)c.raw.ptr,
                               fb_lmax(L), s ? s : ctx->stream),
                 "select kernel");
     }
@@ -269,26 +269,38 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
         const double lr = std::log(rho);
         const int regime = std::fabs(rho - 1.0) < 1e-15 ? 2 : (rho < 1.0 ? 0 : 1);
         const double lgc = regime == 0 ? std::log1p(-rho) : (regime == 1 ? std::log(rho - 1.0) : 0.0);
-        std::vector<float> QS(2 * kTabN);
+        // QS [n] {Q, S}; then the pair tables {Q_n, Q_n+1, S_n, S_n+1} and
+        // {Q_n, Q_n-1, S_n, S_n-1} (index 0: Q_0, S_0 twice) for two consecutive cells
+        std::vector<float> QS(2 * kTabN + 8 * kTabN);
         std::vector<double> G(kTabN);
-        for (uint32_t n = 0; n < kTabN; ++n) {
+        std::vector<float> qf(kTabN + 1), sf(kTabN + 1);
+        for (uint32_t n = 0; n <= kTabN; ++n) {
             const double qn = (n == 0) ? 1.0 : (q > 0.0 ? std::exp((double)n * lq) : 0.0);
             const double om = (n == 0) ? 0.0 : (q > 0.0 ? -std::expm1((double)n * lq) : 1.0);
-            QS[2 * n] = (float)qn;
-            QS[2 * n + 1] = (float)(om / (double)L);
+            qf[n] = (float)qn;
+            sf[n] = (float)(om / (double)L);
+        }
+        float* up = QS.data() + 2 * kTabN;
+        float* dn = up + 4 * kTabN;
+        for (uint32_t n = 0; n < kTabN; ++n) {
+            QS[2 * n] = qf[n];
+            QS[2 * n + 1] = sf[n];
+            up[4 * n] = qf[n]; up[4 * n + 1] = qf[n + 1]; up[4 * n + 2] = sf[n]; up[4 * n + 3] = sf[n + 1];
+            const uint32_t b = n ? n - 1 : 0;
+            dn[4 * n] = qf[n]; dn[4 * n + 1] = qf[b]; dn[4 * n + 2] = sf[n]; dn[4 * n + 3] = sf[b];
             if (n == 0) G[n] = -INFINITY;
             else if (regime == 0) G[n] = -(double)n * lr + std::log(-std::expm1((double)n * lr)) - lgc;
             else if (regime == 1) G[n] = std::log(-std::expm1(-(double)n * lr)) - lgc;
             else G[n] = std::log((double)n);
         }
-        si_status st = dev_alloc(ctx, ts.QS, kTabN * 8);
+        si_status st = dev_alloc(ctx, ts.QS, QS.size() * 4);
         if (st == SI_OK) st = dev_alloc(ctx, ts.G, kTabN * 8);
         if (st != SI_OK) {
             dev_free(ctx, ts.QS); dev_free(ctx, ts.G);
             ctx->tables.erase(key);
             return st;
         }
-        SI_CUDA(ctx, cudaMemcpy(ts.QS.ptr, QS.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
+        SI_CUDA(ctx, cudaMemcpy(ts.QS.ptr, QS.data(), QS.size() * 4, cudaMemcpyHostToDevice), "copy tables");
         SI_CUDA(ctx, cudaMemcpy(ts.G.ptr, G.data(), kTabN * 8, cudaMemcpyHostToDevice), "copy tables");
         ts.consts[0] = q > 0.0 ? std::log2(q) : -INFINITY;
         ts.consts[1] = lr;
@@ -296,6 +308,8 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
         ts.consts[3] = regime;
     }
     out->QS = (const float2*)ts.QS.ptr; out->G = (const double*)ts.G.ptr;
+    out->QSup = (const float4*)((const float*)ts.QS.ptr + 2 * kTabN);
+    out->QSdn = out->QSup + kTabN;
     out->NT = kTabN; out->log2q = (float)ts.consts[0]; out->invL = 1.0f / (float)L;
     out->lr = ts.consts[1]; out->lgc = ts.consts[2]; out->regime = (int)ts.consts[3];
     return SI_OK;
@@ -364,7 +378,7 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
     a.seed = p->seed;
     a.sid_base = p->sample_id_base;
     a.reg0.masks = (const SlotMasks*)sel->masks.ptr;
-    a.reg0.g = (const float*)sel->g.ptr;
+    a.reg0.g2 = (const float2*)sel->g2.ptr;
     a.reg0.raw = (const uint8_t*)sel->raw.ptr;
     a.reg0.gs = fb_lmax(p->num_states);
     a.reg0.L = p->num_states;
@@ -520,18 +534,18 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             if (j == sweeps.size()) continue;  // cached already under another slot count? swept above
             auto& rs = ctx->region_sel[key];
             st = dev_alloc(ctx, rs.masks, (size_t)(g.m_end - g.m_begin) * sizeof(SlotMasks));
-            if (st == SI_OK) st = dev_alloc(ctx, rs.g, (size_t)(g.m_end - g.m_begin) * fb_lmax(L) * sizeof(float));
+            if (st == SI_OK) st = dev_alloc(ctx, rs.g2, (size_t)(g.m_end - g.m_begin) * fb_lmax(L) * sizeof(float2));
             if (st == SI_OK && ctx->n_ex) st = dev_alloc(ctx, rs.raw, (size_t)(g.m_end - g.m_begin) * fb_lmax(L) * 2);
             if (st != SI_OK) {
                 dev_free(ctx, rs.masks);
-                dev_free(ctx, rs.g);
+                dev_free(ctx, rs.g2);
                 ctx->region_sel.erase(key);
                 break;
             }
             e = launch_select((const uint32_t*)head.ptr + sweeps[j].head_off,
                               (const uint32_t*)ctx->panel.ptr + (size_t)g.m_begin * W, g.m_end - g.m_begin, N, W, L,
                               kind, ctx->n_ex ? (const unsigned long long*)ctx->ex_off.ptr + g.m_begin : nullptr,
-                              (const uint32_t*)ctx->ex_ent.ptr, nullptr, (SlotMasks*)rs.masks.ptr, (float*)rs.g.ptr,
+                              (const uint32_t*)ctx->ex_ent.ptr, nullptr, (SlotMasks*)rs.masks.ptr, (float2*)rs.g2.ptr,
                               (uint8_t*)rs.raw.ptr, fb_lmax(L), s);
         }
         if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(s);  // scratch reuse below
@@ -549,7 +563,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             SelectionCache* sel = nullptr;
             SI_TRY(ensure_selection(ctx, L, p->selection_kind, &sel, false, s));
             tr[r].masks = (const SlotMasks*)sel->masks.ptr + g.m_begin;
-            tr[r].g = (const float*)sel->g.ptr + (size_t)g.m_begin * fb_lmax(L);
+            tr[r].g2 = (const float2*)sel->g2.ptr + (size_t)g.m_begin * fb_lmax(L);
             tr[r].raw = sel->raw.ptr ? (const uint8_t*)sel->raw.ptr + (size_t)g.m_begin * fb_lmax(L) * 2 : nullptr;
             tr[r].gs = fb_lmax(L);
             SI_TRY(tables_for(ctx, ctx->trans0, L, &tr[r].tabs));
@@ -557,7 +571,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             const int kind = (L <= 32 && N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
             const auto& rs = ctx->region_sel[std::make_tuple(g.m_begin, g.m_end, L, kind)];
             tr[r].masks = (const SlotMasks*)rs.masks.ptr;
-            tr[r].g = (const float*)rs.g.ptr;
+            tr[r].g2 = (const float2*)rs.g2.ptr;
             tr[r].raw = (const uint8_t*)rs.raw.ptr;
             tr[r].gs = fb_lmax(L);
             if (!region_first_gap_ok(ctx, p, g.m_begin, g.m_end))
@@ -652,7 +666,7 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     }
     for (auto& kv : ctx->region_sel) {
         dev_free(ctx, kv.second.masks);
-        dev_free(ctx, kv.second.g);
+        dev_free(ctx, kv.second.g2);
         dev_free(ctx, kv.second.raw);
     }
     dev_free(ctx, ctx->ex_off);

@@ -7,9 +7,13 @@ namespace si {
 
 // Closed-form coefficients for runs of untyped markers under one transition
 // (c, delta), computed in FP64 on the host: q = delta / rho, rho = delta + L c,
-// QS[n] = {Q[n], S[n]} = {q^n, (1 - q^n) / L}, G[n] = log sum_{k=1..n} rho^-k.
+// QS[n] = {Q[n], S[n]} = {q^n, (1 - q^n) / L}, G[n] = log sum_{k=1..n} rho^-k;
+// for two consecutive cells QSup[n] = {Q[n], Q[n+1], S[n], S[n+1]} and
+// QSdn[n] = {Q[n], Q[n-1], S[n], S[n-1]}.
 struct TypedTables {
     const float2* QS;
+    const float4* QSup;
+    const float4* QSdn;
     const double* G;
     uint32_t NT;
     float log2q;
@@ -19,13 +23,13 @@ struct TypedTables {
     int regime;  // 0: rho < 1, 1: rho > 1, 2: rho == 1
 };
 
-// A panel slice imputed with L slots: its slot masks, per-slot ALT counts
-// g [marker][gs] and allele bytes raw [marker][gs][2] (null for a 0/1 panel;
-// index 0 = the slice's first marker), and the closed-form tables of its
-// transition.
+// A panel slice imputed with L slots: its slot masks, per-slot ALT counts at
+// m and m + 1 g2 [marker][gs] and allele bytes raw [marker][gs][2] (null for a
+// 0/1 panel; index 0 = the slice's first marker), and the closed-form tables
+// of its transition.
 struct TypedRegion {
     const SlotMasks* masks;
-    const float* g;
+    const float2* g2;
     const uint8_t* raw;
     uint32_t gs;
     uint32_t L;

@@ -571,9 +571,10 @@ __device__ __forceinline__ float vmax(const float (&p)[LM]) {
 
 // Shared memory of one warp: backward records [C][LM/4][32] float4 and
 // [C][32] farg'; the flush descriptors [2][32] uint4; the dosage tile
-// [32][33] f32, the allele tile [32][34] u16 and, for P(hap=1), [32][33] f32x2.
+// [32][36] f32, the allele tile [64][36] u8 (rows 2r and 2r + 1: the two
+// haplotypes of lane r) and, for P(hap=1), [32][34] f32x2.
 __host__ __device__ constexpr size_t post_warp_bytes(uint32_t LM, uint32_t C, bool hprob) {
-    return (size_t)C * LM * 128 + (size_t)C * 256 + 1024 + 32 * 33 * 4 + 32 * 34 * 2 + (hprob ? 32 * 33 * 8 : 0);
+    return (size_t)C * LM * 128 + (size_t)C * 256 + 1024 + 32 * 36 * 4 + 64 * 36 + (hprob ? 32 * 34 * 8 : 0);
 }
 
 // Backward records of window w (anchors [wC, min(wC + C, NA))) of one sample,
@@ -616,7 +617,7 @@ __device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& t
         if (farg + tabG(tb, n) < -104.0) hi = kNegInfHi;  // floor negligible over the run
         else if (farg + tabG(tb, 1) > 60.0) hi = kInfHi;  // floor dominates: beta uniform
         else {
-            const double f = farg - log((double)sw);
+            const double f = farg - (double)logf(sw);
             lo = (uint32_t)__double_as_longlong(f);
             hi = (uint32_t)((unsigned long long)__double_as_longlong(f) >> 32);
         }
@@ -634,20 +635,26 @@ __device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& t
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
 // kFast: argmax picks, no P(hap=1). kPlain: every sample covers the whole
 // panel with the launch's one region (read from the kernel parameters).
+// A lane takes two consecutive cells of a run per step (an even marker and
+// the next one) with f32x2 arithmetic across the two cells; a run's odd first
+// marker or last marker takes a step alone. Tiles are aligned to absolute
+// 32-marker columns, so a tile every lane of a warp fills completely (lanes
+// that share typed positions) leaves as 128-bit row segments.
 template <int LM, bool kFull, bool kFast, bool kPlain>
 __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kernel(const __grid_constant__ TypedArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
     constexpr uint32_t Q4 = LM / 4;
     constexpr uint32_t kAll = 0xffffffffu;
+    constexpr bool kBcast = LM <= 16;  // a', w' held as (x, x) pairs: no per-step pairing moves
     const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
     const uint32_t C = A.C, K = A.K;
     unsigned char* wbase = smem + (size_t)warp * post_warp_bytes(LM, C, !kFast);
     float4* recW = reinterpret_cast<float4*>(wbase);                     // [C][Q4][32]
     uint2* recF = reinterpret_cast<uint2*>(recW + (size_t)C * Q4 * 32);  // [C][32]
     uint4* meta = reinterpret_cast<uint4*>(recF + (size_t)C * 32);       // [2][32]
-    float* tD = reinterpret_cast<float*>(meta + 64);                     // [32][33]
-    uint16_t* tH = reinterpret_cast<uint16_t*>(tD + 32 * 33);            // [32][34]
-    float2* tP = reinterpret_cast<float2*>(tH + 32 * 34);                // [32][33]
+    float* tD = reinterpret_cast<float*>(meta + 64);                     // [32][36]
+    uint8_t* tH = reinterpret_cast<uint8_t*>(tD + 32 * 36);              // [64][36]
+    float2* tP = reinterpret_cast<float2*>(tH + 64 * 36);                // [32][34]
 
     const uint32_t SG = (A.B + 31) / 32;
     const unsigned long long gw = (unsigned long long)blockIdx.x * nw + warp;
@@ -673,6 +680,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     const uint32_t len = kPlain ? A.M : v.len;
     const unsigned long long out = kPlain ? (unsigned long long)s * A.M : v.out;
     const Tabs& tb = R.tabs;
+    const uint32_t Lr = R.L;
     const uint32_t* pos = A.apos + ab;
     const uint32_t* aem = A.aem + ab;
     const uint8_t* ash = A.ashift + ab;
@@ -680,36 +688,37 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
     const bool w_hp = !kFast && A.hprob != nullptr;
     const bool argmax = kFast || A.sampling == SI_SAMPLE_ARGMAX;
     const float keep = 1.0f - A.tie_eps;
-    float act[LM];  // 1 for the region's slots, 0 beyond L (only read when !kFull)
-    {
-        const uint32_t lmask = lmask_of(R.L);
-#pragma unroll
-        for (int l = 0; l < LM; ++l) act[l] = ((lmask >> l) & 1u) ? 1.f : 0.f;
-    }
 
-    float ap[LM], wp[LM];  // a' and w' of the current run
+    float2 a2[kBcast ? LM : 1], w2[kBcast ? LM : 1];  // (a'_l, a'_l), (w'_l, w'_l)
+    float ap[kBcast ? 1 : LM], wp[kBcast ? 1 : LM];
+    auto A2 = [&](int l) { if constexpr (kBcast) return a2[l]; else return make_float2(ap[l], ap[l]); };
+    auto W2 = [&](int l) { if constexpr (kBcast) return w2[l]; else return make_float2(wp[l], wp[l]); };
+    auto a_of = [&](int l) { if constexpr (kBcast) return a2[l].x; else return ap[l]; };
+    auto set_a = [&](int l, float x) { if constexpr (kBcast) a2[l] = make_float2(x, x); else ap[l] = x; };
+    auto set_w = [&](int l, float x) { if constexpr (kBcast) w2[l] = make_float2(x, x); else wp[l] = x; };
+#pragma unroll
+    for (int l = 0; l < LM; ++l) { set_a(l, 0.f); set_w(l, 0.f); }
     uint2 fr = make_uint2(0u, kNegInfHi);
     uint32_t k = w0 * C, p0 = 0, p1 = 0, m = 0, mend = 0;
-#pragma unroll
-    for (int l = 0; l < LM; ++l) { ap[l] = 0.f; wp[l] = 0.f; }
     auto load_record = [&](uint32_t r) {
 #pragma unroll
         for (uint32_t q = 0; q < Q4; ++q) {
             const float4 x = recW[(r * Q4 + q) * 32 + lane];
-            wp[4 * q] = x.x; wp[4 * q + 1] = x.y; wp[4 * q + 2] = x.z; wp[4 * q + 3] = x.w;
+            set_w(4 * q, x.x); set_w(4 * q + 1, x.y); set_w(4 * q + 2, x.z); set_w(4 * q + 3, x.w);
         }
         fr = recF[r * 32 + lane];
     };
     if (live) {
         const float4* src = reinterpret_cast<const float4*>(A.ckptF + (wb + w0) * LM);
+        float x[LM];
 #pragma unroll
         for (uint32_t q = 0; q < Q4; ++q) {
-            const float4 x = src[q];
-            ap[4 * q] = x.x; ap[4 * q + 1] = x.y; ap[4 * q + 2] = x.z; ap[4 * q + 3] = x.w;
+            const float4 y = src[q];
+            x[4 * q] = y.x; x[4 * q + 1] = y.y; x[4 * q + 2] = y.z; x[4 * q + 3] = y.w;
         }
-        const float inv = rcp_approx(vsum<LM>(ap));
+        const float inv = rcp_approx(vsum<LM>(x));
 #pragma unroll
-        for (int l = 0; l < LM; ++l) ap[l] *= inv;
+        for (int l = 0; l < LM; ++l) set_a(l, x[l] * inv);
         p0 = pos[k];
         p1 = k + 1 < NA ? pos[k + 1] : len;
         mend = wend * C < NA ? pos[wend * C] : len;
@@ -717,38 +726,64 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
         rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, len, w0, recW, recF, lane);
         load_record(0);
     }
-    bool in_tab = p1 - p0 < tb.NT;  // every i, j of the run index the tables
+    bool in_tab = p1 - p0 < tb.NT;  // every i, i+1, j, j-1 of the run index the pair tables
 
-    // flush the tile's valid columns (a prefix per lane) as row segments
-    uint32_t tstart = m, tcnt = 0;
+    // Tile: columns m & 31 of the 32-marker block starting at tbase; this
+    // lane wrote columns [tlo, thi) since the last flush.
+    uint32_t tbase = 0, tlo = 32, thi = 0;
+    const bool vec_ok = kPlain && (A.M & 3u) == 0 && !w_hp &&
+                        (reinterpret_cast<uintptr_t>(A.dosage) & 15u) == 0 &&
+                        (reinterpret_cast<uintptr_t>(A.haps) & 3u) == 0;
     auto flush = [&]() {
         __syncwarp();
-        const unsigned long long od = out + tstart, oh = 2ull * out + tstart;
-        meta[lane] = make_uint4((uint32_t)od, (uint32_t)(od >> 32), (uint32_t)oh, (uint32_t)(oh >> 32));
-        meta[32 + lane] = make_uint4(len, live ? tcnt : 0u, 0u, 0u);
-        __syncwarp();
-        for (uint32_t r = 0; r < 32; ++r) {
-            const uint4 m1 = meta[32 + r];
-            if (m1.y == 0) continue;  // same value in every lane
-            const uint4 m0 = meta[r];
-            if (lane < m1.y) {
-                const unsigned long long rd = ((unsigned long long)m0.y << 32) | m0.x;
-                const unsigned long long rh = ((unsigned long long)m0.w << 32) | m0.z;
-                if (w_dos) A.dosage[rd + lane] = tD[r * 33 + lane];
-                if (w_hap) {
-                    const uint32_t h = tH[r * 34 + lane];
-                    A.haps[rh + lane] = (uint8_t)(h & 0xffu);
-                    A.haps[rh + m1.x + lane] = (uint8_t)(h >> 8);
+        const bool has = thi > tlo;
+        const uint32_t tb0 = __shfl_sync(kAll, tbase, 0);
+        if (__all_sync(kAll, vec_ok && has && tlo == 0 && thi == 32 && tbase == tb0)) {
+            // every lane filled the same whole tile: 128-bit rows of dosage, 32-bit rows of alleles
+            const unsigned long long s0 = s - lane;
+            if (w_dos) {
+#pragma unroll 4
+                for (uint32_t it = 0; it < 8; ++it) {
+                    const uint32_t r = it * 4 + (lane >> 3), c = (lane & 7) * 4;
+                    const float4 x = *reinterpret_cast<const float4*>(tD + r * 36 + c);
+                    *reinterpret_cast<float4*>(A.dosage + (s0 + r) * A.M + tb0 + c) = x;
                 }
-                if (w_hp) reinterpret_cast<float2*>(A.hprob)[rd + lane] = tP[r * 33 + lane];
+            }
+            if (w_hap) {
+#pragma unroll 4
+                for (uint32_t it = 0; it < 16; ++it) {
+                    const uint32_t rr = it * 4 + (lane >> 3), c = (lane & 7) * 4;
+                    const uint32_t x = *reinterpret_cast<const uint32_t*>(tH + rr * 36 + c);
+                    *reinterpret_cast<uint32_t*>(A.haps + (2 * (s0 + (rr >> 1)) + (rr & 1)) * A.M + tb0 + c) = x;
+                }
+            }
+        } else {
+            const unsigned long long od = out + tbase, oh = 2ull * out + tbase;
+            meta[lane] = make_uint4((uint32_t)od, (uint32_t)(od >> 32), (uint32_t)oh, (uint32_t)(oh >> 32));
+            meta[32 + lane] = make_uint4(len, tlo, thi, (live && has) ? 1u : 0u);
+            __syncwarp();
+            for (uint32_t r = 0; r < 32; ++r) {
+                const uint4 m1 = meta[32 + r];
+                if (!m1.w) continue;  // same value in every lane
+                const uint4 m0 = meta[r];
+                if (lane >= m1.y && lane < m1.z) {
+                    const unsigned long long rd = ((unsigned long long)m0.y << 32) | m0.x;
+                    const unsigned long long rh = ((unsigned long long)m0.w << 32) | m0.z;
+                    if (w_dos) A.dosage[rd + lane] = tD[r * 36 + lane];
+                    if (w_hap) {
+                        A.haps[rh + lane] = tH[(2 * r) * 36 + lane];
+                        A.haps[rh + m1.x + lane] = tH[(2 * r + 1) * 36 + lane];
+                    }
+                    if (w_hp) reinterpret_cast<float2*>(A.hprob)[rd + lane] = tP[r * 34 + lane];
+                }
             }
         }
         __syncwarp();
-        tstart = m;
-        tcnt = 0;
+        tlo = 32;
+        thi = 0;
     };
 
-    for (uint32_t step = 0;; ++step) {
+    for (;;) {
         const bool on = live && m < mend;
         if (!__any_sync(kAll, on)) break;
         if (on && m == p1) {
@@ -756,105 +791,154 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? 4 : 2)) anchor_posterior_kerne
             const uint32_t kn = k + 1, n = p1 - p0;
             if (kn % C == 0) rebuild_window<LM>(A, tb, pos, aem, ash, wb, NA, len, kn / C, recW, recF, lane);
             const float2 qs = tabQS(tb, n);
-            const float base = vsum<LM>(ap) * qs.y;
+            float x[LM];
+#pragma unroll
+            for (int l = 0; l < LM; ++l) x[l] = a_of(l);
+            const float base = vsum<LM>(x) * qs.y;
             const uint32_t em = aem[kn];
 #pragma unroll
-            for (int l = 0; l < LM; ++l) ap[l] = ((em >> l) & 1u) ? fmaf(qs.x, ap[l], base) : 0.f;
-            const float inv = rcp_approx(vsum<LM>(ap));
+            for (int l = 0; l < LM; ++l) x[l] = ((em >> l) & 1u) ? fmaf(qs.x, x[l], base) : 0.f;
+            const float inv = rcp_approx(vsum<LM>(x));
 #pragma unroll
-            for (int l = 0; l < LM; ++l) ap[l] *= inv;
+            for (int l = 0; l < LM; ++l) set_a(l, x[l] * inv);
             load_record(kn % C);
             k = kn;
             p0 = p1;
             p1 = kn + 1 < NA ? pos[kn + 1] : len;
             in_tab = p1 - p0 < tb.NT;
         }
-        const bool all_tab = __all_sync(kAll, !on || in_tab);
-        const bool fin = (fr.y & kInfHi) != kInfHi;  // finite farg': floor term per marker
-        const bool any_fin = __any_sync(kAll, on && fin);
-        const uint32_t col = step & 31;
         if (on) {
+            const bool pair = (m & 1u) == 0u && m + 1 < p1 && m + 1 < mend;
             const uint32_t i = m - p0, j = p1 - m;
-            float2 qi, qj;
-            if (all_tab) {
-                qi = __ldg(tb.QS + i);
-                qj = __ldg(tb.QS + j);
+            float4 qa, qb;  // {Q_i, Q_i+1, S_i, S_i+1}, {Q_j, Q_j-1, S_j, S_j-1}
+            if (in_tab) {
+                qa = __ldg(tb.QSup + i);
+                qb = __ldg(tb.QSdn + j);
             } else {
-                qi = tabQS(tb, i);
-                qj = tabQS(tb, j);
+                const float2 x0 = tabQS(tb, i), x1 = tabQS(tb, i + 1), y0 = tabQS(tb, j), y1 = tabQS(tb, j - 1);
+                qa = make_float4(x0.x, x1.x, x0.y, x1.y);
+                qb = make_float4(y0.x, y1.x, y0.y, y1.y);
             }
-            float xb = qj.x, yb = fr.y == kInfHi ? 1.f : qj.y;  // uniform run: w' = 0, beta = 1
-            if (any_fin && fin) {
+            float2 XX = make_float2(qb.x, qb.y), YY = make_float2(qb.z, qb.w);
+            if (fr.y == kInfHi) {
+                YY = make_float2(1.f, 1.f);  // uniform run: w' = 0, beta = 1
+            } else if ((fr.y & kInfHi) != kInfHi) {
                 // floor e^ft beside Q w' + S; when it dominates (ft > 0) scale both by e^-ft
-                const float ft = (float)(__hiloint2double((int)fr.y, (int)fr.x) + tabG(tb, j));
-                const float e = expf(-fminf(fabsf(ft), 104.f));
-                const bool big = ft > 0.f;
-                const float xs = big ? e : 1.f;
-                const float F = big ? 1.f : (ft > -104.f ? e : 0.f);
-                xb = qj.x * xs;
-                yb = fmaf(qj.y, xs, F);
-            }
-            const float2 XF = make_float2(qi.x, qi.x), YF = make_float2(qi.y, qi.y);
-            const float2 XB = make_float2(xb, xb), YB = make_float2(yb, yb);
-            const float4* gr = reinterpret_cast<const float4*>(R.g + (size_t)m * R.gs);
-            float p[LM];
-            float2 tot2 = make_float2(0.f, 0.f), d2 = tot2;
+                const double fa = __hiloint2double((int)fr.y, (int)fr.x);
+                float ft[2] = {(float)(fa + tabG(tb, j)), (float)(fa + tabG(tb, j - 1))};
+                float xx[2] = {XX.x, XX.y}, yy[2] = {YY.x, YY.y};
 #pragma unroll
-            for (uint32_t q = 0; q < Q4; ++q) {
-                float2 p01 = __fmul2_rn(__ffma2_rn(XF, make_float2(ap[4 * q], ap[4 * q + 1]), YF),
-                                        __ffma2_rn(XB, make_float2(wp[4 * q], wp[4 * q + 1]), YB));
-                float2 p23 = __fmul2_rn(__ffma2_rn(XF, make_float2(ap[4 * q + 2], ap[4 * q + 3]), YF),
-                                        __ffma2_rn(XB, make_float2(wp[4 * q + 2], wp[4 * q + 3]), YB));
-                if (!kFull) {
-                    p01 = __fmul2_rn(p01, make_float2(act[4 * q], act[4 * q + 1]));
-                    p23 = __fmul2_rn(p23, make_float2(act[4 * q + 2], act[4 * q + 3]));
+                for (int c = 0; c < 2; ++c) {
+                    const float e = expf(-fminf(fabsf(ft[c]), 104.f));
+                    const bool big = ft[c] > 0.f;
+                    const float xs = big ? e : 1.f;
+                    const float F = big ? 1.f : (ft[c] > -104.f ? e : 0.f);
+                    yy[c] = fmaf(yy[c], xs, F);
+                    xx[c] *= xs;
                 }
-                p[4 * q] = p01.x; p[4 * q + 1] = p01.y; p[4 * q + 2] = p23.x; p[4 * q + 3] = p23.y;
-                tot2 = __fadd2_rn(tot2, __fadd2_rn(p01, p23));
-                if (kFull || 4 * q < R.gs) {
-                    const float4 gv = __ldg(gr + q);
-                    d2 = __ffma2_rn(p01, make_float2(gv.x, gv.y), d2);
-                    d2 = __ffma2_rn(p23, make_float2(gv.z, gv.w), d2);
+                XX = make_float2(xx[0], xx[1]);
+                YY = make_float2(yy[0], yy[1]);
+            }
+            const float2 QQ = make_float2(qa.x, qa.y), SS = make_float2(qa.z, qa.w);
+            float2 p2[LM];
+#pragma unroll
+            for (int l = 0; l < LM; ++l) {
+                p2[l] = __fmul2_rn(__ffma2_rn(QQ, A2(l), SS), __ffma2_rn(XX, W2(l), YY));
+                if (!kFull && (uint32_t)l >= Lr) p2[l] = make_float2(0.f, 0.f);
+            }
+            float2 t2[LM / 2];
+#pragma unroll
+            for (int l = 0; l < LM / 2; ++l) t2[l] = __fadd2_rn(p2[2 * l], p2[2 * l + 1]);
+#pragma unroll
+            for (int h = LM / 4; h >= 1; h >>= 1)
+#pragma unroll
+                for (int l = 0; l < h; ++l) t2[l] = __fadd2_rn(t2[l], t2[l + h]);
+            const float2 tot2 = t2[0];
+            float2 d2 = make_float2(0.f, 0.f);
+            const float4* g4 = reinterpret_cast<const float4*>(R.g2 + (size_t)m * R.gs);
+#pragma unroll
+            for (int q = 0; q < LM / 2; ++q) {
+                if (kFull || (uint32_t)(2 * q) < R.gs) {
+                    const float4 gv = __ldg(g4 + q);
+                    d2 = __ffma2_rn(p2[2 * q], make_float2(gv.x, gv.y), d2);
+                    d2 = __ffma2_rn(p2[2 * q + 1], make_float2(gv.z, gv.w), d2);
                 }
             }
-            const float tot = tot2.x + tot2.y;
-            const SlotMasks mk = R.masks[m];
-            uint32_t pick;
-            if (argmax) {
-                const float thr = vmax<LM>(p) * keep;
-                pick = 0;
+            uint32_t pk[2];
 #pragma unroll
-                for (int l = LM - 1; l >= 1; --l) pick = (p[l] >= thr) ? (uint32_t)l : pick;
-                if (p[0] >= thr) pick = 0;
+            for (int c = 0; c < 2; ++c) {
+                float pc[LM];
+#pragma unroll
+                for (int l = 0; l < LM; ++l) pc[l] = c ? p2[l].y : p2[l].x;
+                if (argmax) {
+                    const float thr = vmax<LM>(pc) * keep;
+                    uint32_t pick = 0;
+#pragma unroll
+                    for (int l = LM - 1; l >= 1; --l) pick = (pc[l] >= thr) ? (uint32_t)l : pick;
+                    if (pc[0] >= thr) pick = 0;
+                    pk[c] = pick;
+                } else {
+                    const float tot = c ? tot2.y : tot2.x;
+                    const float target = cell_uniform(A.seed, kPlain ? A.sid_base + s : v.sid,
+                                                      (kPlain ? 0u : v.m0) + m + c) * tot;
+                    float cum = 0.f;
+                    uint32_t last_nz = 0, pick = LM;
+#pragma unroll
+                    for (int l = 0; l < LM; ++l) {
+                        cum += pc[l];
+                        if (pc[l] > 0.f) last_nz = (uint32_t)l;
+                        if (pick == LM && target < cum) pick = (uint32_t)l;
+                    }
+                    pk[c] = pick == LM ? last_nz : pick;
+                }
+            }
+            const float2 inv2 = make_float2(rcp_approx(tot2.x), rcp_approx(tot2.y));
+            const float2 dos2 = __fmul2_rn(d2, inv2);
+            const SlotMasks mkA = R.masks[m];
+            const uint32_t hA = slot_alleles(mkA, R.raw, R.gs, m, pk[0]);
+            const uint32_t c0 = m & 31u;
+            if (thi <= tlo) {
+                tbase = m & ~31u;
+                tlo = c0;
+            }
+            if (pair) {
+                const SlotMasks mkB = R.masks[m + 1];
+                const uint32_t hB = slot_alleles(mkB, R.raw, R.gs, m + 1, pk[1]);
+                *reinterpret_cast<float2*>(tD + lane * 36 + c0) = dos2;
+                *reinterpret_cast<uint16_t*>(tH + (2 * lane) * 36 + c0) = (uint16_t)((hA & 0xffu) | ((hB & 0xffu) << 8));
+                *reinterpret_cast<uint16_t*>(tH + (2 * lane + 1) * 36 + c0) = (uint16_t)((hA >> 8) | (hB & 0xff00u));
+                if (w_hp) {
+                    float q0[2] = {0.f, 0.f}, q1[2] = {0.f, 0.f};
+#pragma unroll
+                    for (int l = 0; l < LM; ++l) {
+                        q0[0] += ((mkA.a0 >> l) & 1u) ? p2[l].x : 0.f;
+                        q1[0] += ((mkA.a1 >> l) & 1u) ? p2[l].x : 0.f;
+                        q0[1] += ((mkB.a0 >> l) & 1u) ? p2[l].y : 0.f;
+                        q1[1] += ((mkB.a1 >> l) & 1u) ? p2[l].y : 0.f;
+                    }
+                    *reinterpret_cast<float4*>(tP + lane * 34 + c0) =
+                        make_float4(q0[0] * inv2.x, q1[0] * inv2.x, q0[1] * inv2.y, q1[1] * inv2.y);
+                }
+                thi = c0 + 2;
+                m += 2;
             } else {
-                const float target = cell_uniform(A.seed, kPlain ? A.sid_base + s : v.sid, (kPlain ? 0u : v.m0) + m) * tot;
-                float cum = 0.f;
-                uint32_t last_nz = 0;
-                pick = LM;
+                tD[lane * 36 + c0] = dos2.x;
+                tH[(2 * lane) * 36 + c0] = (uint8_t)(hA & 0xffu);
+                tH[(2 * lane + 1) * 36 + c0] = (uint8_t)(hA >> 8);
+                if (w_hp) {
+                    float q0 = 0.f, q1 = 0.f;
 #pragma unroll
-                for (int l = 0; l < LM; ++l) {
-                    cum += p[l];
-                    if (p[l] > 0.f) last_nz = (uint32_t)l;
-                    if (pick == LM && target < cum) pick = (uint32_t)l;
+                    for (int l = 0; l < LM; ++l) {
+                        q0 += ((mkA.a0 >> l) & 1u) ? p2[l].x : 0.f;
+                        q1 += ((mkA.a1 >> l) & 1u) ? p2[l].x : 0.f;
+                    }
+                    tP[lane * 34 + c0] = make_float2(q0 * inv2.x, q1 * inv2.x);
                 }
-                if (pick == LM) pick = last_nz;
+                thi = c0 + 1;
+                m += 1;
             }
-            const float inv = rcp_approx(tot);
-            tD[lane * 33 + col] = (d2.x + d2.y) * inv;
-            tH[lane * 34 + col] = (uint16_t)slot_alleles(mk, R.raw, R.gs, m, pick);
-            if (w_hp) {
-                float q0 = 0.f, q1 = 0.f;
-#pragma unroll
-                for (int l = 0; l < LM; ++l) {
-                    q0 += ((mk.a0 >> l) & 1u) ? p[l] : 0.f;
-                    q1 += ((mk.a1 >> l) & 1u) ? p[l] : 0.f;
-                }
-                tP[lane * 33 + col] = make_float2(q0 * inv, q1 * inv);
-            }
-            ++m;
-            ++tcnt;
         }
-        if (col == 31) flush();
+        if (__any_sync(kAll, on && (m & 31u) == 0u)) flush();
     }
     flush();
 }

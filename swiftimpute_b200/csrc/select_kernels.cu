@@ -30,65 +30,85 @@ __device__ __forceinline__ uint32_t allele_of(const uint32_t* prow, uint32_t h, 
     return (lo < nex && (ex[lo] >> 8) == h) ? (ex[lo] & 0xffu) : 1u;
 }
 
-// Outputs (each may be null): pairs [M][L][2]; masks [M]; g [M][gs], the
-// number of non-zero alleles of each slot's pair as a float (0 past L), which
-// the posterior pass weighs by slot to form the dosage; raw [M][gs][2], the
-// pair's allele bytes (panels with alleles other than 0/1).
+// The slot haplotype of slot k at marker m (before the pair expansion).
+__device__ __forceinline__ uint32_t slot_hap(const uint32_t* hrow, uint32_t N, uint32_t L, int kind, uint32_t k) {
+    const uint32_t lane0 = min(4u, (N + 31) / 32);
+    const uint32_t top = min(N, L);
+    if (kind == SI_SEL_WARP) return (k < lane0) ? hrow[32 * k] : (k % N);
+    if (kind == SI_SEL_FIRST_PAIRS) return 2 * k;  // imputer.cpp:938-939, host checks N >= 2L
+    return (k < top) ? hrow[k] : (k % N);
+}
+
+// Outputs (each may be null): pairs [M][L][2]; masks [M]; g2 [M][gs] float2,
+// for each slot the number of non-zero alleles of its pair at m and at m + 1
+// (0 past L and past the last marker), which the posterior pass weighs by slot
+// to form the dosage of two consecutive cells; raw [M][gs][2], the pair's
+// allele bytes (panels with alleles other than 0/1).
 __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t* __restrict__ panel, uint32_t M,
                               uint32_t N, uint32_t W, uint32_t L, int kind,
                               const unsigned long long* __restrict__ ex_off, const uint32_t* __restrict__ ex_ent,
-                              uint32_t* __restrict__ pairs, SlotMasks* __restrict__ masks, float* __restrict__ g,
+                              uint32_t* __restrict__ pairs, SlotMasks* __restrict__ masks, float2* __restrict__ g2,
                               uint8_t* __restrict__ raw, uint32_t gs) {
     const uint32_t m = blockIdx.x * blockDim.x + threadIdx.x;
     if (m >= M) return;
-    const uint32_t* hrow = head ? head + (uint64_t)m * kHead : nullptr;
-    const uint32_t* prow = panel + (uint64_t)m * W;
-    const uint32_t lane0 = min(4u, (N + 31) / 32);
-    const uint32_t top = min(N, L);
-    const uint32_t* ex = ex_ent ? ex_ent + ex_off[m] : nullptr;
-    const uint32_t nex = ex_ent ? (uint32_t)(ex_off[m + 1] - ex_off[m]) : 0u;
+    auto alleles = [&](uint32_t mm, uint32_t k, uint32_t* v0, uint32_t* v1, uint32_t* h0, uint32_t* h1) {
+        const uint32_t* hrow = head ? head + (uint64_t)mm * kHead : nullptr;
+        const uint32_t* prow = panel + (uint64_t)mm * W;
+        const uint32_t* ex = ex_ent ? ex_ent + ex_off[mm] : nullptr;
+        const uint32_t nex = ex_ent ? (uint32_t)(ex_off[mm + 1] - ex_off[mm]) : 0u;
+        *h0 = slot_hap(hrow, N, L, kind, k);
+        *h1 = (*h0 + 1) % N;
+        *v0 = allele_of(prow, *h0, ex, nex);
+        *v1 = allele_of(prow, *h1, ex, nex);
+    };
     uint32_t a0 = 0, a1 = 0, x = 0;
     for (uint32_t k = 0; k < L; ++k) {
-        uint32_t h;
-        if (kind == SI_SEL_WARP) h = (k < lane0) ? hrow[32 * k] : (k % N);
-        else if (kind == SI_SEL_FIRST_PAIRS) h = 2 * k;  // imputer.cpp:938-939, host checks N >= 2L
-        else h = (k < top) ? hrow[k] : (k % N);
-        const uint32_t h1 = (h + 1) % N;
+        uint32_t v0, v1, h, h1;
+        alleles(m, k, &v0, &v1, &h, &h1);
         if (pairs) {
             pairs[((uint64_t)m * L + k) * 2 + 0] = h;
             pairs[((uint64_t)m * L + k) * 2 + 1] = h1;
         }
         if (k < 32) {
-            const uint32_t v0 = allele_of(prow, h, ex, nex), v1 = allele_of(prow, h1, ex, nex);
             a0 |= (v0 != 0u ? 1u : 0u) << k;
             a1 |= (v1 != 0u ? 1u : 0u) << k;
             x |= (v0 > 1u || v1 > 1u ? 1u : 0u) << k;
-            if (raw && k < gs) {
+        }
+        if (k < gs) {
+            if (raw) {
                 raw[((uint64_t)m * gs + k) * 2 + 0] = (uint8_t)v0;
                 raw[((uint64_t)m * gs + k) * 2 + 1] = (uint8_t)v1;
+            }
+            if (g2) {
+                float next = 0.f;
+                if (m + 1 < M) {
+                    uint32_t w0, w1, hh, hh1;
+                    alleles(m + 1, k, &w0, &w1, &hh, &hh1);
+                    next = (float)((w0 != 0u) + (w1 != 0u));
+                }
+                g2[(uint64_t)m * gs + k] = make_float2((float)((v0 != 0u) + (v1 != 0u)), next);
             }
         }
     }
     if (masks) masks[m] = SlotMasks{a0, a1, x, 0u};
-    if (g)
-        for (uint32_t k = 0; k < gs; ++k)
-            g[(uint64_t)m * gs + k] = k < L ? (float)(((a0 >> k) & 1u) + ((a1 >> k) & 1u)) : 0.f;
-    if (raw)
-        for (uint32_t k = L; k < gs; ++k) {
+    for (uint32_t k = L; k < gs; ++k) {
+        if (g2) g2[(uint64_t)m * gs + k] = make_float2(0.f, 0.f);
+        if (raw) {
             raw[((uint64_t)m * gs + k) * 2 + 0] = 0;
             raw[((uint64_t)m * gs + k) * 2 + 1] = 0;
         }
+    }
 }
 
 }  // namespace
 
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
                           uint32_t L, int kind, const unsigned long long* d_ex_off, const uint32_t* d_ex_ent,
-                          uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint8_t* d_raw, uint32_t gs,
+                          uint32_t* d_pairs, SlotMasks* d_masks, float2* d_g2, uint8_t* d_raw, uint32_t gs,
                           cudaStream_t s) {
     const uint32_t bs = 128;
     select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_ex_off, d_ex_ent, d_pairs,
-                                                   d_masks, d_g, d_raw, gs);
+                                                   d_masks, d_g2, d_raw, gs);
     return cudaGetLastError();
 }
 

@@ -192,11 +192,11 @@ void add_need(const si_server* S, Need& n, const si_request& q) {
 void trim_region_cache(si_server* S) {
     si_ctx* c = S->ctx;
     uint64_t b = 0;
-    for (auto& kv : c->region_sel) b += kv.second.masks.bytes + kv.second.g.bytes + kv.second.raw.bytes;
+    for (auto& kv : c->region_sel) b += kv.second.masks.bytes + kv.second.g2.bytes + kv.second.raw.bytes;
     if (b <= c->budget / 8) return;
     for (auto& kv : c->region_sel) {
         si::dev_free(c, kv.second.masks);
-        si::dev_free(c, kv.second.g);
+        si::dev_free(c, kv.second.g2);
         si::dev_free(c, kv.second.raw);
     }
     c->region_sel.clear();

@@ -70,7 +70,7 @@ struct SelectionCache {
     int kind = 0;
     DeviceBuffer pairs;  // [M][L][2] u32
     DeviceBuffer masks;  // [M] SlotMasks
-    DeviceBuffer g;      // [M][fb_lmax(L)] f32 ALT allele count per slot
+    DeviceBuffer g2;     // [M][fb_lmax(L)] f32x2 non-zero alleles per slot at m and m + 1
     DeviceBuffer raw;    // [M][fb_lmax(L)][2] u8 allele bytes (panels with alleles other than 0/1 only)
 };
 
@@ -124,7 +124,7 @@ struct si_ctx {
     // region-local selection tables (index restarted at the region start), per (m_begin, m_end, L, kind)
     struct RegionSel {
         si::DeviceBuffer masks;
-        si::DeviceBuffer g;
+        si::DeviceBuffer g2;
         si::DeviceBuffer raw;
     };
     std::map<std::tuple<uint32_t, uint32_t, uint32_t, int>, RegionSel> region_sel;
@@ -167,7 +167,7 @@ cudaError_t launch_panel_checksum(const uint32_t* d_words, uint64_t n, unsigned 
 // null) are the rows' exception lists, raw (may be null) receives allele bytes.
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
                           uint32_t L, int kind, const unsigned long long* d_ex_off, const uint32_t* d_ex_ent,
-                          uint32_t* d_pairs, SlotMasks* d_masks, float* d_g, uint8_t* d_raw, uint32_t gs,
+                          uint32_t* d_pairs, SlotMasks* d_masks, float2* d_g2, uint8_t* d_raw, uint32_t gs,
                           cudaStream_t s);
 
 // Compact host formats (formats.cu): 2-bit codes [rows][ceil(M/4)] -> bytes
