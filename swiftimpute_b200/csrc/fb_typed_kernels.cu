@@ -15,8 +15,8 @@
 // per-cell work runs in parallel. Kernels:
 //   anchor_count / anchor_scan / anchor_fill   per-sample anchor lists (marker 0
 //                                              is always an anchor)
-//   anchor_chain     one group of L/4 lanes (four slots each) per sample and
-//                    direction: forward and backward over anchors; backward
+//   anchor_chain     one lane per sample and direction (all slots in
+//                    registers): forward and backward over anchors; backward
 //                    checkpoints every C anchors (a window), forward ones
 //                    every K windows
 //   anchor_posterior one lane per sample walks the markers of K windows:
@@ -300,34 +300,25 @@ __device__ __forceinline__ void init_forward(float (&a)[LM], uint32_t em) {
     for (int k = 0; k < LM; ++k) a[k] = ((em >> k) & 1u) ? 1.f : 0.f;
 }
 
-// Sum over a chain's group of G lanes (aligned runs of G lanes; xor offsets
-// below G stay inside the group). Full-warp mask: every lane of the warp calls
-// it at the same step.
-template <int G>
-__device__ __forceinline__ float group_sum(float v) {
-#pragma unroll
-    for (int o = G / 2; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
-    return v;
-}
+constexpr uint32_t kChainBlock = 8;  // anchors per block of list entries
 
-constexpr uint32_t kChainBlock = 8;  // anchors per block of list entries (loaded one block ahead)
-
-// One chain per group of G = LM/4 lanes, four slots per lane. Even warps run
-// forward chains, odd warps the backward chains of the same samples. The warp
+// One chain per lane with all LM slots in registers: even warps run forward
+// chains, odd warps the backward chains of the same 32 samples. The warp
 // steps in lockstep to the longest of its chains (a finished chain holds its
-// state), in blocks of kChainBlock anchors: step j of a block is held by lane
-// j % G of the group in register j / G, loaded one block ahead and read by
-// shuffle. Checkpoints: backward vector and the log of its unit at anchors
-// k % C == 0 (window starts); forward vector at anchors k % (K C) == 0.
+// state), in blocks of kChainBlock anchors. A block's list entries are loaded
+// two blocks ahead and its run-table entries one block ahead, so a step's
+// dependent path is its own arithmetic: the slot update, the sum over the
+// slots and the power-of-two rescale (and, backward, the unit's log when
+// beta's e^-999 floor matters). Checkpoints: backward vector and the log of
+// its unit at anchors k % C == 0 (window starts); forward vector at anchors
+// k % (K C) == 0.
 template <int LM>
 __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
-    constexpr uint32_t G = LM / 4, GPW = 32 / G, R = kChainBlock / G;
-    static_assert(LM % 4 == 0 && kChainBlock % G == 0, "chain layout");
+    constexpr uint32_t KB = kChainBlock;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
     const bool forward = (wg & 1u) == 0;
-    const uint32_t gl = lane / G, kl = lane % G, g0 = gl * G, sl = kl * 4;  // sl: first slot of the lane
-    const uint32_t s = (wg >> 1) * GPW + gl;
+    const uint32_t s = (wg >> 1) * 32 + lane;
     const bool live = s < A.B;
     View v{};
     uint32_t NA = 0;
@@ -344,172 +335,168 @@ __global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
     const uint32_t* pos = A.apos + base;
     const uint32_t* aem = A.aem + base;
     const uint8_t* ash = A.ashift + base;
-    const uint32_t C = A.C;
-    auto sum4 = [](const float (&x)[4]) { return (x[0] + x[1]) + (x[2] + x[3]); };
+    const uint32_t C = A.C, K = A.K;
+    auto store = [&](float* dst, const float (&x)[LM]) {
+#pragma unroll
+        for (int q = 0; q < LM / 4; ++q)
+            reinterpret_cast<float4*>(dst)[q] = make_float4(x[4 * q], x[4 * q + 1], x[4 * q + 2], x[4 * q + 3]);
+    };
     if (forward) {
-        float a[4] = {0.f, 0.f, 0.f, 0.f};
+        // step k (anchor k = 1 .. NA - 1): the run from anchor k - 1, then anchor k's emission
+        float a[LM];
         uint32_t prev = 0;
+#pragma unroll
+        for (int l = 0; l < LM; ++l) a[l] = 0.f;
         if (NA > 0) {
-            const uint32_t e0 = aem[0] >> sl;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] = ((e0 >> i) & 1u) ? 1.f : 0.f;
+            init_forward<LM>(a, aem[0]);
             prev = pos[0];
-        }
-        float sa = group_sum<G>(sum4(a));
-        {
-            const float sc = NA > 0 ? pow2_neg(exp2_of(sa)) : 1.f;
+            const float sc = pow2_neg(exp2_of(vsum<LM>(a)));
 #pragma unroll
-            for (int i = 0; i < 4; ++i) a[i] *= sc;
-            sa *= sc;
+            for (int l = 0; l < LM; ++l) a[l] *= sc;
+            store(A.ckptF + wb * LM, a);
         }
-        if (NA > 0) *reinterpret_cast<float4*>(A.ckptF + wb * LM + sl) = make_float4(a[0], a[1], a[2], a[3]);
+        float sa = vsum<LM>(a);
         uint32_t cc = C, ci = 1;  // anchors to the next checkpoint, its window
-        uint32_t pv[R], ev[R];
+        auto load = [&](uint32_t k0, uint32_t (&p)[KB], uint32_t (&e)[KB]) {
 #pragma unroll
-        for (uint32_t i = 0; i < R; ++i) {
-            const uint32_t k = 1 + kl + G * i;
-            pv[i] = k < NA ? pos[k] : 0u;
-            ev[i] = k < NA ? aem[k] : 0u;
-        }
-        for (uint32_t k0 = 1; k0 < NAw; k0 += kChainBlock) {
-            uint32_t pn[R], en[R];
-#pragma unroll
-            for (uint32_t i = 0; i < R; ++i) {  // next block, in flight during this one
-                const uint32_t k = k0 + kChainBlock + kl + G * i;
-                pn[i] = k < NA ? pos[k] : 0u;
-                en[i] = k < NA ? aem[k] : 0u;
+            for (uint32_t j = 0; j < KB; ++j) {
+                const uint32_t k = k0 + j;
+                p[j] = k < NA ? pos[k] : 0u;
+                e[j] = k < NA ? aem[k] : 0u;
             }
-            // the block's entries and run tables first, off the dependent chain
-            uint32_t pj[kChainBlock], ej[kChainBlock];
-            float2 qj[kChainBlock];
+        };
+        auto tables = [&](uint32_t k0, const uint32_t (&p)[KB], uint32_t before, float2 (&q)[KB]) {
 #pragma unroll
-            for (uint32_t j = 0; j < kChainBlock; ++j) {
-                pj[j] = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
-                ej[j] = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
-            }
+            for (uint32_t j = 0; j < KB; ++j) q[j] = tabQS(tb, k0 + j < NA ? p[j] - (j ? p[j - 1] : before) : 0u);
+        };
+        uint32_t p0[KB], e0[KB], p1[KB], e1[KB];
+        float2 q0[KB];
+        load(1, p0, e0);
+        load(1 + KB, p1, e1);
+        tables(1, p0, prev, q0);
+        for (uint32_t k0 = 1; k0 < NAw; k0 += KB) {
+            uint32_t p2[KB], e2[KB];
+            float2 q1[KB];
+            load(k0 + 2 * KB, p2, e2);           // two blocks ahead
+            tables(k0 + KB, p1, p0[KB - 1], q1);  // one block ahead
 #pragma unroll
-            for (uint32_t j = 0; j < kChainBlock; ++j) {
-                const uint32_t before = j ? pj[j - 1] : prev;
-                qj[j] = tabQS(tb, k0 + j < NA ? pj[j] - before : 0u);
-            }
-#pragma unroll
-            for (uint32_t j = 0; j < kChainBlock; ++j) {
-                const uint32_t p = pj[j], em = ej[j];
+            for (uint32_t j = 0; j < KB; ++j) {
                 const bool act = k0 + j < NA;
-                const float2 qs = qj[j];
-                const float b = sa * qs.y;
-                float an[4];
+                const uint32_t em = e0[j];
+                const float b = sa * q0[j].y;
+                float an[LM];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) an[i] = act ? (((em >> i) & 1u) ? fmaf(qs.x, a[i], b) : 0.f) : a[i];
-                const float s2 = group_sum<G>(sum4(an));
+                for (int l = 0; l < LM; ++l) an[l] = act ? (((em >> l) & 1u) ? fmaf(q0[j].x, a[l], b) : 0.f) : a[l];
+                const float s2 = vsum<LM>(an);
                 const float sc = act ? pow2_neg(exp2_of(s2)) : 1.f;
 #pragma unroll
-                for (int i = 0; i < 4; ++i) a[i] = an[i] * sc;
+                for (int l = 0; l < LM; ++l) a[l] = an[l] * sc;
                 sa = act ? s2 * sc : sa;
-                prev = act ? p : prev;
                 cc = act ? cc - 1 : cc;
                 if (act && cc == 0) {
-                    if (ci % A.K == 0)
-                        *reinterpret_cast<float4*>(A.ckptF + (wb + ci) * LM + sl) = make_float4(a[0], a[1], a[2], a[3]);
+                    if (ci % K == 0) store(A.ckptF + (wb + ci) * LM, a);
                     ++ci;
                     cc = C;
                 }
             }
 #pragma unroll
-            for (uint32_t i = 0; i < R; ++i) {
-                pv[i] = pn[i];
-                ev[i] = en[i];
+            for (uint32_t j = 0; j < KB; ++j) {
+                p0[j] = p1[j]; e0[j] = e1[j]; q0[j] = q1[j];
+                p1[j] = p2[j]; e1[j] = e2[j];
             }
         }
     } else {
-        // step t handles anchor k = NA - 2 - t (t = 0 .. NA - 2)
-        float w[4] = {0.f, 0.f, 0.f, 0.f};
+        // step t handles anchor k = NA - 2 - t (t = 0 .. NA - 2): the run to anchor k + 1
+        float w[LM];
         uint32_t nextp = 0;
         double logU = 0.0;
+#pragma unroll
+        for (int l = 0; l < LM; ++l) w[l] = 0.f;
         if (NA > 0) {
             nextp = pos[NA - 1];
             logU = chain_end_logU(tb, v.len - 1 - nextp) - 999.0 * (double)ash[NA - 1];
-            const uint32_t eL = aem[NA - 1] >> sl;
-#pragma unroll
-            for (int i = 0; i < 4; ++i) w[i] = ((eL >> i) & 1u) ? 1.f : 0.f;
+            init_forward<LM>(w, aem[NA - 1]);
+            if ((NA - 1) % C == 0) {
+                store(A.ckptB + (wb + (NA - 1) / C) * LM, w);
+                A.ckptU[wb + (NA - 1) / C] = logU;
+            }
         }
-        float sw = group_sum<G>(sum4(w));
-        if (NA > 0 && (NA - 1) % C == 0) {
-            *reinterpret_cast<float4*>(A.ckptB + (wb + (NA - 1) / C) * LM + sl) = make_float4(w[0], w[1], w[2], w[3]);
-            if (kl == 0) A.ckptU[wb + (NA - 1) / C] = logU;
-        }
+        float sw = vsum<LM>(w);
         uint32_t cc = NA >= 2 ? (NA - 2) % C + 1 : 0u;  // anchors to the next checkpoint (k % C == 0)
         uint32_t ci = NA >= 2 ? (NA - 2) / C : 0u;      // its window
-        auto load = [&](uint32_t t, uint32_t& p, uint32_t& e, uint32_t& h) {
-            const bool ok = t + 2 <= NA;
-            const uint32_t k = NA - 2 - t;
-            p = ok ? pos[k] : 0u;
-            e = ok ? aem[k] : 0u;
-            h = ok ? ash[k] : 0u;
+        auto load = [&](uint32_t t0, uint32_t (&p)[KB], uint32_t (&e)[KB], uint32_t (&h)[KB]) {
+#pragma unroll
+            for (uint32_t j = 0; j < KB; ++j) {
+                const uint32_t t = t0 + j;
+                const bool ok = t + 2 <= NA;
+                const uint32_t k = NA - 2 - t;
+                p[j] = ok ? pos[k] : 0u;
+                e[j] = ok ? aem[k] : 0u;
+                h[j] = ok ? ash[k] : 0u;
+            }
         };
-        uint32_t pv[R], ev[R], hv[R];
+        // per step: {Q, S} of the run, G(n) - 999 and the unit's change n log rho - 999 shift
+        auto tables = [&](uint32_t t0, const uint32_t (&p)[KB], const uint32_t (&h)[KB], uint32_t after,
+                          float2 (&q)[KB], double (&g)[KB], double (&c)[KB]) {
 #pragma unroll
-        for (uint32_t i = 0; i < R; ++i) load(kl + G * i, pv[i], ev[i], hv[i]);
-        for (uint32_t t0 = 0; t0 + 1 < NAw; t0 += kChainBlock) {
-            uint32_t pn[R], en[R], hn[R];
-#pragma unroll
-            for (uint32_t i = 0; i < R; ++i) load(t0 + kChainBlock + kl + G * i, pn[i], en[i], hn[i]);
-            // the block's entries and run tables first, off the dependent chain
-            uint32_t pj[kChainBlock], ej[kChainBlock], hj[kChainBlock], nj[kChainBlock];
-            float2 qj[kChainBlock];
-            double gj[kChainBlock];
-#pragma unroll
-            for (uint32_t j = 0; j < kChainBlock; ++j) {
-                pj[j] = __shfl_sync(0xffffffffu, pv[j / G], g0 + j % G);
-                ej[j] = __shfl_sync(0xffffffffu, ev[j / G], g0 + j % G) >> sl;
-                hj[j] = __shfl_sync(0xffffffffu, hv[j / G], g0 + j % G);
+            for (uint32_t j = 0; j < KB; ++j) {
+                const uint32_t n = t0 + j + 2 <= NA ? (j ? p[j - 1] : after) - p[j] : 0u;
+                q[j] = tabQS(tb, n);
+                g[j] = tabG(tb, n) - 999.0;
+                c[j] = (double)n * tb.lr - 999.0 * (double)h[j];
             }
+        };
+        uint32_t p0[KB], e0[KB], h0[KB], p1[KB], e1[KB], h1[KB];
+        float2 q0[KB];
+        double g0[KB], c0[KB];
+        load(0, p0, e0, h0);
+        load(KB, p1, e1, h1);
+        tables(0, p0, h0, nextp, q0, g0, c0);
+        for (uint32_t t0 = 0; t0 + 1 < NAw; t0 += KB) {
+            uint32_t p2[KB], e2[KB], h2[KB];
+            float2 q1[KB];
+            double g1[KB], c1[KB];
+            load(t0 + 2 * KB, p2, e2, h2);
+            tables(t0 + KB, p1, h1, p0[KB - 1], q1, g1, c1);
 #pragma unroll
-            for (uint32_t j = 0; j < kChainBlock; ++j) {
-                const uint32_t after = j ? pj[j - 1] : nextp;
-                nj[j] = t0 + j + 2 <= NA ? after - pj[j] : 0u;
-                qj[j] = tabQS(tb, nj[j]);
-                gj[j] = tabG(tb, nj[j]);
-            }
-#pragma unroll
-            for (uint32_t j = 0; j < kChainBlock; ++j) {
-                const uint32_t p = pj[j], em = ej[j], sh = hj[j];
+            for (uint32_t j = 0; j < KB; ++j) {
                 const bool act = t0 + j + 2 <= NA;
-                const uint32_t n = nj[j];
-                const float2 qs = qj[j];
-                const double fterm = act ? -999.0 - logU + gj[j] : -1000.0;
-                // fterm > 0: the floor dominates and the unit becomes U rho^n e^fterm
+                const uint32_t em = e0[j];
+                // the floor's log in units of U: fterm > 0, the floor dominates and the unit
+                // becomes U rho^n e^fterm; fterm <= -104, it is negligible (the common case:
+                // the carried terms alone, and the unit's bookkeeping stays off this step's path)
+                const double fterm = act ? g0[j] - logU : -1000.0;
                 const bool big = fterm > 0.0;
-                const float ex = expf(-(float)fmin(fabs(fterm), 104.0));
-                const float xs = big ? ex : 1.f;                          // scale of the carried terms
-                const float F = big ? 1.f : (fterm > -104.0 ? ex : 0.f);  // the floor term
-                const float b = fmaf(xs * sw, qs.y, F), gq = xs * qs.x;
-                float wn[4];
+                float xs = 1.f, F = 0.f;
+                if (fterm > -104.0) {
+                    const float ex = expf(-(float)fmin(fabs(fterm), 104.0));
+                    xs = big ? ex : 1.f;  // scale of the carried terms
+                    F = big ? 1.f : ex;   // the floor term
+                }
+                const float b = fmaf(xs * sw, q0[j].y, F), gq = xs * q0[j].x;
+                float wn[LM];
 #pragma unroll
-                for (int i = 0; i < 4; ++i) wn[i] = act ? (((em >> i) & 1u) ? fmaf(gq, w[i], b) : 0.f) : w[i];
-                const float s2 = group_sum<G>(sum4(wn));
+                for (int l = 0; l < LM; ++l) wn[l] = act ? (((em >> l) & 1u) ? fmaf(gq, w[l], b) : 0.f) : w[l];
+                const float s2 = vsum<LM>(wn);
                 const int e = act ? exp2_of(s2) : 0;
                 const float sc = pow2_neg(e);
 #pragma unroll
-                for (int i = 0; i < 4; ++i) w[i] = wn[i] * sc;
+                for (int l = 0; l < LM; ++l) w[l] = wn[l] * sc;
                 sw = act ? s2 * sc : sw;
-                const double lu = logU + (double)n * tb.lr + (big ? fterm : 0.0) - 999.0 * (double)sh +
-                                  (double)e * 0.69314718055994530942;
+                const double lu = ((big ? g0[j] : logU) + c0[j]) + (double)e * 0.69314718055994530942;
                 logU = act ? lu : logU;
-                nextp = act ? p : nextp;
                 cc = act ? cc - 1 : cc;
                 if (act && cc == 0) {
-                    *reinterpret_cast<float4*>(A.ckptB + (wb + ci) * LM + sl) = make_float4(w[0], w[1], w[2], w[3]);
-                    if (kl == 0) A.ckptU[wb + ci] = logU;
+                    store(A.ckptB + (wb + ci) * LM, w);
+                    A.ckptU[wb + ci] = logU;
                     --ci;
                     cc = C;
                 }
             }
 #pragma unroll
-            for (uint32_t i = 0; i < R; ++i) {
-                pv[i] = pn[i];
-                ev[i] = en[i];
-                hv[i] = hn[i];
+            for (uint32_t j = 0; j < KB; ++j) {
+                p0[j] = p1[j]; e0[j] = e1[j]; h0[j] = h1[j]; q0[j] = q1[j]; g0[j] = g1[j]; c0[j] = c1[j];
+                p1[j] = p2[j]; e1[j] = e2[j]; h1[j] = h2[j];
             }
         }
     }
@@ -975,8 +962,7 @@ cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
 
 template <int LM>
 cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
-    constexpr uint32_t kChainsPerWarp = 128 / LM;  // LM / 4 lanes per chain
-    const unsigned long long warps = 2ull * ((a.B + kChainsPerWarp - 1) / kChainsPerWarp);  // forward + backward
+    const unsigned long long warps = 2ull * ((a.B + 31) / 32);  // a lane per chain, forward and backward warps
     anchor_chain_kernel<LM><<<(uint32_t)((warps + 3) / 4), 128, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
