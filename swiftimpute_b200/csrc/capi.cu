@@ -332,10 +332,14 @@ si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32
     if (!ctx->totals_ev) SI_CUDA(ctx, cudaEventCreateWithFlags(&ctx->totals_ev, cudaEventDisableTiming), "event");
     a.host_totals = ctx->pinned_totals_dev;
     a.K = kPostGroup;
-    const uint32_t B = a.B;
+    const uint32_t B = a.B, G = typed_groups(B);
+    a.nseg = typed_nseg(a.max_len);
     SI_TRY(dev_reserve(ctx, ctx->t_counts, (size_t)B * 4));
-    SI_TRY(dev_reserve(ctx, ctx->t_aoff, ((size_t)B + 1) * 8));
-    SI_TRY(dev_reserve(ctx, ctx->t_woff, ((size_t)B + 1) * 8));
+    SI_TRY(dev_reserve(ctx, ctx->t_segc, (size_t)B * a.nseg * 4));
+    a.segc = (uint32_t*)ctx->t_segc.ptr;
+    SI_TRY(dev_reserve(ctx, ctx->t_aoff, ((size_t)G + 1) * 8));
+    SI_TRY(dev_reserve(ctx, ctx->t_woff, ((size_t)G + 1) * 8));
+    a.cap = nullptr;
     a.counts = (uint32_t*)ctx->t_counts.ptr;
     a.aoff = (unsigned long long*)ctx->t_aoff.ptr;
     a.woff = (unsigned long long*)ctx->t_woff.ptr;
@@ -347,13 +351,11 @@ si_status run_typed(si_ctx* ctx, const si_impute_params* p, TypedArgs& a, uint32
     a.max_windows = (uint32_t)tot[2];
     SI_TRY(dev_reserve(ctx, ctx->t_apos, (size_t)NA * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_aem, (size_t)NA * 4));
-    SI_TRY(dev_reserve(ctx, ctx->t_acode, (size_t)NA));
     SI_TRY(dev_reserve(ctx, ctx->t_ckF, (size_t)NW * lmax * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_ckB, (size_t)NW * lmax * 4));
     SI_TRY(dev_reserve(ctx, ctx->t_ckU, (size_t)NW * 8));
     a.apos = (uint32_t*)ctx->t_apos.ptr;
     a.aem = (uint32_t*)ctx->t_aem.ptr;
-    a.ashift = (uint8_t*)ctx->t_acode.ptr;
     a.total_windows = NW;
     a.ckptF = (float*)ctx->t_ckF.ptr;
     a.ckptB = (float*)ctx->t_ckB.ptr;
@@ -373,6 +375,7 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
     a.geno = d_geno;
     a.B = B;
     a.M = ctx->M;
+    a.max_len = ctx->M;
     a.sampling = p->sampling;
     a.tie_eps = (float)p->tie_eps;
     a.seed = p->seed;
@@ -596,6 +599,13 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
         ts[j].region = jobs[j].region;
         ts[j].pad = 0;
     }
+    // Launch order: longest slices first, a region's jobs together, so the 32
+    // lanes of a warp (one group of the interleaved anchor lists) share their
+    // slice length and, for targets of one array, their typed positions. Each
+    // job still writes at its own offsets with its own sample id.
+    std::stable_sort(ts.begin(), ts.end(), [](const TypedSample& x, const TypedSample& y) {
+        return x.len != y.len ? x.len > y.len : x.region < y.region;
+    });
     return SI_OK;
 }
 
@@ -656,7 +666,7 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     dev_free(ctx, ctx->io_haps);
     dev_free(ctx, ctx->io_geno2);
     dev_free(ctx, ctx->io_hbits);
-    for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_acode, &ctx->t_aem,
+    for (si::DeviceBuffer* b : {&ctx->t_counts, &ctx->t_segc, &ctx->t_aoff, &ctx->t_woff, &ctx->t_apos, &ctx->t_aem,
                                 &ctx->t_ckF, &ctx->t_ckB, &ctx->t_ckU, &ctx->job_regions,
                                 &ctx->job_samples})
         dev_free(ctx, *b);
@@ -696,6 +706,7 @@ si_status si_panel_upload_packed(si_ctx* ctx, const uint32_t* words, uint32_t M,
     if (!ctx) return SI_ERR_INVALID_ARG;
     if (!words || M == 0 || N < 2 || words_per_row < (N + 31) / 32)
         return fail(ctx, SI_ERR_INVALID_ARG, "bad packed panel arguments (need M >= 1, N >= 2)");
+    if (M >= kMaxMarkers) return fail(ctx, SI_ERR_UNSUPPORTED, "panels hold at most 2^31 - 1 markers");
     SI_TRY(set_device(ctx));
     reset_index(ctx);
     clear_exceptions(ctx);
@@ -733,6 +744,7 @@ si_status si_panel_upload_packed(si_ctx* ctx, const uint32_t* words, uint32_t M,
 si_status si_panel_upload_u8(si_ctx* ctx, const uint8_t* alleles, uint32_t M, uint32_t N) {
     if (!ctx) return SI_ERR_INVALID_ARG;
     if (!alleles || M == 0 || N < 2) return fail(ctx, SI_ERR_INVALID_ARG, "bad panel arguments (need M >= 1, N >= 2)");
+    if (M >= kMaxMarkers) return fail(ctx, SI_ERR_UNSUPPORTED, "panels hold at most 2^31 - 1 markers");
     SI_TRY(set_device(ctx));
     reset_index(ctx);
     clear_exceptions(ctx);
@@ -1143,6 +1155,7 @@ si_status si_impute_jobs_device(si_ctx* ctx, const si_impute_params* p, const si
     a.geno = d_geno;
     a.B = n_jobs;
     a.M = 0;
+    a.max_len = ts.empty() ? 0u : ts.front().len;  // jobs are ordered longest first
     a.sampling = p->sampling;
     a.tie_eps = (float)p->tie_eps;
     a.seed = p->seed;

@@ -60,15 +60,22 @@ struct TypedArgs {
     TypedRegion reg0;                // the region of a plain batch
     const TypedRegion* regions;      // device array, uneven batches (else null)
     const TypedSample* samples;      // device array, uneven batches (else null)
-    unsigned long long* aoff;        // [B+1] anchor offsets (exact, or per-job capacities in a plan)
-    unsigned long long* woff;        // [B+1] window offsets (likewise)
+    // Anchor lists and window checkpoints are interleaved over groups of 32
+    // consecutive samples (a warp's lanes): entry k of sample s sits at
+    // aoff[s / 32] + 32 k + s % 32, window w at woff[s / 32] + 32 w + s % 32,
+    // so the lanes of a warp reading the same anchor share cache lines.
+    unsigned long long* aoff;        // [G+1] list offsets of the groups (32 x the group's most anchors, or capacities)
+    unsigned long long* woff;        // [G+1] window offsets of the groups (likewise)
     uint32_t* counts;                // [B] anchors of each job (written by the count kernel)
-    int capacity;                    // offsets are capacities fixed in advance: clamp counts to them
+    uint32_t* segc;                  // [B][nseg] anchors in each segment of kFillSeg markers (count kernel)
+    uint32_t nseg;                   // segments of the longest job: ceil(max_len / kFillSeg)
+    uint32_t max_len;                // markers of the longest job (M for a plain batch)
+    const uint32_t* cap;             // [B] anchor capacity of each job (a plan), else null: every anchor is listed
     uint32_t* err;                   // device flag: bit 0 set when a job had more anchors than its capacity
     unsigned long long* host_totals; // mapped host memory: anchors, windows, most windows of a sample (may be null)
-    uint32_t* apos;                  // anchor positions (within the slice)
+    uint32_t* apos;                  // anchor position within the slice | 1 << 31 where no slot matches the call
+                                     // (every slot scaled by e^-999)
     uint32_t* aem;                   // anchor emission masks over the slots
-    uint8_t* ashift;                 // 1 where no slot matches the call (every slot scaled by e^-999)
     unsigned long long total_windows;
     float* ckptF;                    // [windows][Lmax] forward anchor at the first anchor of every K-th window
     float* ckptB;                    // [windows][Lmax] backward anchor (E . beta, scaled)
@@ -84,6 +91,10 @@ cudaError_t launch_anchor_count_only(const TypedArgs& a, cudaStream_t s);   // c
 cudaError_t launch_anchor_lists_fill(const TypedArgs& a, cudaStream_t s);
 cudaError_t launch_typed_fb(const TypedArgs& a, uint32_t lmax, bool all_full, cudaStream_t s);
 size_t typed_post_smem_bytes(uint32_t L, uint32_t T, uint32_t C);
+inline uint32_t typed_groups(uint32_t B) { return (B + 31) / 32; }  // 32-sample groups of the interleaved lists
+constexpr uint32_t kShiftBit = 0x80000000u;                         // apos: no slot matches the call
+constexpr uint32_t kFillSeg = 4096;                                 // markers per warp of the list fill (x 512)
+inline uint32_t typed_nseg(uint32_t max_len) { return (max_len + kFillSeg - 1) / kFillSeg; }
 // Uneven batches (capi.cu): argument checks, and the region tables and job
 // descriptors of a batch (region sweeps and selections not cached yet run on s).
 si_status check_jobs_args(si_ctx* ctx, const si_impute_params* p, const si_region* regions, uint32_t n_regions,

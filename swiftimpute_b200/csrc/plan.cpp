@@ -30,8 +30,9 @@ struct si_plan {
     uint32_t lmax = 4;
     bool all_full = true;
     uint32_t B = 0;
-    std::vector<unsigned long long> cap;  // anchor capacity per job
-    si::DeviceBuffer regions, samples, counts, aoff, woff, apos, aem, acode, ckF, ckB, ckU, err;
+    std::vector<uint32_t> cap;             // anchor capacity per job (launch order)
+    std::vector<unsigned long long> gcap;  // per 32-job group of the interleaved lists: its jobs' largest capacity
+    si::DeviceBuffer regions, samples, counts, segc, jcap, aoff, woff, apos, aem, ckF, ckB, ckU, err;
     uint32_t C = 2, T = 128;
     float best_ms = 0.f;
     cudaStream_t capture_stream = nullptr;
@@ -48,17 +49,18 @@ void free_plan(si_plan* P) {
     if (P->exec) cudaGraphExecDestroy(P->exec);
     if (P->graph) cudaGraphDestroy(P->graph);
     if (P->capture_stream) cudaStreamDestroy(P->capture_stream);
-    for (DeviceBuffer* b : {&P->regions, &P->samples, &P->counts, &P->aoff, &P->woff, &P->apos, &P->aem, &P->acode,
+    for (DeviceBuffer* b : {&P->regions, &P->samples, &P->counts, &P->segc, &P->jcap, &P->aoff, &P->woff, &P->apos, &P->aem,
                             &P->ckF, &P->ckB, &P->ckU, &P->err})
         si::dev_free(c, *b);
     delete P;
 }
 
-// Window offsets for window size C and the window count.
-std::vector<unsigned long long> window_offsets(const std::vector<unsigned long long>& cap, uint32_t C) {
-    std::vector<unsigned long long> w(cap.size() + 1, 0);
-    for (size_t j = 0; j < cap.size(); ++j) w[j + 1] = w[j] + (cap[j] + C - 1) / C;
-    return w;
+// Group offsets of the interleaved lists (32 entries per anchor of a group's
+// capacity) or, with C > 0, of its window checkpoints (32 per window).
+std::vector<unsigned long long> group_offsets(const std::vector<unsigned long long>& gcap, uint32_t C) {
+    std::vector<unsigned long long> o(gcap.size() + 1, 0);
+    for (size_t g = 0; g < gcap.size(); ++g) o[g + 1] = o[g] + 32ull * (C ? (gcap[g] + C - 1) / C : gcap[g]);
+    return o;
 }
 
 cudaError_t enqueue(si_plan* P, cudaStream_t s) {
@@ -70,7 +72,7 @@ cudaError_t enqueue(si_plan* P, cudaStream_t s) {
 
 // Use window size C and CTA size T: upload the window offsets, set the args.
 si_status use_tiles(si_plan* P, uint32_t C, uint32_t T, cudaStream_t s) {
-    const auto w = window_offsets(P->cap, C);
+    const auto w = group_offsets(P->gcap, C);
     const cudaError_t e = cudaMemcpyAsync(P->woff.ptr, w.data(), w.size() * 8, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) {
         const cudaError_t f = cudaStreamSynchronize(s);  // the host vector dies here
@@ -79,7 +81,7 @@ si_status use_tiles(si_plan* P, uint32_t C, uint32_t T, cudaStream_t s) {
         return si::cuda_fail(P->ctx, e, "plan window offsets");
     }
     unsigned long long most = 0;
-    for (unsigned long long c : P->cap) most = std::max(most, (c + C - 1) / C);
+    for (unsigned long long c : P->gcap) most = std::max(most, (c + C - 1) / C);
     P->a.C = C;
     P->a.threads = T;
     P->a.K = si::kPostGroup;
@@ -117,26 +119,30 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
         return st;
     }
     // capacities: marker 0 and the typed markers, at most the job's length
+    const uint32_t G = si::typed_groups(n_jobs);
     P->cap.resize(n_jobs);
-    std::vector<unsigned long long> aoff(n_jobs + 1, 0);
+    P->gcap.assign(G, 0);
     for (uint32_t j = 0; j < n_jobs; ++j) {
-        const unsigned long long len = ts[j].len;
-        P->cap[j] = max_anchors ? std::min<unsigned long long>(len, max_anchors) : len;
-        aoff[j + 1] = aoff[j] + P->cap[j];
+        const uint32_t len = ts[j].len;
+        P->cap[j] = max_anchors ? std::min(len, max_anchors) : len;
+        P->gcap[j / 32] = std::max<unsigned long long>(P->gcap[j / 32], P->cap[j]);
     }
+    const std::vector<unsigned long long> aoff = group_offsets(P->gcap, 0);
     const unsigned long long NA = aoff.back();
     const uint32_t Cmin = p->checkpoint_interval ? p->checkpoint_interval : 1;
-    const unsigned long long NWmax = window_offsets(P->cap, Cmin).back();
+    const unsigned long long NWmax = group_offsets(P->gcap, Cmin).back();
     const uint32_t lm = P->lmax;
     auto alloc = [&](DeviceBuffer& b, size_t bytes) { return st == SI_OK ? (st = si::dev_alloc(ctx, b, bytes)) : st; };
     alloc(P->regions, tr.size() * sizeof(si::TypedRegion));
     alloc(P->samples, ts.size() * sizeof(si::TypedSample));
+    const uint32_t max_len = ts.empty() ? 0u : ts.front().len;  // jobs are ordered longest first
     alloc(P->counts, (size_t)n_jobs * 4);
-    alloc(P->aoff, ((size_t)n_jobs + 1) * 8);
-    alloc(P->woff, ((size_t)n_jobs + 1) * 8);
+    alloc(P->segc, (size_t)n_jobs * si::typed_nseg(max_len) * 4);
+    alloc(P->jcap, (size_t)n_jobs * 4);
+    alloc(P->aoff, ((size_t)G + 1) * 8);
+    alloc(P->woff, ((size_t)G + 1) * 8);
     alloc(P->apos, (size_t)NA * 4);
     alloc(P->aem, (size_t)NA * 4);
-    alloc(P->acode, (size_t)NA);
     alloc(P->ckF, (size_t)NWmax * lm * 4);
     alloc(P->ckB, (size_t)NWmax * lm * 4);
     alloc(P->ckU, (size_t)NWmax * 8);
@@ -149,6 +155,7 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(P->samples.ptr, ts.data(), ts.size() * sizeof(si::TypedSample), cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemcpyAsync(P->aoff.ptr, aoff.data(), aoff.size() * 8, cudaMemcpyHostToDevice, s);
+    if (e == cudaSuccess) e = cudaMemcpyAsync(P->jcap.ptr, P->cap.data(), (size_t)n_jobs * 4, cudaMemcpyHostToDevice, s);
     if (e == cudaSuccess) e = cudaMemsetAsync(P->err.ptr, 0, 4, s);
     if (e == cudaSuccess) e = cudaStreamSynchronize(s);
     if (e != cudaSuccess) {
@@ -166,13 +173,15 @@ si_status si_plan_create(si_ctx* ctx, const si_impute_params* p, const si_region
     a.regions = (const si::TypedRegion*)P->regions.ptr;
     a.samples = (const si::TypedSample*)P->samples.ptr;
     a.counts = (uint32_t*)P->counts.ptr;
+    a.max_len = max_len;
+    a.nseg = si::typed_nseg(max_len);
+    a.segc = (uint32_t*)P->segc.ptr;
     a.aoff = (unsigned long long*)P->aoff.ptr;
     a.woff = (unsigned long long*)P->woff.ptr;
-    a.capacity = 1;
+    a.cap = (const uint32_t*)P->jcap.ptr;
     a.err = (uint32_t*)P->err.ptr;
     a.apos = (uint32_t*)P->apos.ptr;
     a.aem = (uint32_t*)P->aem.ptr;
-    a.ashift = (uint8_t*)P->acode.ptr;
     a.ckptF = (float*)P->ckF.ptr;
     a.ckptB = (float*)P->ckB.ptr;
     a.ckptU = (double*)P->ckU.ptr;

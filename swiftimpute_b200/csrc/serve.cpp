@@ -9,6 +9,7 @@
 // staging slots alternate: while the worker runs launch k+1 on the device, a
 // completion thread waits for launch k's copies and scatters its outputs into
 // the requests' own buffers.
+#include "fb_typed.hpp"
 #include "si_internal.hpp"
 
 #include <algorithm>
@@ -50,15 +51,19 @@ double ms_between(Clock::time_point a, Clock::time_point b) {
 // Device bytes one launch may need beyond what the ctx keeps between calls,
 // an upper bound: inputs and outputs, anchor lists (every marker typed at
 // worst), window checkpoints (two anchors per window), job descriptors, and
-// the temporary index sweep of a region-local slice not cached yet.
+// the temporary index sweep of a region-local slice not cached yet. The lists
+// of a 32-job group take 32 x its longest job; with jobs ordered longest
+// first, the groups' first jobs sum to at most the cells plus one longest job
+// per lane, hence cells + 32 max_len.
 struct Need {
     uint64_t cells = 0, jobs = 0, sweep = 0;
-    uint32_t lmax = 4;
+    uint32_t lmax = 4, max_len = 0;
     bool hap_prob = false;
     uint64_t bytes() const {
         const uint64_t io = cells * (1 + 4 + 2) + (hap_prob ? cells * 8 : 0);
-        const uint64_t lists = cells * 9 + jobs * (4 + 8 + 8 + 64);
-        const uint64_t windows = cells / 2 + jobs;
+        const uint64_t slots = cells + 32ull * max_len;
+        const uint64_t lists = slots * 8 + jobs * (4 + 4 + 8 + 8 + 64) + jobs * 4ull * si::typed_nseg(max_len);
+        const uint64_t windows = slots / 2 + jobs + 32;
         const uint64_t ckpt = windows * (2ull * lmax * 4 + 8 + 4);
         return io + lists + ckpt + sweep + (1ull << 20);
     }
@@ -159,7 +164,7 @@ uint64_t reclaimable(const si_server* S, int k) {
     const si_ctx* c = S->ctx;
     const auto& z = S->slot[k];
     uint64_t b = 0;
-    for (const si::DeviceBuffer* x : {&c->t_counts, &c->t_aoff, &c->t_woff, &c->t_apos, &c->t_acode, &c->t_aem,
+    for (const si::DeviceBuffer* x : {&c->t_counts, &c->t_segc, &c->t_aoff, &c->t_woff, &c->t_apos, &c->t_aem,
                                       &c->t_ckF, &c->t_ckB, &c->t_ckU, &c->job_regions,
                                       &c->job_samples, &z.d_geno, &z.d_dos, &z.d_haps, &z.d_hp})
         b += x->bytes;
@@ -177,6 +182,7 @@ uint64_t headroom(const si_server* S, int k) {
 void add_need(const si_server* S, Need& n, const si_request& q) {
     n.cells += cells_of(q);
     n.jobs += q.n_samples;
+    n.max_len = std::max(n.max_len, q.m_end - q.m_begin);
     n.lmax = std::max(n.lmax, lmax_of(q.num_states));
     n.hap_prob |= q.hap_prob != nullptr;
     if (q.index_origin == SI_INDEX_REGION) {

@@ -32,13 +32,14 @@ inline uint32_t words_per_row_pad(uint32_t N) { return ((N + 31) / 32 + 3) & ~3u
 // reads positions 0, 32, 64, 96 and the insertion pattern positions 0..L-1
 // (L <= 64), so the first 128 entries of each row cover every pattern.
 constexpr uint32_t kHead = 128;
+constexpr uint32_t kMaxMarkers = 0x80000000u;  // anchor lists keep a flag in bit 31 of a position
 
 // Per-marker slot data consumed by the forward-backward kernels: for slot k,
 // bit k of a0 / a1 is set when the pair's first / second haplotype carries a
 // non-zero allele (the PBWT's "1" side), and bit k of x when either of its
 // alleles is neither 0 nor 1 (missing, 255, or multi-allelic); such slots take
 // their allele bytes from the selection's raw table.
-struct SlotMasks {
+struct alignas(16) SlotMasks {
     uint32_t a0;
     uint32_t a1;
     uint32_t x;
@@ -115,7 +116,7 @@ struct si_ctx {
     si::LinTrans trans0{1.f, 0.f};  // host copy of the first gap's transition
     si::DeviceBuffer ckpt;           // forward checkpoints (full-chain kernel)
     // typed-marker kernel scratch and tables
-    si::DeviceBuffer t_counts, t_aoff, t_woff, t_apos, t_acode, t_aem, t_ckF, t_ckB, t_ckU;
+    si::DeviceBuffer t_counts, t_segc, t_aoff, t_woff, t_apos, t_aem, t_ckF, t_ckB, t_ckU;
     struct TableSet {
         si::DeviceBuffer QS, G;
         double consts[4] = {0, 0, 0, 0};  // log2q, lr, lgc, regime
