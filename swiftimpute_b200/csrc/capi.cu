@@ -508,7 +508,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
         for (uint32_t q : sweep_region)
             if (regions[q].m_begin == g.m_begin && regions[q].m_end == g.m_end) dup = true;
         if (dup) continue;
-        sweeps.push_back(SweepJob{g.m_begin, g.m_end - g.m_begin, head_rows * kHead});
+        sweeps.push_back(SweepJob{g.m_begin, g.m_end - g.m_begin, head_rows * kHead, kIota});
         sweep_region.push_back(r);
         head_rows += g.m_end - g.m_begin;
     }
@@ -523,7 +523,7 @@ si_status prepare_jobs(si_ctx* ctx, const si_impute_params* p, const si_region* 
             e = cudaMemcpyAsync(jb.ptr, sweeps.data(), sweeps.size() * sizeof(SweepJob), cudaMemcpyHostToDevice, s);
         if (st == SI_OK && e == cudaSuccess)
             e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, (const SweepJob*)jb.ptr, (uint32_t)sweeps.size(),
-                                  N, W, (uint32_t*)head.ptr, nullptr, nullptr, (uint32_t*)perm.ptr, s);
+                                  N, W, nullptr, (uint32_t*)head.ptr, nullptr, nullptr, (uint32_t*)perm.ptr, s);
         // selection tables of every region (and slot count) that uses these sweeps
         for (uint32_t r = 0; st == SI_OK && e == cudaSuccess && r < n_regions; ++r) {
             const si_region& g = regions[r];
@@ -822,21 +822,57 @@ si_status si_pbwt_build(si_ctx* ctx, uint32_t flags) {
         SI_TRY(dev_alloc(ctx, ctx->row_hash, (size_t)M * 8));
         SI_CUDA(ctx, cudaMemsetAsync(ctx->row_hash.ptr, 0, (size_t)M * 8, ctx->stream), "memset hash");
     }
-    DeviceBuffer perm, jobbuf;
-    SI_TRY(dev_alloc(ctx, perm, (size_t)2 * N * 4));
-    SI_TRY(dev_alloc(ctx, jobbuf, sizeof(SweepJob)));
-    const SweepJob job{0, M, 0};
-    cudaError_t e = cudaMemcpy(jobbuf.ptr, &job, sizeof job, cudaMemcpyHostToDevice);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
-    if (e == cudaSuccess)
-        e = launch_pbwt_sweep((const uint32_t*)ctx->panel.ptr, (const SweepJob*)jobbuf.ptr, 1, N, ctx->W,
-                              (uint32_t*)ctx->head.ptr, (uint32_t*)ctx->prefix.ptr,
-                              (unsigned long long*)ctx->row_hash.ptr, (uint32_t*)perm.ptr, ctx->stream);
-    if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
-    if (e == cudaSuccess) e = cudaEventElapsedTime(&ctx->pbwt_ms, ctx->ev[0], ctx->ev[1]);
-    dev_free(ctx, perm);
-    dev_free(ctx, jobbuf);
+    // Segments of at least kMinSegment markers, one per SM: the groups pass and
+    // the final sweep run every segment on its own CTA, the composition of the
+    // segments' start orders runs once per segment (pbwt_kernels.cu).
+    constexpr uint32_t kMinSegment = 64;
+    int nsm = 148;
+    cudaDeviceGetAttribute(&nsm, cudaDevAttrMultiProcessorCount, ctx->device);
+    const uint32_t S0 = std::max(1u, std::min<uint32_t>((uint32_t)nsm, M / kMinSegment));
+    const uint32_t Lseg = (M + S0 - 1) / S0;
+    const uint32_t S = (M + Lseg - 1) / Lseg;
+    std::vector<SweepJob> jobs(S);
+    for (uint32_t j = 0; j < S; ++j)
+        jobs[j] = SweepJob{j * Lseg, std::min(Lseg, M - j * Lseg), (uint64_t)j * Lseg * kHead,
+                           j == 0 ? kIota : (uint64_t)j * N};
+    int max_optin = 0;
+    cudaDeviceGetAttribute(&max_optin, cudaDevAttrMaxSharedMemoryPerBlockOptin, ctx->device);
+    const bool sweep_global = pbwt_sweep_smem_bytes(N, ctx->W) > (size_t)max_optin;
+    const bool group_global = S > 1 && pbwt_group_smem_bytes(N, ctx->W) > (size_t)max_optin;
+    const size_t scratch_words = std::max<size_t>(sweep_global ? (size_t)2 * N * S : 0,
+                                                  group_global ? (size_t)4 * N * (S - 1) : 0);
+    DeviceBuffer scratch, jobbuf, orders, gid, sortbuf;
+    si_status st = dev_alloc(ctx, jobbuf, S * sizeof(SweepJob));
+    if (st == SI_OK && scratch_words) st = dev_alloc(ctx, scratch, scratch_words * 4);
+    if (st == SI_OK && S > 1) st = dev_alloc(ctx, orders, (size_t)S * N * 4);
+    if (st == SI_OK && S > 1) st = dev_alloc(ctx, gid, (size_t)(S - 1) * N * 4);
+    if (st == SI_OK && S > 1) st = dev_alloc(ctx, sortbuf, (size_t)4 * N * 4);
+    cudaError_t e = cudaSuccess;
+    if (st == SI_OK) {
+        e = cudaMemcpy(jobbuf.ptr, jobs.data(), S * sizeof(SweepJob), cudaMemcpyHostToDevice);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[0], ctx->stream);
+        const uint32_t* panel = (const uint32_t*)ctx->panel.ptr;
+        const SweepJob* dj = (const SweepJob*)jobbuf.ptr;
+        uint32_t* ord = (uint32_t*)orders.ptr;
+        if (e == cudaSuccess && S > 1) {
+            e = launch_iota(ord, N, ctx->stream);
+            if (e == cudaSuccess)
+                e = launch_pbwt_groups(panel, dj, S - 1, N, ctx->W, (uint32_t*)gid.ptr, (uint32_t*)scratch.ptr,
+                                       ctx->stream);
+            for (uint32_t j = 0; e == cudaSuccess && j + 1 < S; ++j)
+                e = launch_pbwt_compose(ord + (size_t)j * N, (const uint32_t*)gid.ptr + (size_t)j * N,
+                                        ord + (size_t)(j + 1) * N, N, (uint32_t*)sortbuf.ptr, ctx->stream);
+        }
+        if (e == cudaSuccess)
+            e = launch_pbwt_sweep(panel, dj, S, N, ctx->W, ord, (uint32_t*)ctx->head.ptr,
+                                  (uint32_t*)ctx->prefix.ptr, (unsigned long long*)ctx->row_hash.ptr,
+                                  (uint32_t*)scratch.ptr, ctx->stream);
+        if (e == cudaSuccess) e = cudaEventRecord(ctx->ev[1], ctx->stream);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&ctx->pbwt_ms, ctx->ev[0], ctx->ev[1]);
+    }
+    for (DeviceBuffer* b : {&scratch, &jobbuf, &orders, &gid, &sortbuf}) dev_free(ctx, *b);
+    if (st != SI_OK) return st;
     if (e != cudaSuccess) return cuda_fail(ctx, e, "PBWT sweep");
     ctx->has_index = true;
     ctx->pbwt_flags = flags;

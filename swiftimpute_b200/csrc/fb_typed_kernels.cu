@@ -81,6 +81,24 @@ __device__ __forceinline__ double tabG(const Tabs& t, uint32_t n) {
     return log((double)n);
 }
 
+// asynchronous global -> shared copies (cp.async); a thread waits for its own copies
+__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
+    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
+    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
+                 : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait_group() { asm volatile("cp.async.wait_group %0;" ::"n"(N) : "memory"); }
+
 // ---------------------------------------------------------------- anchor lists
 
 constexpr uint32_t kWarpsPerBlock = 8;
@@ -91,8 +109,10 @@ __device__ __forceinline__ uint4 load16(const uint8_t* g, uint32_t base, uint32_
     if (base >= len) return make_uint4(0x03030303u, 0x03030303u, 0x03030303u, 0x03030303u);
     if (vec && base + 16 <= len) return *reinterpret_cast<const uint4*>(g + base);
     uint32_t w[4] = {0x03030303u, 0x03030303u, 0x03030303u, 0x03030303u};
-    for (uint32_t j = 0; j < 16 && base + j < len; ++j)
-        w[j >> 2] = (w[j >> 2] & ~(0xffu << (8 * (j & 3)))) | ((uint32_t)g[base + j] << (8 * (j & 3)));
+#pragma unroll
+    for (uint32_t j = 0; j < 16; ++j)  // unrolled: the word index is a constant, w stays in registers
+        if (base + j < len)
+            w[j >> 2] = (w[j >> 2] & ~(0xffu << (8 * (j & 3)))) | ((uint32_t)g[base + j] << (8 * (j & 3)));
     return make_uint4(w[0], w[1], w[2], w[3]);
 }
 
@@ -221,24 +241,22 @@ __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __res
 // Anchor lists: marker position (with the "no slot matches" flag, which
 // scales every slot by e^-999, counted in beta's unit, in bit 31) and emission
 // mask over the slots, in marker order; marker 0 is always an anchor. A warp
-// fills one segment of kFillSeg markers of the 32 samples of a group, lane =
-// sample: chunks of 32 rows x 512 codes come into shared memory as coalesced
-// row loads, each lane scans its own row there, and lanes that meet their
-// anchors in step (shared typed positions) write whole 128-byte lines of the
-// interleaved lists. A lane's first entry of the segment is the sum of its
-// earlier segments' counts.
-constexpr uint32_t kFillWarps = 2;  // 33 KB of shared memory per CTA
+// (one CTA) fills one segment of kFillSeg markers of the 32 samples of a
+// group, lane = sample: chunks of 32 rows x 512 codes come into shared memory
+// by cp.async, the next chunk in flight while each lane scans its own row of
+// the current one, and lanes that meet their anchors in step (shared typed
+// positions) write whole 128-byte lines of the interleaved lists. A lane's
+// first entry of the segment is the sum of its earlier segments' counts.
 constexpr uint32_t kFillRow = 512 + 16;  // row stride in shared memory (bytes): conflict-free 128-bit reads
+constexpr size_t kFillSmem = 2 * 32 * kFillRow + 32 * 16;  // two chunk buffers and the row descriptors
 
-__global__ void __launch_bounds__(kFillWarps * 32) anchor_fill_kernel(TypedArgs A) {
+__global__ void __launch_bounds__(32) anchor_fill_kernel(TypedArgs A) {
     extern __shared__ __align__(16) unsigned char fsm[];
-    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-    const unsigned long long gw = (unsigned long long)blockIdx.x * kFillWarps + warp;
+    const uint32_t lane = threadIdx.x;
     const uint32_t G = (A.B + 31) / 32;
-    if (gw >= (unsigned long long)G * A.nseg) return;  // whole warp
-    const uint32_t g = (uint32_t)(gw % G), seg = (uint32_t)(gw / G);
+    const uint32_t g = blockIdx.x % G, seg = blockIdx.x / G;
     const uint32_t s = g * 32 + lane;
-    unsigned char* tile = fsm + (size_t)warp * 32 * kFillRow;
+    uint4* rowd = reinterpret_cast<uint4*>(fsm + 2 * 32 * kFillRow);  // [32] {ptr lo, ptr hi, len, 16-byte aligned}
     View v{};
     uint32_t len = 0, at = 0, lim = 0;
     if (s < A.B) {
@@ -251,35 +269,50 @@ __global__ void __launch_bounds__(kFillWarps * 32) anchor_fill_kernel(TypedArgs 
     const uint32_t m0 = seg * kFillSeg;
     const uint32_t mlast = __reduce_max_sync(0xffffffffu, len);
     if (m0 >= mlast) return;  // whole warp: no row reaches this segment
+    const unsigned long long gp = reinterpret_cast<unsigned long long>(v.geno);
+    rowd[lane] = make_uint4((uint32_t)gp, (uint32_t)(gp >> 32), len, (gp & 15u) == 0 ? 1u : 0u);
+    __syncwarp();
     const uint32_t lmask = lmask_of(v.r.L);
     const unsigned long long lb = A.aoff[g] + lane;
-    const bool vec = (reinterpret_cast<uintptr_t>(v.geno) & 15u) == 0;
-    const unsigned long long gp = reinterpret_cast<unsigned long long>(v.geno);
-    for (uint32_t c0 = m0; c0 < min(m0 + kFillSeg, mlast); c0 += 512) {
-        // row r's 512 codes from c0: lane i loads bytes [16 i, 16 i + 16)
+    // chunk at c0 into b: lane i copies bytes [16 i, 16 i + 16) of every row
+    auto issue = [&](uint32_t c0, unsigned char* b) {
+        const uint32_t mm = c0 + 16 * lane;
 #pragma unroll 8
         for (uint32_t r = 0; r < 32; ++r) {
-            const uint8_t* gr = reinterpret_cast<const uint8_t*>(__shfl_sync(0xffffffffu, gp, r));
-            const uint32_t lr = __shfl_sync(0xffffffffu, len, r);
-            const bool vr = __shfl_sync(0xffffffffu, vec, r);
-            *reinterpret_cast<uint4*>(tile + r * kFillRow + 16 * lane) = load16(gr, c0 + 16 * lane, lr, vr);
+            const uint4 d = rowd[r];
+            const uint8_t* gr = reinterpret_cast<const uint8_t*>(((unsigned long long)d.y << 32) | d.x);
+            unsigned char* dst = b + r * kFillRow + 16 * lane;
+            if (d.w && mm + 16 <= d.z) cp_async16(dst, gr + mm);
+            else *reinterpret_cast<uint4*>(dst) = load16(gr, mm, d.z, d.w != 0);  // a ragged or unaligned row
         }
-        __syncwarp();
+        cp_async_commit();
+    };
+    const uint32_t cend = min(m0 + kFillSeg, mlast);
+    issue(m0, fsm);
+    uint32_t bi = 0;
+    for (uint32_t c0 = m0; c0 < cend; c0 += 512, bi ^= 1) {
+        if (c0 + 512 < cend) {
+            issue(c0 + 512, fsm + (bi ^ 1) * 32 * kFillRow);
+            cp_async_wait_group<1>();  // this lane's copies of the current chunk have landed
+        } else {
+            cp_async_wait_group<0>();
+        }
+        __syncwarp();  // ... and every lane's
         if (c0 < len) {
+            const unsigned char* row = fsm + bi * 32 * kFillRow + lane * kFillRow;
             for (uint32_t q = 0; q < 32; ++q) {
-                const uint4 x = *reinterpret_cast<const uint4*>(tile + lane * kFillRow + 16 * q);
+                const uint4 x = *reinterpret_cast<const uint4*>(row + 16 * q);
                 uint32_t bits = typed_bits(x);
                 const uint32_t base = c0 + 16 * q;
                 if (base == 0) bits |= 1u;
-                const uint32_t cw[4] = {x.x, x.y, x.z, x.w};
                 while (bits) {
                     const uint32_t j = __ffs(bits) - 1;
                     bits &= bits - 1;
                     const uint32_t m = base + j;
                     if (at < lim) {
                         uint32_t sh;
-                        const uint32_t em = emission_mask((cw[j >> 2] >> (8 * (j & 3))) & 0xffu, v.r.masks[m], lmask,
-                                                          &sh);
+                        const uint32_t w = j < 8 ? (j < 4 ? x.x : x.y) : (j < 12 ? x.z : x.w);
+                        const uint32_t em = emission_mask((w >> (8 * (j & 3))) & 0xffu, v.r.masks[m], lmask, &sh);
                         A.apos[lb + 32ull * at] = m | (sh ? kShiftBit : 0u);
                         A.aem[lb + 32ull * at] = em;
                     }
@@ -287,7 +320,7 @@ __global__ void __launch_bounds__(kFillWarps * 32) anchor_fill_kernel(TypedArgs 
                 }
             }
         }
-        __syncwarp();
+        __syncwarp();  // the buffer is read before it is refilled
     }
 }
 
@@ -386,7 +419,7 @@ constexpr uint32_t kChainBlock = 8;  // anchors per block of list entries
 // its unit at anchors k % C == 0 (window starts); forward vector at anchors
 // k % (K C) == 0.
 template <int LM>
-__global__ void __launch_bounds__(128) anchor_chain_kernel(TypedArgs A) {
+__global__ void __launch_bounds__(32) anchor_chain_kernel(TypedArgs A) {
     constexpr uint32_t KB = kChainBlock;
     const uint32_t lane = threadIdx.x & 31;
     const uint32_t wg = (blockIdx.x * blockDim.x + threadIdx.x) >> 5;
@@ -655,21 +688,26 @@ __device__ __forceinline__ float vmax(const float (&p)[LM]) {
     return m;
 }
 
-// asynchronous global -> shared copies of a lane's own words (sm_80+ cp.async)
-__device__ __forceinline__ void cp_async4(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 4;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
+
+// Argmax picks of two cells: the first slot with p >= (1 - eps) max; the
+// sign of p - thr marks the slots below the threshold.
+template <int LM>
+__device__ __forceinline__ void pick_pair(const float2 (&p2)[LM], float keep, uint32_t& k0, uint32_t& k1) {
+    float px[LM], py[LM];
+#pragma unroll
+    for (int l = 0; l < LM; ++l) { px[l] = p2[l].x; py[l] = p2[l].y; }
+    const float2 thr2 = __fmul2_rn(make_float2(vmax<LM>(px), vmax<LM>(py)), make_float2(-keep, -keep));
+    uint32_t bx = 0u, by = 0u;  // bit LM-1-l: slot l below the threshold
+#pragma unroll
+    for (int l = 0; l < LM; ++l) {
+        const float2 d = __fadd2_rn(p2[l], thr2);
+        bx = __funnelshift_l(__float_as_uint(d.x), bx, 1);
+        by = __funnelshift_l(__float_as_uint(d.y), by, 1);
+    }
+    constexpr uint32_t kLow = LM >= 32 ? 0xffffffffu : ((1u << LM) - 1u);
+    k0 = (uint32_t)__clz(~bx & kLow) - (32u - LM);
+    k1 = (uint32_t)__clz(~by & kLow) - (32u - LM);
 }
-__device__ __forceinline__ void cp_async8(void* dst, const void* src) {
-    asm volatile("cp.async.ca.shared.global [%0], [%1], 8;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async16(void* dst, const void* src) {
-    asm volatile("cp.async.cg.shared.global [%0], [%1], 16;" ::"r"((uint32_t)__cvta_generic_to_shared(dst)), "l"(src)
-                 : "memory");
-}
-__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;" ::: "memory"); }
-__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;" ::: "memory"); }
 
 // Shared memory of one warp: backward records [C][LM/4][32] float4 and
 // [C][32] {farg' lo, farg' hi, run end, end emission}; the flush descriptors
@@ -993,21 +1031,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
         }
         uint32_t pk[2];
         if (argmax) {
-            // first slot with p >= (1 - eps) max: the sign of p - thr marks the slots below it
-            float px[LM], py[LM];
-#pragma unroll
-            for (int l = 0; l < LM; ++l) { px[l] = p2[l].x; py[l] = p2[l].y; }
-            const float2 thr2 = __fmul2_rn(make_float2(vmax<LM>(px), vmax<LM>(py)), make_float2(-keep, -keep));
-            uint32_t bx = 0u, by = 0u;  // bit LM-1-l: slot l below the threshold
-#pragma unroll
-            for (int l = 0; l < LM; ++l) {
-                const float2 d = __fadd2_rn(p2[l], thr2);
-                bx = __funnelshift_l(__float_as_uint(d.x), bx, 1);
-                by = __funnelshift_l(__float_as_uint(d.y), by, 1);
-            }
-            constexpr uint32_t kLow = LM >= 32 ? 0xffffffffu : ((1u << LM) - 1u);
-            pk[0] = (uint32_t)__clz(~bx & kLow) - (32u - LM);
-            pk[1] = (uint32_t)__clz(~by & kLow) - (32u - LM);
+            pick_pair<LM>(p2, keep, pk[0], pk[1]);
         } else {
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
@@ -1151,8 +1175,9 @@ cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
 
 template <int LM>
 cudaError_t launch_typed_lm(const TypedArgs& a, bool full, cudaStream_t s) {
-    const unsigned long long warps = 2ull * ((a.B + 31) / 32);  // a lane per chain, forward and backward warps
-    anchor_chain_kernel<LM><<<(uint32_t)((warps + 3) / 4), 128, 0, s>>>(a);
+    // a lane per chain, forward and backward warps; one warp per CTA spreads the few warps evenly over the SMs
+    const unsigned long long warps = 2ull * ((a.B + 31) / 32);
+    anchor_chain_kernel<LM><<<(uint32_t)warps, 32, 0, s>>>(a);
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return e;
     if (a.ev_chain_done && (e = cudaEventRecord(a.ev_chain_done, s)) != cudaSuccess) return e;
@@ -1185,12 +1210,10 @@ cudaError_t launch_anchor_count_only(const TypedArgs& a, cudaStream_t s) {
 }
 
 cudaError_t launch_anchor_lists_fill(const TypedArgs& a, cudaStream_t s) {
-    const unsigned long long warps = (unsigned long long)typed_groups(a.B) * a.nseg;
-    const unsigned long long grid = (warps + kFillWarps - 1) / kFillWarps;
+    const unsigned long long grid = (unsigned long long)typed_groups(a.B) * a.nseg;  // a warp per CTA
     if (grid == 0) return cudaSuccess;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    constexpr size_t sm = (size_t)kFillWarps * 32 * kFillRow;
-    anchor_fill_kernel<<<(uint32_t)grid, kFillWarps * 32, sm, s>>>(a);
+    anchor_fill_kernel<<<(uint32_t)grid, 32, kFillSmem, s>>>(a);
     return cudaGetLastError();
 }
 

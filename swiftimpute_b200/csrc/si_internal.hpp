@@ -59,7 +59,9 @@ struct SweepJob {
     uint32_t m0;
     uint32_t len;
     uint64_t head_off;
+    uint64_t init_off;  // the order before m0: init[init_off .. init_off + N), or kIota for 0 .. N-1
 };
+constexpr uint64_t kIota = ~0ull;
 
 struct DeviceBuffer {
     void* ptr = nullptr;
@@ -159,10 +161,21 @@ bool region_first_gap_ok(const si_ctx* ctx, const si_impute_params* p, uint32_t 
 // Kernel launchers (pbwt_kernels.cu, select_kernels.cu, fb_kernels.cu).
 cudaError_t launch_pack_panel(const uint8_t* d_u8, uint32_t M, uint32_t N, uint32_t W, uint32_t* d_words,
                               cudaStream_t s);
+// d_init: the orders jobs with init_off != kIota start from (may be null when none does)
 cudaError_t launch_pbwt_sweep(const uint32_t* d_panel, const SweepJob* d_jobs, uint32_t n_jobs, uint32_t N,
-                              uint32_t W, uint32_t* d_head, uint32_t* d_prefix, unsigned long long* d_hash,
-                              uint32_t* d_perm_scratch, cudaStream_t s);
+                              uint32_t W, const uint32_t* d_init, uint32_t* d_head, uint32_t* d_prefix,
+                              unsigned long long* d_hash, uint32_t* d_perm_scratch, cudaStream_t s);
 size_t pbwt_sweep_smem_bytes(uint32_t N, uint32_t W);
+size_t pbwt_group_smem_bytes(uint32_t N, uint32_t W);
+// Segmented whole-panel sweep (pbwt_kernels.cu): per segment the groups of
+// haplotypes equal over its markers, swept from 0 .. N-1 (d_gid [n_jobs][N],
+// by haplotype; d_scratch 4 N words per job), and the composition of an order
+// with one segment's groups (a stable sort by group; d_sortbuf 4 N words).
+cudaError_t launch_pbwt_groups(const uint32_t* d_panel, const SweepJob* d_jobs, uint32_t n_jobs, uint32_t N,
+                               uint32_t W, uint32_t* d_gid, uint32_t* d_scratch, cudaStream_t s);
+cudaError_t launch_pbwt_compose(const uint32_t* d_order, const uint32_t* d_gid, uint32_t* d_next, uint32_t N,
+                                uint32_t* d_sortbuf, cudaStream_t s);
+cudaError_t launch_iota(uint32_t* d, uint32_t N, cudaStream_t s);
 cudaError_t launch_panel_checksum(const uint32_t* d_words, uint64_t n, unsigned long long* d_out, cudaStream_t s);
 // Selection over markers [0, M) of the given panel rows; ex_off/ex_ent (may be
 // null) are the rows' exception lists, raw (may be null) receives allele bytes.
