@@ -334,6 +334,14 @@ __device__ __forceinline__ float vsum(const float (&v)[LM]) {
     return s;
 }
 
+// Exact int -> double on the FP64 pipe: 2^52 + 2^31 + x has x + 2^31 in its
+// low word, so one subtraction recovers x (a conversion instruction would use
+// the special-function pipe, which the backward chain otherwise saturates).
+__device__ __forceinline__ double i2d(int x) {
+    return __hiloint2double(0x43300000, (int)((uint32_t)x ^ 0x80000000u)) - 4503601774854144.0;  // 2^52 + 2^31
+}
+__device__ __forceinline__ double u2d(uint32_t x) { return __hiloint2double(0x43300000, (int)x) - 4503599627370496.0; }
+
 // sum over slot pairs, as a tree
 template <uint32_t H>
 __device__ __forceinline__ float vsum2(const float2 (&v)[H]) {
@@ -575,7 +583,7 @@ __global__ void __launch_bounds__(32) anchor_chain_kernel(TypedArgs A) {
                 const uint32_t n = t0 + j + 2 <= NA ? (j ? p[j - 1] : after) - p[j] : 0u;
                 q[j] = tabQS(tb, n);
                 g[j] = tabG(tb, n) - 999.0;
-                c[j] = (double)n * tb.lr - 999.0 * (double)h[j];
+                c[j] = fma(u2d(n), tb.lr, h[j] ? -999.0 : 0.0);
             }
         };
         auto step = [&](uint32_t em, float2 q, double g, double c) {
@@ -592,7 +600,7 @@ __global__ void __launch_bounds__(32) anchor_chain_kernel(TypedArgs A) {
             }
             int e;
             update(w, em, xs * q.x, fmaf(xs * sw, q.y, F), sw, e);
-            logU = ((big ? g : logU) + c) + (double)e * 0.69314718055994530942;
+            logU = fma(i2d(e), 0.69314718055994530942, (big ? g : logU) + c);
             if (--cc == 0) {
                 store(A.ckptB + ck(ci) * LM, w);
                 A.ckptU[ck(ci)] = logU;
