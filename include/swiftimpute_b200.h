@@ -40,7 +40,20 @@ typedef struct si_ctx si_ctx;
  * reference Imputer's choice without an index or with PBWT selection off:
  * slot k = haplotypes (2k, 2k+1) at every marker (imputer.cpp:929-942); it
  * needs no index and N >= 2L. */
-enum { SI_SEL_AUTO = 0, SI_SEL_WARP = 1, SI_SEL_INSERTION = 2, SI_SEL_FIRST_PAIRS = 3 };
+enum { SI_SEL_AUTO = 0, SI_SEL_WARP = 1, SI_SEL_INSERTION = 2, SI_SEL_FIRST_PAIRS = 3, SI_SEL_TARGET = 4 };
+/* SI_SEL_TARGET (opt-in; changes results, so never the default): slots chosen
+ * per target from the haplotypes that match it longest, the way Durbin's PBWT
+ * follows an inserted sequence. It replaces the positional patterns of
+ * PBWTIndex::select_states (pbwt_index.cpp:20-79), whose divergences all equal
+ * m. The target's pseudo-haplotype carries 0 at code 0, 1 at code 2, and
+ * elsewhere the allele of the panel haplotype at its position in the order;
+ * its position p moves as z(p) (allele 0) or Z + p - z(p) (allele 1), with Z
+ * the zeros at the marker and z(p) those among the first p entries of the
+ * previous order (the target goes before equal keys). Slots: the L haplotypes
+ * at positions clamp(p - L/2, 0, N - L) .. + L of the marker's order, paired
+ * (h, (h + 1) % N). Needs the index built with SI_PBWT_STORE_INDEX and a panel
+ * of 0/1 alleles; si_impute / si_impute_device run it through the full-chain
+ * kernel with each target's own slots ([M][B] slot masks of scratch). */
 
 /* Transition modes. MATRIX0 reproduces the reference, whose forward-backward
  * reads the first gap's matrix for every gap (forward_backward.cu:108,201,234,269).
@@ -167,6 +180,12 @@ si_status si_pbwt_load(si_ctx* ctx, const void* in, uint64_t bytes);
  * depend on the target sample, so it is computed once per marker. */
 si_status si_select_states(si_ctx* ctx, uint32_t L, int32_t kind, uint32_t m0, uint32_t m1,
                            uint32_t* out_pairs);
+
+/* SI_SEL_TARGET slots of B targets: codes [B][M] (host), pairs out
+ * [B][M][L][2] (host), L <= 32. No reference counterpart (the reference's
+ * selection is the same for every target). */
+si_status si_select_states_target(si_ctx* ctx, uint32_t L, const uint8_t* geno_codes, uint32_t B,
+                                  uint32_t* out_pairs);
 
 /* Imputation ------------------------------------------------------------- */
 

@@ -61,6 +61,7 @@ def lib() -> ctypes.CDLL:
         L.sio_pbwt_build.argtypes = [c_void_p, c_uint32, c_uint32, c_void_p]
         L.sio_pbwt_build_packed.argtypes = [c_void_p, c_uint32, c_uint32, c_uint32, c_void_p, c_void_p]
         L.sio_select_row.argtypes = [c_void_p, c_uint32, c_uint32, c_int, c_void_p]
+        L.sio_select_target.argtypes = [c_void_p, c_void_p, c_void_p, c_uint32, c_uint32, c_uint32, c_void_p]
         L.sio_fb_sample.argtypes = [POINTER(FbArgs)] + [c_void_p] * 11
         L.sio_fb_batch.argtypes = [POINTER(FbArgs), c_uint32] + [c_void_p] * 10 + [c_int]
         L.sio_codes_to_gl.argtypes = [c_void_p, c_uint64, c_void_p]
@@ -108,6 +109,17 @@ def select_pairs(prefix: np.ndarray, L: int, kind: int = SEL_AUTO) -> np.ndarray
         lib().sio_select_row(_p(pre[m]), N, L, kind, _p(row))
         slots[m] = row
     return np.stack([slots, (slots + 1) % N], axis=-1).astype(np.uint32)
+
+
+def select_pairs_target(prefix: np.ndarray, panel: np.ndarray, codes: np.ndarray, L: int) -> np.ndarray:
+    """[M][L][2] target-aware slot pairs of one target (codes [M]) from the full prefix array."""
+    pre = np.ascontiguousarray(prefix, dtype=np.uint32)
+    pan = np.ascontiguousarray(panel, dtype=np.uint8)
+    cod = np.ascontiguousarray(codes, dtype=np.uint8)
+    M, N = pan.shape
+    out = np.empty((M, L, 2), dtype=np.uint32)
+    lib().sio_select_target(_p(pre), _p(pan), _p(cod), M, N, L, _p(out))
+    return out
 
 
 def transition_log10(gd0: float, gd1: float, ne: float, rho_rate: float) -> tuple[float, float]:

@@ -123,6 +123,49 @@ void sio_select_row(const uint32_t* prefix_row, uint32_t N, uint32_t L, int kind
     }
 }
 
+/* Target-aware selection (the opt-in SI_SEL_TARGET; the reference has none:
+ * its select_states, pbwt_index.cpp:20-79, sees only divergences equal to m).
+ * One target, the Durbin (2014) PBWT extension of an inserted sequence: the
+ * pseudo-haplotype carries 0 at code 0, 1 at code 2, else the allele of the
+ * panel haplotype at its current position of the previous order (the last
+ * entry when it sits past the end); its position p counts the haplotypes whose
+ * reversed prefix sorts before it (it goes before equal keys):
+ *   p' = zeros among prev[0, p)                   (allele 0)
+ *   p' = Z + (p - zeros among prev[0, p))          (allele 1), Z = zeros at m.
+ * Slots: positions clamp(p - L/2, 0, N - L) .. + L of the marker's order
+ * (r % N when L > N), each as (h, (h + 1) % N). Non-zero alleles sort as 1,
+ * as in the sweep. pairs: [M][L][2]. */
+void sio_select_target(const uint32_t* prefix, const uint8_t* panel, const uint8_t* codes, uint32_t M, uint32_t N,
+                       uint32_t L, uint32_t* pairs) {
+    uint32_t p = 0;
+    for (uint32_t m = 0; m < M; ++m) {
+        const uint8_t* x = panel + (size_t)m * N;
+        const uint32_t* prev = m ? prefix + (size_t)(m - 1) * N : NULL;
+        uint32_t Z = 0, zb = 0;
+        for (uint32_t i = 0; i < N; ++i) {
+            const uint32_t h = prev ? prev[i] : i;
+            const uint32_t z = x[h] == 0;
+            Z += z;
+            if (i < p) zb += z;
+        }
+        const uint32_t q = p < N ? p : N - 1;
+        const uint32_t hq = prev ? prev[q] : q;
+        const uint32_t xt = codes[m] == 0 ? 0u : codes[m] == 2 ? 1u : (x[hq] != 0);
+        p = xt ? Z + (p - zb) : zb;
+        const uint32_t* row = prefix + (size_t)m * N;
+        uint32_t s0 = 0;
+        if (L <= N) {
+            s0 = p > L / 2 ? p - L / 2 : 0;
+            if (s0 > N - L) s0 = N - L;
+        }
+        for (uint32_t r = 0; r < L; ++r) {
+            const uint32_t h = L <= N ? row[s0 + r] : row[r % N];
+            pairs[((size_t)m * L + r) * 2] = h;
+            pairs[((size_t)m * L + r) * 2 + 1] = (h + 1) % N;
+        }
+    }
+}
+
 /* ------------------------------------------------------------------------ */
 /* Transition (transition.cu:83-115)                                         */
 /* ------------------------------------------------------------------------ */

@@ -43,6 +43,8 @@ uint64_t sio_row_hash(const uint32_t* row, uint32_t N);
 /* Slot haplotypes for one marker, given that marker's prefix row. */
 int sio_select_kind(uint32_t N, uint32_t L);
 void sio_select_row(const uint32_t* prefix_row, uint32_t N, uint32_t L, int kind, uint32_t* slots);
+void sio_select_target(const uint32_t* prefix, const uint8_t* panel, const uint8_t* codes, uint32_t M, uint32_t N,
+                       uint32_t L, uint32_t* pairs);
 
 /* Li–Stephens log10 transition values (transition.cu:83-115), stored as float
  * like the reference. gd0/gd1 are genetic positions in Morgans. */

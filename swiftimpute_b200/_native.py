@@ -18,7 +18,7 @@ STATUS_NAMES = {
     4: "SI_ERR_UNSUPPORTED", 5: "SI_ERR_STATE", 6: "SI_ERR_TIMEOUT", 7: "SI_ERR_BUDGET",
     8: "SI_ERR_CANCELLED",
 }
-SEL_AUTO, SEL_WARP, SEL_INSERTION, SEL_FIRST_PAIRS = 0, 1, 2, 3
+SEL_AUTO, SEL_WARP, SEL_INSERTION, SEL_FIRST_PAIRS, SEL_TARGET = 0, 1, 2, 3, 4
 TRANS_MATRIX0, TRANS_PER_GAP = 0, 1
 SAMPLE_ARGMAX, SAMPLE_PHILOX = 0, 1
 PBWT_STORE_INDEX, PBWT_ROW_HASHES = 1, 2
@@ -115,6 +115,7 @@ SIGNATURES = [
     ("si_pbwt_row_hashes", c_int, [c_void_p, c_void_p]),
     ("si_pbwt_last_ms", c_int, [c_void_p, POINTER(c_float)]),
     ("si_select_states", c_int, [c_void_p, c_uint32, c_int32, c_uint32, c_uint32, c_void_p]),
+    ("si_select_states_target", c_int, [c_void_p, c_uint32, c_void_p, c_uint32, c_void_p]),
     ("si_impute_params_default", c_int, [POINTER(ImputeParams)]),
     ("si_impute", c_int, [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p]),
     ("si_impute_gl", c_int, [c_void_p, POINTER(ImputeParams), c_void_p, c_uint32, c_void_p, c_void_p, c_void_p]),

@@ -83,6 +83,8 @@ void reset_index(si_ctx* ctx) {
     dev_free(ctx, ctx->head);
     dev_free(ctx, ctx->prefix);
     dev_free(ctx, ctx->row_hash);
+    dev_free(ctx, ctx->rank_bits);
+    dev_free(ctx, ctx->rank_zeros);
     for (auto& kv : ctx->sel) {
         dev_free(ctx, kv.second.pairs);
         dev_free(ctx, kv.second.masks);
@@ -195,6 +197,10 @@ si_status ensure_trans(si_ctx* ctx, const si_impute_params* p) {
 si_status ensure_selection(si_ctx* ctx, uint32_t L, int kind, SelectionCache** out, bool force = false,
                            cudaStream_t s = nullptr) {
     if (L == 0 || L > kHead) return fail(ctx, SI_ERR_INVALID_ARG, "L must be in 1..128");
+    if (kind == SI_SEL_TARGET)
+        return fail(ctx, SI_ERR_UNSUPPORTED,
+                    "target-aware selection (SI_SEL_TARGET) is per target: si_impute, si_impute_device and "
+                    "si_select_states_target only");
     if (kind == SI_SEL_FIRST_PAIRS) {
         if ((uint64_t)2 * L > ctx->N)
             return fail(ctx, SI_ERR_UNSUPPORTED, "first-pairs selection needs N >= 2L haplotypes");
@@ -393,13 +399,49 @@ si_status run_device_typed(si_ctx* ctx, const si_impute_params* p, const Selecti
     return run_typed(ctx, p, a, lmax, lmax == p->num_states, s);
 }
 
+// Target-aware selection of B targets (codes d_geno [B][M]) on stream s: the
+// rank tables on first use, then each target's slot masks into ctx->smasks
+// [M][B] and, when d_pairs is given, its pairs [B][M][L][2].
+si_status run_target_select(si_ctx* ctx, uint32_t L, const uint8_t* d_geno, uint32_t B, uint32_t* d_pairs,
+                            cudaStream_t s) {
+    if (!ctx->has_index) return fail(ctx, SI_ERR_STATE, "PBWT index not built (si_pbwt_build)");
+    if (!ctx->prefix.ptr)
+        return fail(ctx, SI_ERR_STATE,
+                    "target-aware selection reads the full prefix rows: build the index with SI_PBWT_STORE_INDEX");
+    if (ctx->n_ex) return fail(ctx, SI_ERR_UNSUPPORTED, "target-aware selection needs a panel of 0/1 alleles");
+    if (L == 0 || L > 32) return fail(ctx, SI_ERR_UNSUPPORTED, "target-aware selection takes 1..32 states");
+    const uint32_t M = ctx->M, N = ctx->N, W = ctx->W;
+    if (!ctx->rank_bits.ptr) {
+        SI_TRY(dev_alloc(ctx, ctx->rank_bits, (size_t)M * W * 4));
+        si_status st = dev_alloc(ctx, ctx->rank_zeros, (size_t)M * (W + 1) * 4);
+        if (st != SI_OK) {
+            dev_free(ctx, ctx->rank_bits);
+            return st;
+        }
+        SI_CUDA(ctx,
+                launch_target_ranks((const uint32_t*)ctx->prefix.ptr, (const uint32_t*)ctx->panel.ptr, M, N, W,
+                                    (uint32_t*)ctx->rank_bits.ptr, (uint32_t*)ctx->rank_zeros.ptr, ctx->stream),
+                "target rank tables");
+        SI_CUDA(ctx, cudaStreamSynchronize(ctx->stream), "target rank tables");
+    }
+    SI_TRY(dev_reserve(ctx, ctx->smasks, (size_t)M * B * sizeof(SlotMasks)));
+    SI_CUDA(ctx,
+            launch_target_select(d_geno, B, M, N, W, L, (const uint32_t*)ctx->prefix.ptr,
+                                 (const uint32_t*)ctx->panel.ptr, (const uint32_t*)ctx->rank_bits.ptr,
+                                 (const uint32_t*)ctx->rank_zeros.ptr, (SlotMasks*)ctx->smasks.ptr, d_pairs, s),
+            "target-aware selection");
+    return SI_OK;
+}
+
 // Device part of an imputation over B chains whose inputs/outputs are device
 // pointers; queued on stream s.
 si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_geno, uint32_t B, float* d_dosage,
                      float* d_hprob, uint8_t* d_haps, cudaStream_t s) {
     SelectionCache* sel = nullptr;
+    const bool target = p->selection_kind == SI_SEL_TARGET;  // per-target slots: the full-chain kernel
     SI_CUDA(ctx, cudaEventRecord(ctx->kev[0], s), "event");
-    SI_TRY(ensure_selection(ctx, p->num_states, p->selection_kind, &sel, (p->flags & SI_IMPUTE_RESELECT) != 0, s));
+    if (target) SI_TRY(run_target_select(ctx, p->num_states, d_geno, B, nullptr, s));
+    else SI_TRY(ensure_selection(ctx, p->num_states, p->selection_kind, &sel, (p->flags & SI_IMPUTE_RESELECT) != 0, s));
     SI_CUDA(ctx, cudaEventRecord(ctx->kev[1], s), "event");
     ctx->kernel_pending = true;
     if (s != ctx->stream && !(p->flags & SI_IMPUTE_RESELECT)) {
@@ -408,7 +450,7 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
         SI_CUDA(ctx, cudaStreamWaitEvent(s, ctx->ev[3], 0), "stream wait");
     }
     SI_TRY(ensure_trans(ctx, p));
-    if (p->transition_mode == SI_TRANS_MATRIX0 && !(p->flags & SI_IMPUTE_FULL_CHAIN)) {
+    if (!target && p->transition_mode == SI_TRANS_MATRIX0 && !(p->flags & SI_IMPUTE_FULL_CHAIN)) {
         SI_CUDA(ctx, cudaEventRecord(ctx->ev[1], s), "event");
         SI_TRY(run_device_typed(ctx, p, sel, d_geno, B, d_dosage, d_hprob, d_haps, s));
         SI_CUDA(ctx, cudaEventRecord(ctx->ev[2], s), "event");
@@ -425,7 +467,10 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
                         std::to_string(fb_smem_bytes(p->num_states, T, C)) + " bytes of shared memory (max 227 KB)");
     SI_TRY(dev_reserve(ctx, ctx->ckpt, fb_ckpt_bytes(B, ctx->M, p->num_states, C)));
     FbLaunch l;
-    l.geno = d_geno; l.masks = (const SlotMasks*)sel->masks.ptr; l.raw = (const uint8_t*)sel->raw.ptr;
+    l.geno = d_geno;
+    l.masks = target ? nullptr : (const SlotMasks*)sel->masks.ptr;
+    l.smasks = target ? (const SlotMasks*)ctx->smasks.ptr : nullptr;
+    l.raw = target ? nullptr : (const uint8_t*)sel->raw.ptr;
     l.trans = (const LinTrans*)ctx->trans.ptr;
     l.B = B; l.M = ctx->M; l.L = p->num_states; l.C = C; l.threads = T;
     l.sampling = p->sampling; l.tie_eps = (float)p->tie_eps; l.seed = p->seed; l.sample_id_base = p->sample_id_base;
@@ -660,6 +705,7 @@ si_status si_ctx_destroy(si_ctx* ctx) {
     dev_free(ctx, ctx->panel);
     dev_free(ctx, ctx->trans);
     dev_free(ctx, ctx->ckpt);
+    dev_free(ctx, ctx->smasks);
     dev_free(ctx, ctx->io_geno);
     dev_free(ctx, ctx->io_dosage);
     dev_free(ctx, ctx->io_hprob);
@@ -993,6 +1039,30 @@ si_status si_select_states(si_ctx* ctx, uint32_t L, int32_t kind, uint32_t m0, u
             cudaMemcpy(out_pairs, (uint32_t*)c->pairs.ptr + (size_t)m0 * L * 2, (size_t)(m1 - m0) * L * 2 * 4,
                        cudaMemcpyDeviceToHost),
             "copy pairs");
+    return SI_OK;
+}
+
+si_status si_select_states_target(si_ctx* ctx, uint32_t L, const uint8_t* geno_codes, uint32_t B, uint32_t* out_pairs) {
+    Range range("si_select_states_target");
+    if (!ctx) return SI_ERR_INVALID_ARG;
+    if (!geno_codes || !out_pairs || B == 0) return fail(ctx, SI_ERR_INVALID_ARG, "NULL argument or empty batch");
+    if (!ctx->panel.ptr) return fail(ctx, SI_ERR_STATE, "no panel uploaded");
+    SI_TRY(set_device(ctx));
+    const size_t cells = (size_t)B * ctx->M, npairs = cells * L * 2;
+    DeviceBuffer g, pr;
+    SI_TRY(dev_alloc(ctx, g, cells));
+    si_status st = dev_alloc(ctx, pr, npairs * 4);
+    cudaError_t e = cudaSuccess;
+    if (st == SI_OK) e = cudaMemcpyAsync(g.ptr, geno_codes, cells, cudaMemcpyHostToDevice, ctx->stream);
+    if (st == SI_OK && e == cudaSuccess)
+        st = run_target_select(ctx, L, (const uint8_t*)g.ptr, B, (uint32_t*)pr.ptr, ctx->stream);
+    if (st == SI_OK && e == cudaSuccess)
+        e = cudaMemcpyAsync(out_pairs, pr.ptr, npairs * 4, cudaMemcpyDeviceToHost, ctx->stream);
+    if (st == SI_OK && e == cudaSuccess) e = cudaStreamSynchronize(ctx->stream);
+    dev_free(ctx, g);
+    dev_free(ctx, pr);
+    if (st != SI_OK) return st;
+    if (e != cudaSuccess) return cuda_fail(ctx, e, "target-aware selection");
     return SI_OK;
 }
 

@@ -36,6 +36,7 @@ namespace {
 struct FbArgs {
     const uint8_t* geno;
     const SlotMasks* masks;
+    const SlotMasks* smasks;  // per-target [M][B] (target-aware selection), else null
     const uint8_t* raw;
     const LinTrans* trans;
     uint32_t B, M, L, C, nseg;
@@ -103,9 +104,14 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
             if (sr < a.B && lane < cl) gbuf[r * GS + lane] = a.geno[(uint64_t)sr * M + m0 + lane];
         }
         for (uint32_t i = t; i < cl; i += T) {
-            mseg[i] = a.masks[m0 + i];
+            if (!a.smasks) mseg[i] = a.masks[m0 + i];
             tseg[i] = a.trans[m0 + i];
         }
+    };
+    // the slot masks of marker m (staged at i): per marker, or this target's own
+    auto mask_at = [&](uint32_t i, uint32_t m) {
+        if (!a.smasks) return mseg[i];
+        return live ? a.smasks[(uint64_t)m * a.B + s] : SlotMasks{0u, 0u, 0u, 0u};
     };
 
     float al[LM];
@@ -119,7 +125,7 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
         __syncthreads();
         for (uint32_t i = 0; i < cl; ++i) {
             uint32_t sh;
-            const uint32_t em = emission_mask(gbuf[t * GS + i], mseg[i], lmask, &sh);
+            const uint32_t em = emission_mask(gbuf[t * GS + i], mask_at(i, m0 + i), lmask, &sh);
             forward_step<LM>(al, S, em, tseg[i], m0 + i == 0);
         }
         if (live && j + 1 < a.nseg) {
@@ -153,7 +159,7 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
         }
         for (uint32_t i = 0; i < cl; ++i) {
             uint32_t sh;
-            const uint32_t em = emission_mask(gbuf[t * GS + i], mseg[i], lmask, &sh);
+            const uint32_t em = emission_mask(gbuf[t * GS + i], mask_at(i, m0 + i), lmask, &sh);
             forward_step<LM>(al, S, em, tseg[i], m0 + i == 0);
 #pragma unroll
             for (int k = 0; k < LM; ++k) abuf[((size_t)i * LM + k) * T + t] = al[k];
@@ -197,7 +203,7 @@ __global__ void __launch_bounds__(128) fb_chain_kernel(FbArgs a) {
                 }
             }
             // posterior at m
-            const SlotMasks mk = mseg[i];
+            const SlotMasks mk = mask_at(i, m);
             float p[LM];
             float tot = 0.f, q0 = 0.f, q1 = 0.f, pmax = 0.f;
 #pragma unroll
@@ -297,7 +303,7 @@ size_t fb_ckpt_bytes(uint32_t B, uint32_t M, uint32_t L, uint32_t C) {
 
 cudaError_t launch_fb(const FbLaunch& l, cudaStream_t s) {
     FbArgs fa;
-    fa.geno = l.geno; fa.masks = l.masks; fa.raw = l.raw; fa.trans = l.trans;
+    fa.geno = l.geno; fa.masks = l.masks; fa.smasks = l.smasks; fa.raw = l.raw; fa.trans = l.trans;
     fa.B = l.B; fa.M = l.M; fa.L = l.L; fa.C = l.C; fa.nseg = (l.M + l.C - 1) / l.C;
     fa.sampling = l.sampling; fa.tie_eps = l.tie_eps; fa.seed = l.seed; fa.sid_base = l.sample_id_base;
     fa.ckpt = l.ckpt; fa.dosage = l.dosage; fa.hprob = l.hprob; fa.haps = l.haps;

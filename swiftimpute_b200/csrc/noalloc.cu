@@ -74,6 +74,8 @@ extern "C" si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_param
     if (p->flags & ~(uint32_t)SI_IMPUTE_FULL_CHAIN) return fail(ctx, SI_ERR_INVALID_ARG, "unknown flag bits");
     // set-up state must already exist: an earlier allocating call with the same
     // parameters built the slot table and the transition table
+    if (p->selection_kind == SI_SEL_TARGET)
+        return fail(ctx, SI_ERR_UNSUPPORTED, "target-aware selection needs per-target scratch: use si_impute_device");
     const uint32_t L = p->num_states;
     int kind = p->selection_kind;
     if (kind == SI_SEL_AUTO) kind = (L <= 32 && ctx->N <= 10000) ? SI_SEL_WARP : SI_SEL_INSERTION;
@@ -101,6 +103,7 @@ extern "C" si_status si_impute_device_noalloc(si_ctx* ctx, const si_impute_param
     FbLaunch l;
     l.geno = d_geno;
     l.masks = (const SlotMasks*)it->second.masks.ptr;
+    l.smasks = nullptr;
     l.raw = (const uint8_t*)it->second.raw.ptr;
     l.trans = (const LinTrans*)ctx->trans.ptr;
     l.B = B; l.M = ctx->M; l.L = L; l.C = C; l.threads = T;

@@ -100,6 +100,109 @@ __global__ void select_kernel(const uint32_t* __restrict__ head, const uint32_t*
     }
 }
 
+// ---------------------------------------------------------------- target-aware selection (opt-in)
+//
+// The reference's selection ignores the target (every divergence is m, so the
+// slots are fixed positions of the prefix row). SI_SEL_TARGET instead follows
+// each target through the index as Durbin's PBWT follows an inserted sequence:
+// the target's pseudo-haplotype carries allele 0 at a homozygous-reference call
+// (code 0), 1 at a homozygous-alternate call (code 2), and elsewhere the allele
+// of the panel haplotype at its current position in the order; its position p
+// in the order of marker m counts the haplotypes whose reversed prefix sorts
+// before its own (the target goes before equal keys), so with Z zeros at m and
+// z(p) zeros among the first p entries of the previous order,
+//   p' = z(p) (allele 0),   p' = Z + p - z(p) (allele 1).
+// The slots are the L haplotypes at positions clamp(p - L/2, 0, N - L) .. + L
+// of marker m's order (r % N when L > N), as pairs (h, (h + 1) % N).
+//
+// Rank tables, built once from the stored prefix rows: rank_bits[m][w] holds
+// bit i = the allele at m of entry 32 w + i of the previous order (the order
+// before marker 0 is 0 .. N-1); rank_zeros[m][w] = zeros among entries
+// [0, 32 w), rank_zeros[m][W] = Z. One CTA per marker.
+__global__ void target_rank_kernel(const uint32_t* __restrict__ prefix, const uint32_t* __restrict__ panel,
+                                   uint32_t M, uint32_t N, uint32_t W, uint32_t* __restrict__ rank_bits,
+                                   uint32_t* __restrict__ rank_zeros) {
+    const uint32_t m = blockIdx.x;
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nw = blockDim.x >> 5;
+    const uint32_t* prev = m ? prefix + (uint64_t)(m - 1) * N : nullptr;
+    const uint32_t* prow = panel + (uint64_t)m * W;
+    uint32_t* bits = rank_bits + (uint64_t)m * W;
+    uint32_t* zeros = rank_zeros + (uint64_t)m * (W + 1);
+    const uint32_t nwords = (N + 31) / 32;
+    for (uint32_t w = warp; w < W; w += nw) {
+        const uint32_t i = 32 * w + lane;
+        uint32_t b = 0;
+        if (i < N) {
+            const uint32_t h = prev ? prev[i] : i;
+            b = (prow[h >> 5] >> (h & 31)) & 1u;
+        }
+        const uint32_t word = __ballot_sync(0xffffffffu, b);
+        if (lane == 0) bits[w] = word;
+    }
+    __syncthreads();
+    if (warp == 0) {  // exclusive scan of per-word zero counts
+        uint32_t carry = 0;
+        for (uint32_t w0 = 0; w0 < W; w0 += 32) {
+            const uint32_t w = w0 + lane;
+            uint32_t z = 0;
+            if (w < nwords) {
+                const uint32_t valid = (w + 1 < nwords || N % 32 == 0) ? 0xffffffffu : ((1u << (N % 32)) - 1u);
+                z = __popc(~bits[w] & valid);
+            }
+            uint32_t incl = z;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                const uint32_t y = __shfl_up_sync(0xffffffffu, incl, o);
+                if (lane >= (uint32_t)o) incl += y;
+            }
+            if (w < W) zeros[w] = carry + incl - z;
+            carry += __shfl_sync(0xffffffffu, incl, 31);
+        }
+        if (lane == 0) zeros[W] = carry;
+    }
+}
+
+// One thread per target: the walk over all M markers, writing each marker's
+// slot masks (a0, a1 bits of the pairs' two haplotypes) at smasks[m][s] and,
+// when pairs is given, the pairs at pairs[s][m][L][2].
+__global__ void target_select_kernel(const uint8_t* __restrict__ geno, uint32_t B, uint32_t M, uint32_t N,
+                                     uint32_t W, uint32_t L, const uint32_t* __restrict__ prefix,
+                                     const uint32_t* __restrict__ panel, const uint32_t* __restrict__ rank_bits,
+                                     const uint32_t* __restrict__ rank_zeros, SlotMasks* __restrict__ smasks,
+                                     uint32_t* __restrict__ pairs) {
+    const uint32_t s = blockIdx.x * blockDim.x + threadIdx.x;
+    if (s >= B) return;
+    const uint8_t* g = geno + (uint64_t)s * M;
+    uint32_t p = 0;
+    for (uint32_t m = 0; m < M; ++m) {
+        const uint32_t* bits = rank_bits + (uint64_t)m * W;
+        const uint32_t* zeros = rank_zeros + (uint64_t)m * (W + 1);
+        const uint32_t Z = zeros[W];
+        const uint32_t zb = p < N ? zeros[p >> 5] + __popc(~bits[p >> 5] & ((1u << (p & 31)) - 1u)) : Z;
+        const uint32_t q = p < N ? p : N - 1;
+        const uint32_t code = g[m];
+        const uint32_t xt = code == 0 ? 0u : code == 2 ? 1u : ((bits[q >> 5] >> (q & 31)) & 1u);
+        p = xt ? Z + (p - zb) : zb;
+        const uint32_t* row = prefix + (uint64_t)m * N;
+        const uint32_t* prow = panel + (uint64_t)m * W;
+        uint32_t s0 = 0;
+        if (L <= N) s0 = min(p > L / 2 ? p - L / 2 : 0u, N - L);
+        uint32_t a0 = 0, a1 = 0;
+        for (uint32_t r = 0; r < L; ++r) {
+            const uint32_t h0 = L <= N ? row[s0 + r] : row[r % N];
+            const uint32_t h1 = (h0 + 1) % N;
+            a0 |= ((prow[h0 >> 5] >> (h0 & 31)) & 1u) << r;
+            a1 |= ((prow[h1 >> 5] >> (h1 & 31)) & 1u) << r;
+            if (pairs) {
+                uint32_t* o = pairs + (((uint64_t)s * M + m) * L + r) * 2;
+                o[0] = h0;
+                o[1] = h1;
+            }
+        }
+        smasks[(uint64_t)m * B + s] = SlotMasks{a0, a1, 0u, 0u};
+    }
+}
+
 }  // namespace
 
 cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
@@ -109,6 +212,22 @@ cudaError_t launch_select(const uint32_t* d_head, const uint32_t* d_panel, uint3
     const uint32_t bs = 128;
     select_kernel<<<(M + bs - 1) / bs, bs, 0, s>>>(d_head, d_panel, M, N, W, L, kind, d_ex_off, d_ex_ent, d_pairs,
                                                    d_masks, d_g2, d_raw, gs);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_target_ranks(const uint32_t* d_prefix, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
+                                uint32_t* d_bits, uint32_t* d_zeros, cudaStream_t s) {
+    if (M == 0) return cudaSuccess;
+    target_rank_kernel<<<M, 256, 0, s>>>(d_prefix, d_panel, M, N, W, d_bits, d_zeros);
+    return cudaGetLastError();
+}
+
+cudaError_t launch_target_select(const uint8_t* d_geno, uint32_t B, uint32_t M, uint32_t N, uint32_t W, uint32_t L,
+                                 const uint32_t* d_prefix, const uint32_t* d_panel, const uint32_t* d_bits,
+                                 const uint32_t* d_zeros, SlotMasks* d_smasks, uint32_t* d_pairs, cudaStream_t s) {
+    if (B == 0) return cudaSuccess;
+    target_select_kernel<<<(B + 127) / 128, 128, 0, s>>>(d_geno, B, M, N, W, L, d_prefix, d_panel, d_bits, d_zeros,
+                                                        d_smasks, d_pairs);
     return cudaGetLastError();
 }
 

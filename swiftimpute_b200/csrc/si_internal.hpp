@@ -107,6 +107,8 @@ struct si_ctx {
     si::DeviceBuffer head;           // [M][kHead] u32, first entries of each prefix row
     si::DeviceBuffer prefix;         // [M][N] u32 (SI_PBWT_STORE_INDEX)
     si::DeviceBuffer row_hash;       // [M] u64 (SI_PBWT_ROW_HASHES)
+    si::DeviceBuffer rank_bits;      // [M][W] target-aware selection rank tables (built on first use)
+    si::DeviceBuffer rank_zeros;     // [M][W+1]
     float pbwt_ms = 0.f;
 
     // selection, keyed by (L, kind)
@@ -117,6 +119,7 @@ struct si_ctx {
     uint64_t trans_key = ~0ull;
     si::LinTrans trans0{1.f, 0.f};  // host copy of the first gap's transition
     si::DeviceBuffer ckpt;           // forward checkpoints (full-chain kernel)
+    si::DeviceBuffer smasks;         // per-target slot masks [M][B] (target-aware selection)
     // typed-marker kernel scratch and tables
     si::DeviceBuffer t_counts, t_segc, t_aoff, t_woff, t_apos, t_aem, t_ckF, t_ckB, t_ckU;
     struct TableSet {
@@ -192,6 +195,7 @@ cudaError_t launch_pack_haps(const uint8_t* d_in, uint64_t rows, uint32_t M, uin
 struct FbLaunch {
     const uint8_t* geno;   // [B][M]
     const SlotMasks* masks;
+    const SlotMasks* smasks;  // per-target masks [M][B] (target-aware selection), or null: masks per marker
     const uint8_t* raw;    // [M][fb_lmax(L)][2] allele bytes, or null (0/1 panel)
     const LinTrans* trans;
     uint32_t B, M, L, C;
@@ -205,6 +209,14 @@ struct FbLaunch {
     uint8_t* haps;         // [B][2][M] or null
 };
 cudaError_t launch_fb(const FbLaunch& a, cudaStream_t s);
+// Target-aware selection (select_kernels.cu): rank tables [M][W] bits and
+// [M][W+1] zero counts from the stored prefix rows, then per target the slot
+// masks smasks[m][s] (and, if d_pairs, the pairs [s][m][L][2]).
+cudaError_t launch_target_ranks(const uint32_t* d_prefix, const uint32_t* d_panel, uint32_t M, uint32_t N, uint32_t W,
+                                uint32_t* d_bits, uint32_t* d_zeros, cudaStream_t s);
+cudaError_t launch_target_select(const uint8_t* d_geno, uint32_t B, uint32_t M, uint32_t N, uint32_t W, uint32_t L,
+                                 const uint32_t* d_prefix, const uint32_t* d_panel, const uint32_t* d_bits,
+                                 const uint32_t* d_zeros, SlotMasks* d_smasks, uint32_t* d_pairs, cudaStream_t s);
 size_t fb_ckpt_bytes(uint32_t B, uint32_t M, uint32_t L, uint32_t C);
 // slots held per thread (and the stride of per-slot tables) for L slots
 inline __host__ __device__ uint32_t fb_lmax(uint32_t L) { return L <= 4 ? 4 : L <= 8 ? 8 : L <= 16 ? 16 : 32; }

@@ -133,6 +133,13 @@ class Engine:
         self._check(self.lib.si_select_states(self.h, L, kind, m0, m1, _ptr(out)))
         return out
 
+    def select_states_target(self, L: int, codes: np.ndarray) -> np.ndarray:
+        """Target-aware (SI_SEL_TARGET) slot pairs [B][M][L][2] of targets codes [B][M]."""
+        codes = np.ascontiguousarray(codes, dtype=np.uint8)
+        out = np.empty((codes.shape[0], codes.shape[1], L, 2), dtype=np.uint32)
+        self._check(self.lib.si_select_states_target(self.h, L, _ptr(codes), codes.shape[0], _ptr(out)))
+        return out
+
     # -- imputation ---------------------------------------------------------------
     def impute_compact(self, codes2: np.ndarray, params: N.ImputeParams | None = None, *, dosage: bool = False):
         """Impute from 2-bit packed codes ([B][ceil(M/4)], see pack_codes) and

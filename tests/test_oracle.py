@@ -138,3 +138,41 @@ def test_oracle_floor_regime():
     out = oracle.fb_batch(codes, pairs, panel, pos, 8, 10000.0)
     assert np.all((out["dosage"] >= 0) & (out["dosage"] <= 2))
     assert np.allclose(out["dosage"], out["hap_prob"].sum(-1), atol=1e-6)
+
+
+def _target_pairs_bruteforce(panel, prefix, codes, L):
+    """Target-aware slots by explicit key comparison: the target's position at
+    marker m is the number of haplotypes whose reversed prefix (alleles m, m-1,
+    ..., 0, non-zero as 1) sorts strictly before the target's, whose own
+    alleles are its homozygous calls and elsewhere the allele of the haplotype
+    at its previous position (the last one when it sits past the end)."""
+    M, N = panel.shape
+    bits = (panel != 0).astype(np.int64)
+    tgt = []
+    p = 0
+    out = np.empty((M, L, 2), dtype=np.uint32)
+    for m in range(M):
+        prev = prefix[m - 1] if m else np.arange(N)
+        hq = prev[min(p, N - 1)]
+        tgt.append(0 if codes[m] == 0 else 1 if codes[m] == 2 else int(bits[m, hq]))
+        tkey = tgt[::-1]
+        p = 0
+        for h in range(N):
+            if list(bits[m::-1, h]) < tkey:
+                p += 1
+        s0 = min(max(p - L // 2, 0), N - L) if L <= N else 0
+        for r in range(L):
+            h = int(prefix[m][s0 + r]) if L <= N else int(prefix[m][r % N])
+            out[m, r] = (h, (h + 1) % N)
+    return out
+
+
+@pytest.mark.parametrize("M,N,L,seed", [(30, 20, 4, 0), (25, 33, 8, 1), (20, 6, 8, 2), (40, 16, 16, 3)])
+def test_target_selection_matches_key_sort(M, N, L, seed):
+    rng = np.random.default_rng(seed)
+    panel = (rng.random((M, N)) < 0.4).astype(np.uint8)
+    prefix = oracle.pbwt_build(panel)
+    for _ in range(4):
+        codes = rng.integers(0, 4, size=M).astype(np.uint8)
+        assert np.array_equal(oracle.select_pairs_target(prefix, panel, codes, L),
+                              _target_pairs_bruteforce(panel, prefix, codes, L))
