@@ -49,7 +49,7 @@ CONFIGS = {
     "serving": dict(M=120_000, N=8000, founders=200, beta=(0.3, 0.6), switch=0.002, every=20, ne=20000, seed=4,
                     pool=1024, rate=200.0, seconds=10.0, hbm_budget=120 << 30),
 }
-LEGS = ["dense_map", "uneven_batch", "serving", "large_panel"]
+LEGS = ["dense_map", "uneven_batch", "serving", "large_panel", "full_chain"]
 ALGO_BYTES_PER_CELL = 7  # 1 B genotype code in, 4 B dosage + 2 B haplotype alleles out
 POST_BYTES_PER_CELL = 6  # the posterior pass writes the outputs: 4 B dosage + 2 B alleles
 KERNELS = ["select_kernel", "anchor_lists (count+scan+fill)", "anchor_chain_kernel", "anchor_posterior_kernel"]
@@ -460,6 +460,58 @@ def leg_dense_map(local, steps, peak, cpu_targets=1024):
                        "dosage_r2_vs_fp64_oracle_masked": float(np.corrcoef(x, y)[0, 1] ** 2),
                        "argmax_haplotype_cells_differing": int((got_h != want["haps_argmax"]).sum())},
             "cpu_port_imputed_genotypes_per_s": int(masked.sum()) / cpu_s}
+
+
+def leg_full_chain(local, steps, peak, B=4000, check=64):
+    """The per-gap-map path (SI_TRANS_PER_GAP: every gap its own transition, so
+    the full-chain kernel steps every marker): the dense-cohort panel on a 1 kb
+    map, B targets typed at 3,000 markers, timed, and the first `check` targets
+    against the FP64 oracle with per-gap transitions."""
+    import torch
+    import oracle
+    from swiftimpute_b200 import _native as N
+    from swiftimpute_b200 import synth, synth_device
+    from swiftimpute_b200.engine import Engine
+    dev = torch.device("cuda", local)
+    M, Nh, L, NE = 50_000, 4432, 8, 20_000
+    panel_d = synth_device.make_panel(M, Nh, 100, seed=12, device=dev)
+    typed = synth.typed_evenly(M, 3000)
+    codes = synth_device.make_targets(panel_d, B, typed=typed, seed=12)
+    panel = panel_d.cpu().numpy()
+    del panel_d
+    pos = (1 + np.arange(M, dtype=np.uint64) * np.uint64(1000)).astype(np.uint64)
+    with Engine(local) as eng:
+        eng.upload_panel(panel)
+        eng.set_map(pos)
+        eng.pbwt_build()
+        params = N.default_params(num_states=L, ne=NE, transition_mode=N.TRANS_PER_GAP)
+        dos = torch.empty((B, M), dtype=torch.float32, device=dev)
+        haps = torch.empty((B, 2, M), dtype=torch.uint8, device=dev)
+        stream = torch.cuda.Stream(dev)
+        kms = []
+
+        def step():
+            eng.impute_device(codes.data_ptr(), B, params, dos.data_ptr(), None, haps.data_ptr(), stream.cuda_stream)
+            kms.append(eng.last_kernel_ms())
+        step()
+        kms.clear()
+        ms = _events_ms(step, steps, stream)
+        kern = sum(k[3] for k in kms) / len(kms)
+        pairs = eng.select_states(L)
+        c = codes[:check].cpu().numpy()
+        got_d = dos[:check].cpu().numpy()
+    del dos, haps, codes
+    torch.cuda.empty_cache()
+    want = oracle.fb_batch(c, pairs, panel, pos, L, float(NE), per_gap=True, threads=os.cpu_count() or 1)
+    ach = POST_BYTES_PER_CELL * B * M / (kern / 1e3) / 1e9
+    return {"workload": f"per-gap map (full chain): 4432 haplotypes x 50000 markers on a 1 kb map, {B} targets typed "
+                        "at 3000 markers, L=8, Ne=20000",
+            "value": B * (M - len(typed)) / (ms / 1e3), "unit": "imputed genotypes/s", "ms_per_step": ms,
+            "fb_chain_kernel_ms": kern,
+            "roofline": {"bound": "hbm", "kernel": "fb_chain_kernel", "achieved": ach, "peak": peak, "unit": "GB/s",
+                         "frac": ach / peak, "note": "6 B per cell written"},
+            "parity": {"targets": int(check), "max_abs_dosage_diff_vs_fp64_oracle":
+                       float(np.abs(got_d - want["dosage"]).max())}}
 
 
 def uneven_panel(local, seed=2):
@@ -884,6 +936,8 @@ def run_leg(args):
         out = leg_dense_map(local, max(3, args.steps // 2), peak)
     elif args.leg == "large_panel":
         out = leg_large_panel(local, max(3, args.steps // 2), peak)
+    elif args.leg == "full_chain":
+        out = leg_full_chain(local, 3, peak)
     else:
         up = uneven_panel(local)
         out = leg_uneven(local, max(3, args.steps), peak, *up) if args.leg == "uneven_batch" else \

@@ -242,13 +242,16 @@ __global__ void __launch_bounds__(1024) anchor_scan_kernel(const uint32_t* __res
 // scales every slot by e^-999, counted in beta's unit, in bit 31) and emission
 // mask over the slots, in marker order; marker 0 is always an anchor. A warp
 // (one CTA) fills one segment of kFillSeg markers of the 32 samples of a
-// group, lane = sample: chunks of 32 rows x 512 codes come into shared memory
-// by cp.async, the next chunk in flight while each lane scans its own row of
-// the current one, and lanes that meet their anchors in step (shared typed
-// positions) write whole 128-byte lines of the interleaved lists. A lane's
-// first entry of the segment is the sum of its earlier segments' counts.
-constexpr uint32_t kFillRow = 512 + 16;  // row stride in shared memory (bytes): conflict-free 128-bit reads
-constexpr size_t kFillSmem = 2 * 32 * kFillRow + 32 * 16;  // two chunk buffers and the row descriptors
+// group, lane = sample: chunks of 32 rows x 256 codes (and, for a plain batch,
+// the chunk's slot masks) come into shared memory by cp.async, the next chunk
+// in flight while each lane scans its own row of the current one, and lanes
+// that meet their anchors in step (shared typed positions) write whole
+// 128-byte lines of the interleaved lists. A lane's first entry of the segment
+// is the sum of its earlier segments' counts.
+constexpr uint32_t kFillChunk = 256;                 // markers per staged chunk
+constexpr uint32_t kFillRow = kFillChunk + 16;        // row stride in shared memory (bytes): conflict-free 128-bit reads
+constexpr size_t kFillBuf = 32 * kFillRow + kFillChunk * sizeof(SlotMasks);  // codes of 32 rows, the chunk's slot masks
+constexpr size_t kFillSmem = 2 * kFillBuf + 32 * 16;  // two chunk buffers and the row descriptors
 
 __global__ void __launch_bounds__(32) anchor_fill_kernel(TypedArgs A) {
     extern __shared__ __align__(16) unsigned char fsm[];
@@ -256,7 +259,7 @@ __global__ void __launch_bounds__(32) anchor_fill_kernel(TypedArgs A) {
     const uint32_t G = (A.B + 31) / 32;
     const uint32_t g = blockIdx.x % G, seg = blockIdx.x / G;
     const uint32_t s = g * 32 + lane;
-    uint4* rowd = reinterpret_cast<uint4*>(fsm + 2 * 32 * kFillRow);  // [32] {ptr lo, ptr hi, len, 16-byte aligned}
+    uint4* rowd = reinterpret_cast<uint4*>(fsm + 2 * kFillBuf);  // [32] {ptr lo, ptr hi, len, 16-byte aligned}
     View v{};
     uint32_t len = 0, at = 0, lim = 0;
     if (s < A.B) {
@@ -274,33 +277,43 @@ __global__ void __launch_bounds__(32) anchor_fill_kernel(TypedArgs A) {
     __syncwarp();
     const uint32_t lmask = lmask_of(v.r.L);
     const unsigned long long lb = A.aoff[g] + lane;
-    // chunk at c0 into b: lane i copies bytes [16 i, 16 i + 16) of every row
+    // a plain batch shares one slot-mask table: its chunk is staged beside the codes
+    const bool stage_masks = A.samples == nullptr;
+    const SlotMasks* gmasks = A.reg0.masks;
+    // chunk at c0 into buffer b: rows 2 it + lane / 16, bytes 16 (lane % 16) .. + 16, and the masks
     auto issue = [&](uint32_t c0, unsigned char* b) {
-        const uint32_t mm = c0 + 16 * lane;
-#pragma unroll 8
-        for (uint32_t r = 0; r < 32; ++r) {
+        const uint32_t mm = c0 + 16 * (lane & 15);
+#pragma unroll 4
+        for (uint32_t it = 0; it < 16; ++it) {
+            const uint32_t r = 2 * it + (lane >> 4);
             const uint4 d = rowd[r];
             const uint8_t* gr = reinterpret_cast<const uint8_t*>(((unsigned long long)d.y << 32) | d.x);
-            unsigned char* dst = b + r * kFillRow + 16 * lane;
+            unsigned char* dst = b + r * kFillRow + 16 * (lane & 15);
             if (d.w && mm + 16 <= d.z) cp_async16(dst, gr + mm);
             else *reinterpret_cast<uint4*>(dst) = load16(gr, mm, d.z, d.w != 0);  // a ragged or unaligned row
+        }
+        if (stage_masks) {
+            SlotMasks* sm = reinterpret_cast<SlotMasks*>(b + 32 * kFillRow);
+            for (uint32_t i = lane; i < kFillChunk && c0 + i < A.M; i += 32) cp_async16(sm + i, gmasks + c0 + i);
         }
         cp_async_commit();
     };
     const uint32_t cend = min(m0 + kFillSeg, mlast);
     issue(m0, fsm);
     uint32_t bi = 0;
-    for (uint32_t c0 = m0; c0 < cend; c0 += 512, bi ^= 1) {
-        if (c0 + 512 < cend) {
-            issue(c0 + 512, fsm + (bi ^ 1) * 32 * kFillRow);
+    for (uint32_t c0 = m0; c0 < cend; c0 += kFillChunk, bi ^= 1) {
+        if (c0 + kFillChunk < cend) {
+            issue(c0 + kFillChunk, fsm + (bi ^ 1) * kFillBuf);
             cp_async_wait_group<1>();  // this lane's copies of the current chunk have landed
         } else {
             cp_async_wait_group<0>();
         }
         __syncwarp();  // ... and every lane's
         if (c0 < len) {
-            const unsigned char* row = fsm + bi * 32 * kFillRow + lane * kFillRow;
-            for (uint32_t q = 0; q < 32; ++q) {
+            const unsigned char* buf = fsm + bi * kFillBuf;
+            const unsigned char* row = buf + lane * kFillRow;
+            const SlotMasks* sm = reinterpret_cast<const SlotMasks*>(buf + 32 * kFillRow);
+            for (uint32_t q = 0; q < kFillChunk / 16; ++q) {
                 const uint4 x = *reinterpret_cast<const uint4*>(row + 16 * q);
                 uint32_t bits = typed_bits(x);
                 const uint32_t base = c0 + 16 * q;
@@ -312,7 +325,8 @@ __global__ void __launch_bounds__(32) anchor_fill_kernel(TypedArgs A) {
                     if (at < lim) {
                         uint32_t sh;
                         const uint32_t w = j < 8 ? (j < 4 ? x.x : x.y) : (j < 12 ? x.z : x.w);
-                        const uint32_t em = emission_mask((w >> (8 * (j & 3))) & 0xffu, v.r.masks[m], lmask, &sh);
+                        const SlotMasks mk = stage_masks ? sm[m - c0] : v.r.masks[m];
+                        const uint32_t em = emission_mask((w >> (8 * (j & 3))) & 0xffu, mk, lmask, &sh);
                         A.apos[lb + 32ull * at] = m | (sh ? kShiftBit : 0u);
                         A.aem[lb + 32ull * at] = em;
                     }
