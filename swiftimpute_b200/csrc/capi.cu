@@ -459,6 +459,9 @@ si_status run_device(si_ctx* ctx, const si_impute_params* p, const uint8_t* d_ge
     }
     uint32_t T, C;
     default_tiles(p->num_states, &T, &C);
+    // one chain per thread: a batch that fills fewer than two CTAs per SM takes 32-chain CTAs
+    // (the CTA size changes nothing numerically)
+    if (T > 32 && (B + T - 1) / T < 2u * 148u) T = 32;
     if (p->checkpoint_interval) C = p->checkpoint_interval;
     if (p->block_threads) T = p->block_threads;
     if (fb_smem_bytes(p->num_states, T, C) > 227u * 1024u)
