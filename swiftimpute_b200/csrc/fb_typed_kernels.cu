@@ -448,11 +448,13 @@ __global__ void __launch_bounds__(32) anchor_chain_kernel(TypedArgs A) {
     const bool forward = (wg & 1u) == 0;
     const uint32_t s = (wg >> 1) * 32 + lane;
     const bool live = s < A.B;
-    View v{};
+    // A lane past the batch's end takes the last sample's tables: its discarded
+    // lookups (gap 0) then read the tables like its warp's live lanes instead of
+    // evaluating the FP64 closed form past a table of zero entries every step.
+    const View v = view_of(A, live ? s : A.B - 1);
     uint32_t NA = 0;
     unsigned long long base = 0, wb = 0;
     if (live) {
-        v = view_of(A, s);
         base = A.aoff[s >> 5] + lane;
         wb = A.woff[s >> 5] + lane;
         NA = A.counts[s];

@@ -4,9 +4,12 @@ markers, L = 8, Ne = 20,000, markers 1 kb apart (rho = 1 - exp(-16 Ne d)
 stays below 1, so the transition is not the memoryless one the 0.5 cM map
 gives, transition.cu:91-96).
 
-All 10,000 targets are imputed on the device; the first 1,024 are checked
-against the FP64 oracle (dosage and P(hap=1) within 1e-4, argmax haplotypes
-bit-exact except at threshold flips). Panel and targets come from the device
+All 10,000 targets are imputed on the device; 768 from the start and the
+last 256 (ending in the batch's partial 32-sample group, whose chain warp
+also runs lanes past the batch's end) are checked against the FP64 oracle
+(dosage and P(hap=1) within 1e-4, argmax haplotypes bit-exact except at
+threshold flips), and the last 1,000 imputed alone match the full batch bit
+for bit. Panel and targets come from the device
 generator (swiftimpute_b200.synth_device) with the workload's shapes.
 """
 import numpy as np
@@ -20,6 +23,7 @@ pytestmark = pytest.mark.gpu
 
 M, NH, B, NTYPED, L, NE = 50_000, 4432, 10_000, 3000, 8, 20_000
 CHECK = 1024
+ROWS = np.r_[0:768, B - 256:B]  # the batch's start and its end (partial last group)
 
 
 @pytest.mark.parametrize("spacing", [1000])
@@ -43,10 +47,22 @@ def test_dense_cohort_full_size_against_oracle(engine, spacing):
     engine.impute_device(codes_d.data_ptr(), B, params, dos.data_ptr(), hp.data_ptr(), haps.data_ptr())
     torch.cuda.synchronize(dev)
     assert bool(torch.isfinite(dos).all()) and float(dos.min()) >= -1e-6 and float(dos.max()) <= 2 + 1e-5
-    codes = codes_d[:CHECK].cpu().numpy()
-    got_d = dos[:CHECK].cpu().numpy()
-    got_p = hp[:CHECK].cpu().numpy()
-    got_h = haps[:CHECK].cpu().numpy()
+    # batch invariance: the last 1,000 targets alone
+    tail = B - 1000
+    dos1 = torch.empty((1000, M), dtype=torch.float32, device=dev)
+    hp1 = torch.empty((1000, M, 2), dtype=torch.float32, device=dev)
+    haps1 = torch.empty((1000, 2, M), dtype=torch.uint8, device=dev)
+    p1 = N.default_params(num_states=L, ne=NE)
+    p1.sample_id_base = tail
+    engine.impute_device(codes_d[tail:].data_ptr(), 1000, p1, dos1.data_ptr(), hp1.data_ptr(), haps1.data_ptr())
+    torch.cuda.synchronize(dev)
+    assert torch.equal(dos1, dos[tail:]) and torch.equal(hp1, hp[tail:]) and torch.equal(haps1, haps[tail:])
+    del dos1, hp1, haps1
+    rows = torch.from_numpy(ROWS).to(dev)
+    codes = codes_d[rows].cpu().numpy()
+    got_d = dos[rows].cpu().numpy()
+    got_p = hp[rows].cpu().numpy()
+    got_h = haps[rows].cpu().numpy()
     pairs = engine.select_states(L)
     want = oracle.fb_batch(codes, pairs, panel, pos, L, float(NE))
     dd = np.abs(got_d - want["dosage"]).max()
