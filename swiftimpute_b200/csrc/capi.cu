@@ -277,7 +277,7 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
         const double lgc = regime == 0 ? std::log1p(-rho) : (regime == 1 ? std::log(rho - 1.0) : 0.0);
         // QS [n] {Q, S}; then the pair tables {Q_n, Q_n+1, S_n, S_n+1} and
         // {Q_n, Q_n-1, S_n, S_n-1} (index 0: Q_0, S_0 twice) for two consecutive cells
-        std::vector<float> QS(2 * kTabN + 8 * kTabN);
+        std::vector<float> QS(2 * kTabN + 12 * kTabN);
         std::vector<double> G(kTabN);
         std::vector<float> qf(kTabN + 1), sf(kTabN + 1);
         for (uint32_t n = 0; n <= kTabN; ++n) {
@@ -299,6 +299,15 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
             else if (regime == 1) G[n] = std::log(-std::expm1(-(double)n * lr)) - lgc;
             else G[n] = std::log((double)n);
         }
+        // Gdn [n] {hi G_n, hi G_n-1, lo G_n, lo G_n-1}: G as a float pair, so the floor's
+        // log farg' + G_j (nearly cancelling where the floor matters) is formed in FP32
+        float* gd = dn + 4 * kTabN;
+        auto hi = [&](uint32_t n) { return n == 0 ? -1e30f : (float)G[n]; };
+        auto lo = [&](uint32_t n) { return n == 0 ? 0.f : (float)(G[n] - (double)(float)G[n]); };
+        for (uint32_t n = 0; n < kTabN; ++n) {
+            const uint32_t b = n ? n - 1 : 0;
+            gd[4 * n] = hi(n); gd[4 * n + 1] = hi(b); gd[4 * n + 2] = lo(n); gd[4 * n + 3] = lo(b);
+        }
         si_status st = dev_alloc(ctx, ts.QS, QS.size() * 4);
         if (st == SI_OK) st = dev_alloc(ctx, ts.G, kTabN * 8);
         if (st != SI_OK) {
@@ -316,6 +325,7 @@ si_status tables_for(si_ctx* ctx, const LinTrans& t0, uint32_t L, TypedTables* o
     out->QS = (const float2*)ts.QS.ptr; out->G = (const double*)ts.G.ptr;
     out->QSup = (const float4*)((const float*)ts.QS.ptr + 2 * kTabN);
     out->QSdn = out->QSup + kTabN;
+    out->Gdn = out->QSdn + kTabN;
     out->NT = kTabN; out->log2q = (float)ts.consts[0]; out->invL = 1.0f / (float)L;
     out->lr = ts.consts[1]; out->lgc = ts.consts[2]; out->regime = (int)ts.consts[3];
     return SI_OK;

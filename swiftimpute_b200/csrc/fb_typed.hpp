@@ -9,11 +9,13 @@ namespace si {
 // (c, delta), computed in FP64 on the host: q = delta / rho, rho = delta + L c,
 // QS[n] = {Q[n], S[n]} = {q^n, (1 - q^n) / L}, G[n] = log sum_{k=1..n} rho^-k;
 // for two consecutive cells QSup[n] = {Q[n], Q[n+1], S[n], S[n+1]} and
-// QSdn[n] = {Q[n], Q[n-1], S[n], S[n-1]}.
+// QSdn[n] = {Q[n], Q[n-1], S[n], S[n-1]}; Gdn[n] = {hi G[n], hi G[n-1],
+// lo G[n], lo G[n-1]}, G as a float pair hi + lo (G[0] = -inf stands as -1e30).
 struct TypedTables {
     const float2* QS;
     const float4* QSup;
     const float4* QSdn;
+    const float4* Gdn;
     const double* G;
     uint32_t NT;
     float log2q;

@@ -907,6 +907,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
     auto set_a = [&](int l, float x) { if constexpr (kBcast) a2[l] = make_float2(x, x); else ap[l] = x; };
     auto set_w = [&](int l, float x) { if constexpr (kBcast) w2[l] = make_float2(x, x); else wp[l] = x; };
     uint4 fr = make_uint4(0u, kNegInfHi, 0u, 0u);  // the current run's record: farg' lo, hi, end, end emission
+    float2 FH = make_float2(0.f, 0.f), FL = make_float2(0.f, 0.f);  // a floor run's farg' as float hi + lo
     uint32_t k = w0 * C, p0 = 0, p1 = 0, m = 0, mend = 0;
     auto load_record = [&](uint32_t r) {
 #pragma unroll
@@ -915,6 +916,12 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
             set_w(4 * q, x.x); set_w(4 * q + 1, x.y); set_w(4 * q + 2, x.z); set_w(4 * q + 3, x.w);
         }
         fr = recF[r * 32 + lane];
+        if ((fr.y & kInfHi) != kInfHi) {
+            const double fa = __hiloint2double((int)fr.y, (int)fr.x);
+            const float h = (float)fa, l = (float)(fa - (double)h);
+            FH = make_float2(h, h);
+            FL = make_float2(l, l);
+        }
     };
     if (live) {
         stage_window<LM>(A, apos, aem, wb, NA, w0, st, lane);
@@ -1010,13 +1017,22 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
         if (fr.y == kInfHi) {
             YY = make_float2(1.f, 1.f);  // uniform run: w' = 0, beta = 1
         } else if ((fr.y & kInfHi) != kInfHi) {
-            // floor e^ft beside Q w' + S; when it dominates (ft > 0) scale both by e^-ft
-            const double fa = __hiloint2double((int)fr.y, (int)fr.x);
-            float ft[2] = {(float)(fa + tabG(tb, j)), (float)(fa + tabG(tb, j - 1))};
+            // floor e^ft beside Q w' + S, ft = farg' + G(j); when it dominates (ft > 0) scale both by e^-ft
+            float2 ft2;
+            if (in_tab) {
+                // (hi + hi) + (lo + lo) in FP32: where the floor is within reach of the carried
+                // terms the high parts nearly cancel, and their sum is exact
+                const float4 g = __ldg(tb.Gdn + j);
+                ft2 = __fadd2_rn(__fadd2_rn(FH, make_float2(g.x, g.y)), __fadd2_rn(FL, make_float2(g.z, g.w)));
+            } else {
+                const double fa = __hiloint2double((int)fr.y, (int)fr.x);
+                ft2 = make_float2((float)(fa + tabG(tb, j)), (float)(fa + tabG(tb, j - 1)));
+            }
+            const float ft[2] = {ft2.x, ft2.y};
             float xx[2] = {XX.x, XX.y}, yy[2] = {YY.x, YY.y};
 #pragma unroll
             for (int c = 0; c < 2; ++c) {
-                const float e = expf(-fminf(fabsf(ft[c]), 104.f));
+                const float e = exp2f(fminf(fabsf(ft[c]), 104.f) * -1.44269504088896341f);  // e^-|ft|
                 const bool big = ft[c] > 0.f;
                 const float xs = big ? e : 1.f;
                 const float F = big ? 1.f : (ft[c] > -104.f ? e : 0.f);
