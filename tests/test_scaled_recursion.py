@@ -67,3 +67,45 @@ def test_scaled_recursion_equals_log_space_oracle(spacing, every, M):
         deep |= bool(lp.min() < -1500)
     if spacing == 100 and every == 5:
         assert deep  # the case reaches the floor regime with unmatched calls on top
+
+
+def _floor_tables(spacing, L, ne=20000.0, NT=4096):
+    """G[n] = log sum_{k=1..n} rho^-k of the run tables, rho = delta + L c of the map's first gap,
+    in FP64 as the host builds them (three regimes of rho)."""
+    pos = 1 + np.arange(3, dtype=np.uint64) * np.uint64(spacing)
+    td, to = oracle.transitions(pos, ne)
+    c = float(np.float32(math.exp(float(to[0]))))
+    dl = float(np.float32(float(np.float32(math.exp(float(td[0])))) - c))
+    rho = dl + L * c
+    lr = math.log(rho)
+    regime = 2 if abs(rho - 1.0) < 1e-15 else (0 if rho < 1.0 else 1)
+    lgc = math.log1p(-rho) if regime == 0 else (math.log(rho - 1.0) if regime == 1 else 0.0)
+    n = np.arange(1, NT, dtype=np.float64)
+    if regime == 0:
+        G = -n * lr + np.log(-np.expm1(n * lr)) - lgc
+    elif regime == 1:
+        G = np.log(-np.expm1(-n * lr)) - lgc
+    else:
+        G = np.log(n)
+    return G
+
+
+@pytest.mark.parametrize("spacing", [30, 1000, 500_000])
+@pytest.mark.parametrize("L", [4, 8, 32])
+def test_floor_log_as_float_pairs(spacing, L):
+    """The posterior forms a cell's floor log farg' + G(j) in FP32 as (hi + hi) + (lo + lo),
+    farg' and G(j) each split into a float and the float of its remainder. Wherever the floor
+    can matter (sum in [-120, 80]) that is within 1 ulp of the FP64 sum rounded to FP32, for
+    every table entry j and run constants drawn over that window."""
+    G = _floor_tables(spacing, L)
+    hi = G.astype(np.float32)
+    lo = (G - hi.astype(np.float64)).astype(np.float32)
+    rng = np.random.default_rng(spacing + L)
+    for _ in range(8):
+        fa = rng.uniform(-120.0, 80.0, size=G.size) - G
+        fah = fa.astype(np.float32)
+        fal = (fa - fah.astype(np.float64)).astype(np.float32)
+        ft = (fah + hi) + (fal + lo)
+        ref = (fa + G).astype(np.float32)
+        err = np.abs(ft.astype(np.float64) - ref.astype(np.float64))
+        assert (err <= np.spacing(np.abs(ref)).astype(np.float64)).all()
