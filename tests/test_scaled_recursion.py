@@ -109,3 +109,62 @@ def test_floor_log_as_float_pairs(spacing, L):
         ref = (fa + G).astype(np.float32)
         err = np.abs(ft.astype(np.float64) - ref.astype(np.float64))
         assert (err <= np.spacing(np.abs(ref)).astype(np.float64)).all()
+
+
+def _anchor_steps(M, spacing, every, L=8, seed=0):
+    """Emission masks at the typed markers of one target and the closed-form run coefficients
+    {Q_n, S_n} between consecutive typed markers (the chain's step maps)."""
+    panel, pos, _ = synth.make_panel(M, 300, 12, seed=seed + M, spacing=spacing)
+    typed = synth.typed_every(M, every)
+    codes, _, _ = synth.make_targets(panel, 1, typed, seed=seed + 3)
+    pairs = oracle.select_pairs(oracle.pbwt_build(panel), L)
+    td, to = oracle.transitions(pos, 20000.0)
+    c = math.exp(float(to[0])); d = math.exp(float(td[0])); dl = d - c
+    q = dl / (dl + L * c)
+    alt = (panel[np.arange(M)[:, None], pairs[:, :, 0]].astype(int)
+           + panel[np.arange(M)[:, None], pairs[:, :, 1]].astype(int))
+    E = (alt[typed] == codes[0, typed][:, None]).astype(np.float64)
+    E[E.sum(1) == 0] = 1.0  # no slot matches the call: every slot scaled alike
+    Q = q ** np.diff(typed).astype(np.float64)
+    return E, Q, (1.0 - Q) / L
+
+
+def _forward(E, Q, S, dt, x, k0, k1, out):
+    for k in range(k0 + 1, k1 + 1):
+        x = (E[k] * (dt(Q[k - 1]) * x + dt(S[k - 1]) * x.sum())).astype(dt)
+        x /= x.sum()
+        out[k] = x
+    return x
+
+
+@pytest.mark.parametrize("spacing,every", [(100, 5), (1000, 17), (30, 3), (500_000, 5)])
+def test_forward_segment_products_fp32(spacing, every):
+    """Chunked parallel-in-time form of the forward chain over typed anchors: each segment's
+    8 x 8 product of step maps D_k (Q_n I + S_n 11^T) in FP32 (rescaled by its maximum), the
+    segment starts by a short sequential pass of products, then every segment re-run from its
+    start. Its alpha stays as close to the FP64 sequential chain as the FP32 sequential chain
+    is, at 8 and 64 segments."""
+    E, Q, S = _anchor_steps(20_000, spacing, every)
+    K, L = E.shape
+    ref = np.empty((K, L)); ref[0] = E[0] / E[0].sum()
+    _forward(E, Q, S, np.float64, ref[0], 0, K - 1, ref)
+    seq = np.empty((K, L), np.float32); seq[0] = ref[0]
+    _forward(E, Q, S, np.float32, seq[0].copy(), 0, K - 1, seq)
+    err_seq = np.abs(seq - ref).max()
+    for nseg in (8, 64):
+        b = np.linspace(0, K - 1, nseg + 1).astype(int)
+        x = seq[0].copy()
+        out = np.empty((K, L), np.float32); out[0] = x
+        starts = [x]
+        for s in range(nseg):
+            P = np.eye(L, dtype=np.float32)
+            for k in range(b[s] + 1, b[s + 1] + 1):
+                P = (E[k][:, None] * (np.float32(Q[k - 1]) * P + np.float32(S[k - 1]) * P.sum(0)[None, :]))
+                P = (P / P.max()).astype(np.float32)
+            x = (P @ x).astype(np.float32); x /= x.sum()
+            starts.append(x)
+        for s in range(nseg):
+            out[b[s]] = starts[s]
+            _forward(E, Q, S, np.float32, starts[s].copy(), b[s], b[s + 1], out)
+        err = np.abs(out - ref).max()
+        assert err <= max(2.0 * err_seq, 1e-7), (nseg, err, err_seq)
