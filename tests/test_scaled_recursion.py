@@ -168,3 +168,74 @@ def test_forward_segment_products_fp32(spacing, every):
             _forward(E, Q, S, np.float32, starts[s].copy(), b[s], b[s + 1], out)
         err = np.abs(out - ref).max()
         assert err <= max(2.0 * err_seq, 1e-7), (nseg, err, err_seq)
+
+
+def _combine(v1, l1, v2, l2):
+    """e^l1 v1 + e^l2 v2 as (v, l) with max(v) = 1, FP32 vectors and FP64 logs."""
+    if l1 < l2:
+        v1, l1, v2, l2 = v2, l2, v1, l1
+    v = v1 if (l2 == -math.inf or l1 - l2 > 104.0) else (v1 + np.float32(math.exp(l2 - l1)) * v2).astype(np.float32)
+    mx = float(v.max())
+    return (v / np.float32(mx)).astype(np.float32), l1 + math.log(mx)
+
+
+@pytest.mark.parametrize("spacing,every,M", [(100, 5, 900), (500_000, 5, 400), (30, 50, 1200), (100, 2, 600)])
+def test_backward_segment_maps_with_floor_fp32(spacing, every, M):
+    """Chunked parallel-in-time form of the backward chain with the reference's e^-999 floor.
+    In absolute units a step is affine, beta_m = e^(-999 sh) T diag(E_m+1) beta_m+1 + e^-999 1,
+    so a segment composes to beta_start = e^a A beta_end + e^bs b: A (L x L) and b in FP32 with
+    their logs a, bs in FP64, the floor column merged like the sequential step (dropped beyond
+    e^104). Applied from the chain's end one segment at a time, it lands on the FP64 sequential
+    chain's state (unit-sum w and log U) at every segment start."""
+    panel, pos, _ = synth.make_panel(M, 300, 12, seed=M + every, spacing=spacing)
+    codes, _, _ = synth.make_targets(panel, 1, synth.typed_every(M, every), seed=3)
+    L = 8
+    pairs = oracle.select_pairs(oracle.pbwt_build(panel), L)
+    td, to = oracle.transitions(pos, 10000.0)
+    c = math.exp(float(to[0])); dl = math.exp(float(td[0])) - c
+    alt = (panel[np.arange(M)[:, None], pairs[:, :, 0]].astype(int)
+           + panel[np.arange(M)[:, None], pairs[:, :, 1]].astype(int))
+    E, SH = np.ones((M, L)), np.zeros(M, int)
+    for m in range(M):
+        if codes[0, m] < 3:
+            e = (alt[m] == codes[0, m]).astype(float)
+            if e.sum() == 0:
+                SH[m] = 1
+            else:
+                E[m] = e
+    # FP64 sequential chain (the kernel's reformulation, equal to the log-space oracle above)
+    ref_w, ref_l = np.empty((M, L)), np.empty(M)
+    be, logs = np.ones(L) / L, math.log(L)
+    ref_w[M - 1], ref_l[M - 1] = be, logs
+    for m in range(M - 2, -1, -1):
+        u = c * (E[m + 1] * be).sum() + dl * E[m + 1] * be
+        lu = logs - 999.0 * SH[m + 1]
+        f = -999.0 - lu
+        v, ln = (1.0 + math.exp(-f) * u, -999.0) if f > 0 else ((math.exp(f) if f > -700 else 0.0) + u, lu)
+        be, logs = v / v.sum(), ln + math.log(v.sum())
+        ref_w[m], ref_l[m] = be, logs
+    T = (np.float32(c) * np.ones((L, L)) + np.float32(dl) * np.eye(L)).astype(np.float32)
+    for nseg in (4, 16):
+        bnd = np.linspace(0, M - 1, nseg + 1).astype(int)
+        w, lw = ref_w[M - 1].astype(np.float32), ref_l[M - 1]
+        for s in range(nseg - 1, -1, -1):
+            A, a, b, bs = np.eye(L, dtype=np.float32), 0.0, np.zeros(L, np.float32), -math.inf
+            for m in range(bnd[s + 1] - 1, bnd[s] - 1, -1):
+                Ai = (T * E[m + 1][None, :]).astype(np.float32)
+                A = (Ai @ A).astype(np.float32)
+                mx = float(A.max())
+                A, a = (A / np.float32(mx)).astype(np.float32), a - 999.0 * SH[m + 1] + math.log(mx)
+                if bs > -math.inf:
+                    v = (Ai @ b).astype(np.float32)
+                    mv = float(v.max())
+                    b, bs = _combine((v / np.float32(mv)).astype(np.float32), bs - 999.0 * SH[m + 1] + math.log(mv),
+                                     np.ones(L, np.float32), -999.0)
+                else:
+                    b, bs = np.ones(L, np.float32), -999.0
+            v = (A @ w).astype(np.float32)
+            mv = float(v.max())
+            v, lv = _combine((v / np.float32(mv)).astype(np.float32), a + lw + math.log(mv), b, bs)
+            sm = float(v.sum())
+            w, lw = (v / np.float32(sm)).astype(np.float32), lv + math.log(sm)
+            assert np.abs(w - ref_w[bnd[s]]).max() <= 1e-6
+            assert abs(lw - ref_l[bnd[s]]) <= 1e-4
