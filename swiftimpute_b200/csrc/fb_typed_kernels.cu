@@ -834,6 +834,8 @@ __device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& t
 // kFull: every sample of the launch uses all LM slots (no active-slot masking).
 // kFast: argmax picks, no P(hap=1). kPlain: every sample covers the whole
 // panel with the launch's one region (read from the kernel parameters).
+// kDos: dosage written (false only with kFast, for calls that return the
+// phased alleles alone: no dosage sums and no g2 loads).
 // A lane takes two consecutive cells of a run per step (an even marker and
 // the next one) with f32x2 arithmetic across the two cells; a run's odd first
 // marker or last marker takes a step alone (the second half is discarded).
@@ -841,7 +843,7 @@ __device__ __forceinline__ void rebuild_window(const TypedArgs& A, const Tabs& t
 // Tiles are aligned to absolute 32-marker columns, so a tile every lane of a
 // warp fills completely (lanes that share typed positions) leaves as 128-bit
 // row segments.
-template <int LM, bool kFull, bool kFast, bool kPlain>
+template <int LM, bool kFull, bool kFast, bool kPlain, bool kDos>
 __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
     anchor_posterior_kernel(const __grid_constant__ TypedArgs A) {
     extern __shared__ __align__(16) unsigned char smem[];
@@ -889,7 +891,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
     const uint32_t Lr = R.L;
     const uint32_t* apos = A.apos + ab;  // entry k at [32 k]
     const uint32_t* aem = A.aem + ab;
-    const bool w_dos = A.dosage != nullptr, w_hap = A.haps != nullptr;
+    const bool w_dos = kDos && A.dosage != nullptr, w_hap = A.haps != nullptr;
     const bool w_hp = !kFast && A.hprob != nullptr;
     const bool argmax = kFast || A.sampling == SI_SAMPLE_ARGMAX;
     const float keep = 1.0f - A.tie_eps;
@@ -1063,7 +1065,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
         float2 d2 = make_float2(0.f, 0.f);
 #pragma unroll
         for (int q = 0; q < LM / 2; ++q) {
-            if (kFull || (uint32_t)(2 * q) < R.gs) {
+            if (kDos && (kFull || (uint32_t)(2 * q) < R.gs)) {
                 const float4 gv = __ldg(g4 + q);
                 d2 = __ffma2_rn(p2[2 * q], make_float2(gv.x, gv.y), d2);
                 d2 = __ffma2_rn(p2[2 * q + 1], make_float2(gv.z, gv.w), d2);
@@ -1097,7 +1099,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
         const uint32_t hA = slot_alleles(mkA, R.raw, R.gs, mm, pk[0]);
         if (two) {
             const uint32_t hB = slot_alleles(mkB, R.raw, R.gs, mm + 1, pk[1]);
-            *reinterpret_cast<float2*>(tD + lane * 36 + c0) = dos2;
+            if constexpr (kDos) *reinterpret_cast<float2*>(tD + lane * 36 + c0) = dos2;
             *reinterpret_cast<uint16_t*>(tH + (2 * lane) * 36 + c0) = (uint16_t)((hA & 0xffu) | ((hB & 0xffu) << 8));
             *reinterpret_cast<uint16_t*>(tH + (2 * lane + 1) * 36 + c0) = (uint16_t)((hA >> 8) | (hB & 0xff00u));
             if (w_hp) {
@@ -1113,7 +1115,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
                     make_float4(q0[0] * inv2.x, q1[0] * inv2.x, q0[1] * inv2.y, q1[1] * inv2.y);
             }
         } else {
-            tD[lane * 36 + c0] = dos2.x;
+            if constexpr (kDos) tD[lane * 36 + c0] = dos2.x;
             tH[(2 * lane) * 36 + c0] = (uint8_t)(hA & 0xffu);
             tH[(2 * lane + 1) * 36 + c0] = (uint8_t)(hA >> 8);
             if (w_hp) {
@@ -1183,7 +1185,7 @@ __global__ void __launch_bounds__(128, (LM <= 8 ? (kPlain ? 4 : 3) : 2))
     }
 }
 
-template <int LM, bool kFull, bool kFast, bool kPlain>
+template <int LM, bool kFull, bool kFast, bool kPlain, bool kDos = true>
 cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     const uint32_t T = a.threads;
     const size_t sm = (size_t)(T / 32) * post_warp_bytes(LM, a.C, !kFast);
@@ -1192,7 +1194,7 @@ cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     cudaError_t e = cudaStreamIsCapturing(s, &cs);
     if (e != cudaSuccess) return e;
     if (cs == cudaStreamCaptureStatusNone) {
-        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull, kFast, kPlain>,
+        e = cudaFuncSetAttribute(anchor_posterior_kernel<LM, kFull, kFast, kPlain, kDos>,
                                  cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sm);
         if (e != cudaSuccess) return e;
     }
@@ -1201,13 +1203,16 @@ cudaError_t launch_post_v(const TypedArgs& a, cudaStream_t s) {
     const unsigned long long grid = (warps + T / 32 - 1) / (T / 32);
     if (grid == 0) return cudaSuccess;
     if (grid > 0x7fffffffull) return cudaErrorInvalidConfiguration;
-    anchor_posterior_kernel<LM, kFull, kFast, kPlain><<<(uint32_t)grid, T, sm, s>>>(a);
+    anchor_posterior_kernel<LM, kFull, kFast, kPlain, kDos><<<(uint32_t)grid, T, sm, s>>>(a);
     return cudaGetLastError();
 }
 
 template <int LM, bool kFull>
 cudaError_t launch_post(const TypedArgs& a, cudaStream_t s) {
     const bool fast = !a.hprob && a.sampling == SI_SAMPLE_ARGMAX;
+    if (fast && !a.dosage)
+        return a.samples ? launch_post_v<LM, kFull, true, false, false>(a, s)
+                         : launch_post_v<LM, kFull, true, true, false>(a, s);
     if (!a.samples)
         return fast ? launch_post_v<LM, kFull, true, true>(a, s) : launch_post_v<LM, kFull, false, true>(a, s);
     return fast ? launch_post_v<LM, kFull, true, false>(a, s) : launch_post_v<LM, kFull, false, false>(a, s);

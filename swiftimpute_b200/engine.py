@@ -197,11 +197,12 @@ class Engine:
                                               c_void_p(stream) if stream else None))
 
     def impute_jobs(self, regions, jobs, params: N.ImputeParams | None = None, *, hap_prob: bool = False,
-                    stream: int | None = None):
+                    dosage: bool = True, stream: int | None = None):
         """Uneven batch. ``regions``: list of (m_begin, m_end, L, index_origin);
         ``jobs``: list of (region, codes[len] u8, sample_id). Outputs are packed per
-        job; returns a list of dicts (dosage [len], haps [2][len], hap_prob [len][2]).
-        Device buffers are allocated with torch (plumbing only)."""
+        job; returns a list of dicts (dosage [len] unless ``dosage`` is false,
+        haps [2][len], hap_prob [len][2]). Device buffers are allocated with torch
+        (plumbing only)."""
         import torch
         params = params or N.default_params()
         R = (N.Region * len(regions))(*[N.Region(a, b, L, o) for a, b, L, o in regions])
@@ -212,22 +213,25 @@ class Engine:
         geno = np.concatenate([np.asarray(c, dtype=np.uint8).ravel() for _, c, _ in jobs] + [np.zeros(1, np.uint8)])
         dev = torch.device("cuda", self.device)
         d_geno = torch.from_numpy(geno).to(dev)
-        d_dos = torch.empty(total, dtype=torch.float32, device=dev)
+        d_dos = torch.empty(total, dtype=torch.float32, device=dev) if dosage else None
         d_haps = torch.empty(2 * total, dtype=torch.uint8, device=dev)
         d_hp = torch.empty(2 * total, dtype=torch.float32, device=dev) if hap_prob else None
         torch.cuda.synchronize(dev)
         self._check(self.lib.si_impute_jobs_device(self.h, byref(params), R, len(regions), J, len(jobs),
-                                                   c_void_p(d_geno.data_ptr()), c_void_p(d_dos.data_ptr()),
+                                                   c_void_p(d_geno.data_ptr()),
+                                                   c_void_p(d_dos.data_ptr()) if dosage else None,
                                                    c_void_p(d_hp.data_ptr()) if hap_prob else None,
                                                    c_void_p(d_haps.data_ptr()),
                                                    c_void_p(stream) if stream else None))
         torch.cuda.synchronize(dev)
-        dos, haps = d_dos.cpu().numpy(), d_haps.cpu().numpy()
+        dos, haps = (d_dos.cpu().numpy() if dosage else None), d_haps.cpu().numpy()
         hp = d_hp.cpu().numpy() if hap_prob else None
         out = []
         for i in range(len(jobs)):
             a, n = int(offs[i]), lens[i]
-            o = {"dosage": dos[a:a + n], "haps": haps[2 * a:2 * a + 2 * n].reshape(2, n)}
+            o = {"haps": haps[2 * a:2 * a + 2 * n].reshape(2, n)}
+            if dosage:
+                o["dosage"] = dos[a:a + n]
             if hap_prob:
                 o["hap_prob"] = hp[2 * a:2 * a + 2 * n].reshape(n, 2)
             out.append(o)

@@ -80,6 +80,23 @@ def test_job_alone_equals_job_in_the_mix(engine):
                 assert np.array_equal(alone[key], mix[i][key]), (i, key)
 
 
+def test_haplotypes_without_dosage(engine):
+    # argmax haplotypes alone (no dosage buffer: the posterior variant without the dosage sums)
+    # equal those of the call that also writes dosage, for every job
+    panel, pos = _setup(engine, seed=54)
+    regions = [(0, 1999, 16, N.INDEX_REGION), (10, 900, 8, N.INDEX_GLOBAL), (800, 1200, 4, N.INDEX_REGION)]
+    jobs = []
+    for r, (m0, m1, L, _) in enumerate(regions):
+        codes = _targets(panel, m0, m1, 5, 5, seed=90 + r)
+        jobs += [(r, codes[b], 10 * r + b) for b in range(5)]
+    p = N.default_params()
+    both = engine.impute_jobs(regions, jobs, p)
+    only = engine.impute_jobs(regions, jobs, p, dosage=False)
+    for i in range(len(jobs)):
+        assert "dosage" not in only[i]
+        assert np.array_equal(only[i]["haps"], both[i]["haps"]), i
+
+
 def test_plain_batch_equals_single_full_region(engine):
     panel, pos = _setup(engine, seed=52)
     codes = _targets(panel, 0, 2000, 8, 5, seed=80)

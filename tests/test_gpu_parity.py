@@ -205,6 +205,8 @@ def test_compact_host_formats(engine):
     assert np.array_equal(got["dosage"], full["dosage"])
     only = engine.impute_compact(pack_codes(codes), p)
     assert np.array_equal(only["hap_bits"], got["hap_bits"])
+    # byte haplotypes without a dosage buffer (the posterior variant without the dosage sums)
+    assert np.array_equal(engine.impute(codes, p, dosage=False)["haps"], full["haps"])
     # a panel with alleles other than 0/1 needs the byte output
     engine.upload_panel(with_other_alleles(panel, 71))
     engine.set_map(pos)
